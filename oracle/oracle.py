@@ -1,0 +1,297 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes binding of the CPU oracle.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg may
+import this module, and only as the checker or the CPU baseline.  The
+product package (``topopt3d_b200``) never imports it.
+
+The oracle is an FP64 C restatement of the darinpeetz/TopOpt3D FE path
+(see topopt_oracle.h).  Parity against the reference itself is unpinned: the
+reference has no tests or golden vectors and cannot be built here (PETSc,
+SLEPc, ParMETIS, MPI and Eigen are absent); the oracle is pinned by
+mathematical known-answer tests and an independent scipy sparse solve.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libtopopt_oracle.so")
+_lib = None
+
+
+def build() -> str:
+    """Compile the oracle shared library (make, system gcc + OpenMP)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        src = os.path.join(_HERE, "topopt_oracle.c")
+        if (not os.path.exists(_LIB_PATH)
+                or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src)):
+            build()
+        _lib = C.CDLL(_LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_u8 = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+_i64 = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+_i32 = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+class Params(C.Structure):
+    _fields_ = [("nel", C.c_int * 3), ("dx", C.c_double * 3), ("E0", C.c_double),
+                ("nu", C.c_double), ("rmin", C.c_double), ("mg_levels", C.c_int)]
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("rtol", C.c_double), ("maxit", C.c_int), ("cheb_degree", C.c_int),
+                ("cheb_lo", C.c_double), ("cheb_hi", C.c_double),
+                ("power_its", C.c_int)]
+
+
+def _declare(L):
+    vp = C.c_void_p
+    L.tor_constitutive.argtypes = [C.c_double, C.c_double, _dp]
+    L.tor_element_stiffness.argtypes = [_dp, C.c_double, C.c_double, _dp]
+    L.tor_element_nodes.argtypes = [C.POINTER(C.c_int), C.c_int64, _i64]
+    L.tor_select_nodes.restype = C.c_int64
+    L.tor_select_nodes.argtypes = [C.POINTER(C.c_int), _dp, _dp, _dp, _dp, _dp, vp]
+    L.tor_filter_build.restype = C.c_int64
+    L.tor_filter_build.argtypes = [C.POINTER(C.c_int), _dp, C.c_double, vp, vp, vp]
+    L.tor_vecpow.restype = C.c_double
+    L.tor_vecpow.argtypes = [C.c_double, C.c_double]
+    L.tor_create.restype = vp
+    L.tor_create.argtypes = [C.POINTER(Params)]
+    L.tor_destroy.argtypes = [vp]
+    L.tor_n_nodes.restype = C.c_int64
+    L.tor_n_nodes.argtypes = [vp]
+    L.tor_n_elems.restype = C.c_int64
+    L.tor_n_elems.argtypes = [vp]
+    L.tor_set_bc_arrays.argtypes = [vp, vp, vp]
+    L.tor_add_bc.restype = C.c_int64
+    L.tor_add_bc.argtypes = [vp, C.c_int, _dp, _dp, _dp, _dp]
+    L.tor_get_bc.argtypes = [vp, _u8, _dp]
+    L.tor_set_design.argtypes = [vp, _dp, C.c_double, C.c_double]
+    L.tor_get_material.argtypes = [vp, vp, vp, vp]
+    L.tor_set_moduli.argtypes = [vp, _dp, vp]
+    L.tor_assemble.restype = C.c_int
+    L.tor_assemble.argtypes = [vp, C.POINTER(SolveOpts)]
+    L.tor_apply.argtypes = [vp, _dp, _dp]
+    L.tor_apply_level.argtypes = [vp, C.c_int, _dp, _dp]
+    L.tor_level_nodes.restype = C.c_int64
+    L.tor_level_nodes.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
+    L.tor_level_block.restype = C.c_int
+    L.tor_level_block.argtypes = [vp, C.c_int, C.c_int64, C.c_int64, _dp]
+    L.tor_level_lambda.restype = C.c_double
+    L.tor_level_lambda.argtypes = [vp, C.c_int]
+    L.tor_prolong_weight.restype = C.c_double
+    L.tor_prolong_weight.argtypes = [vp, C.c_int, C.c_int64, C.c_int64]
+    L.tor_vcycle.argtypes = [vp, _dp, _dp]
+    L.tor_solve.restype = C.c_int
+    L.tor_solve.argtypes = [vp, C.POINTER(SolveOpts), _dp, C.POINTER(C.c_int),
+                            C.POINTER(C.c_double)]
+    L.tor_solve_rhs.restype = C.c_int
+    L.tor_solve_rhs.argtypes = [vp, C.POINTER(SolveOpts), _dp, _dp,
+                                C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    L.tor_compliance.argtypes = [vp, _dp, C.POINTER(C.c_double), vp, vp]
+    L.tor_volume.argtypes = [vp, C.POINTER(C.c_double), vp]
+    L.tor_filter.argtypes = [vp, _dp, _dp, C.c_int]
+    L.tor_oc_update.restype = C.c_double
+    L.tor_oc_update.argtypes = [C.c_int64, _dp, _dp, _dp, _dp, C.c_double, _dp,
+                                C.c_double]
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _ivec3(v):
+    return (C.c_int * 3)(*[int(t) for t in v])
+
+
+def element_stiffness(dx=(1.0, 1.0, 1.0), E0=1.0, nu=0.3) -> np.ndarray:
+    K = np.zeros(576)
+    lib().tor_element_stiffness(np.asarray(dx, float), E0, nu, K)
+    return K.reshape(24, 24)
+
+
+def element_nodes(nel, e) -> np.ndarray:
+    out = np.zeros(8, np.int64)
+    lib().tor_element_nodes(_ivec3(nel), int(e), out)
+    return out
+
+
+def select_nodes(nel, dx, center, radius, limits, origin=(0.0, 0.0, 0.0)):
+    L = lib()
+    args = [_ivec3(nel), np.asarray(dx, float), np.asarray(origin, float),
+            np.asarray(center, float), np.asarray(radius, float),
+            np.asarray(limits, float)]
+    n = L.tor_select_nodes(*args, None)
+    out = np.zeros(max(n, 1), np.int64)
+    L.tor_select_nodes(*args, _ptr(out))
+    return out[:n]
+
+
+def filter_csr(nel, dx, R):
+    L = lib()
+    nel3, dx3 = _ivec3(nel), np.asarray(dx, float)
+    nnz = L.tor_filter_build(nel3, dx3, float(R), None, None, None)
+    ne = int(np.prod(nel))
+    rp = np.zeros(ne + 1, np.int64)
+    col = np.zeros(nnz, np.int32)
+    val = np.zeros(nnz)
+    L.tor_filter_build(nel3, dx3, float(R), _ptr(rp), _ptr(col), _ptr(val))
+    return rp, col, val
+
+
+def vecpow(v, p):
+    return lib().tor_vecpow(float(v), float(p))
+
+
+def default_opts(rtol=1e-8, maxit=500, cheb_degree=2, cheb_lo=0.1, cheb_hi=1.1,
+                 power_its=15) -> SolveOpts:
+    return SolveOpts(rtol, maxit, cheb_degree, cheb_lo, cheb_hi, power_its)
+
+
+class Problem:
+    """One oracle TopOpt problem: mesh, filter, BCs, material, hierarchy."""
+
+    def __init__(self, nel, dx=(1.0, 1.0, 1.0), E0=1.0, nu=0.3, rmin=1.5,
+                 mg_levels=3):
+        self.L = lib()
+        self.params = Params(_ivec3(nel), (C.c_double * 3)(*dx), E0, nu, rmin,
+                             mg_levels)
+        self.h = self.L.tor_create(C.byref(self.params))
+        self.nel = tuple(int(t) for t in nel)
+        self.nn = self.L.tor_n_nodes(self.h)
+        self.ne = self.L.tor_n_elems(self.h)
+        self.mg_levels = mg_levels
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.tor_destroy(self.h)
+            self.h = None
+
+    # boundary conditions
+    def add_bc(self, kind, center, radius, limits, values) -> int:
+        t = {"support": 0, "load": 1}[kind]
+        return self.L.tor_add_bc(self.h, t, np.asarray(center, float),
+                                 np.asarray(radius, float),
+                                 np.asarray(limits, float),
+                                 np.asarray(values, float))
+
+    def set_bc(self, fixmask=None, F=None):
+        fm = None if fixmask is None else np.ascontiguousarray(fixmask, np.uint8)
+        ff = None if F is None else np.ascontiguousarray(F, np.float64)
+        self.L.tor_set_bc_arrays(self.h, _ptr(fm), _ptr(ff))
+
+    def get_bc(self):
+        fm = np.zeros(self.nn, np.uint8)
+        F = np.zeros(3 * self.nn)
+        self.L.tor_get_bc(self.h, fm, F)
+        return fm, F
+
+    # material
+    def set_design(self, x, penal=3.0, eps=1e-10):
+        self.L.tor_set_design(self.h, np.ascontiguousarray(x, np.float64),
+                              float(penal), float(eps))
+
+    def set_moduli(self, E, dEdz=None):
+        d = None if dEdz is None else np.ascontiguousarray(dEdz, np.float64)
+        self.L.tor_set_moduli(self.h, np.ascontiguousarray(E, np.float64), _ptr(d))
+
+    def material(self):
+        rho, E, dEdz = np.zeros(self.ne), np.zeros(self.ne), np.zeros(self.ne)
+        self.L.tor_get_material(self.h, _ptr(rho), _ptr(E), _ptr(dEdz))
+        return rho, E, dEdz
+
+    # FE
+    def assemble(self, opts=None):
+        self.opts = opts or default_opts()
+        rc = self.L.tor_assemble(self.h, C.byref(self.opts))
+        if rc != 0:
+            raise RuntimeError("oracle coarse Cholesky failed")
+
+    def apply(self, u):
+        y = np.zeros(3 * self.nn)
+        self.L.tor_apply(self.h, np.ascontiguousarray(u, np.float64), y)
+        return y
+
+    def apply_level(self, level, u):
+        n = self.level_nodes(level)[0]
+        y = np.zeros(3 * n)
+        self.L.tor_apply_level(self.h, level, np.ascontiguousarray(u, np.float64), y)
+        return y
+
+    def level_nodes(self, level):
+        dims = (C.c_int * 3)()
+        n = self.L.tor_level_nodes(self.h, level, dims)
+        return n, tuple(dims)
+
+    def level_block(self, level, i, j):
+        b = np.zeros(9)
+        self.L.tor_level_block(self.h, level, int(i), int(j), b)
+        return b.reshape(3, 3)
+
+    def level_lambda(self, level):
+        return self.L.tor_level_lambda(self.h, level)
+
+    def prolong_weight(self, level, f, c):
+        return self.L.tor_prolong_weight(self.h, level, int(f), int(c))
+
+    def vcycle(self, r):
+        z = np.zeros(3 * self.nn)
+        self.L.tor_vcycle(self.h, np.ascontiguousarray(r, np.float64), z)
+        return z
+
+    def solve(self, U0=None, b=None, opts=None):
+        o = opts or self.opts
+        U = np.zeros(3 * self.nn) if U0 is None else np.array(U0, np.float64)
+        its, rr = C.c_int(0), C.c_double(0)
+        if b is None:
+            st = self.L.tor_solve(self.h, C.byref(o), U, C.byref(its), C.byref(rr))
+        else:
+            st = self.L.tor_solve_rhs(self.h, C.byref(o),
+                                      np.ascontiguousarray(b, np.float64), U,
+                                      C.byref(its), C.byref(rr))
+        return U, st, its.value, rr.value
+
+    def compliance(self, U):
+        c = C.c_double(0)
+        dx, dr = np.zeros(self.ne), np.zeros(self.ne)
+        self.L.tor_compliance(self.h, np.ascontiguousarray(U, np.float64),
+                              C.byref(c), _ptr(dx), _ptr(dr))
+        return c.value, dx, dr
+
+    def volume(self):
+        v = C.c_double(0)
+        dv = np.zeros(self.ne)
+        self.L.tor_volume(self.h, C.byref(v), _ptr(dv))
+        return v.value, dv
+
+    def filter(self, v, transpose=False):
+        out = np.zeros(self.ne)
+        self.L.tor_filter(self.h, np.ascontiguousarray(v, np.float64), out,
+                          int(bool(transpose)))
+        return out
+
+
+def oc_update(x, dfdx, g, dgdx, move, xmin=None, xmax=None):
+    """MMA::OCsub (MMA.cpp:103-180); returns (x_new, change)."""
+    n = x.size
+    xx = np.array(x, np.float64)
+    xmin = np.zeros(n) if xmin is None else np.asarray(xmin, np.float64)
+    xmax = np.ones(n) if xmax is None else np.asarray(xmax, np.float64)
+    df = np.array(dfdx, np.float64)
+    ch = lib().tor_oc_update(n, xx, xmin, xmax, df, float(g),
+                             np.ascontiguousarray(dgdx, np.float64), float(move))
+    return xx, ch
