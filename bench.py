@@ -1,0 +1,432 @@
+"""Benchmark: PCG+GMG solves/s at 5.4M DOF (192x96x96 hex8 cantilever) to
+a relative residual of 1e-8, mixed FP32/FP64 against plain FP64 on the same
+GPU, with the matrix-free apply's achieved HBM bandwidth.
+
+One step = one FE solve from U = 0 (the reference's KSPSolve,
+FEAnalysis.cpp:673) plus the compliance and its filtered sensitivity
+(Compliance.cpp:15-57), with the GMG hierarchy already set up for the
+design -- the split the reference's own timer uses (FEAnalysis.cpp:707-710).
+`e2e` is the whole design iteration through the C ABI with host buffers:
+design upload, MatIntFnc, FEAssemble/PCSetUp, the solve, the sensitivity
+and the download of C and dC/dx.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+For N > 1 (torchrun), every rank solves its own replica of the workload:
+the path does not shard, so there is no data-path collective; the timing
+is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = ("PCG+GMG solves/s at 5.4M DOF to 1e-8: mixed FP32/FP64 vs FP64 "
+          "GPU; apply GB/s")
+UNIT = "solves/s"
+CONFIG = "cfg1"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- helpers
+
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([float(v)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def measured_peaks():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic(name):
+    """dram bytes per launch from a committed ncu summary line
+    `dram_bytes_per_launch: <int>` in profiles/<name>, else None."""
+    p = os.path.join(HERE, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            if line.strip().startswith("dram_bytes_per_launch:"):
+                try:
+                    return int(float(line.split(":", 1)[1]))
+                except ValueError:
+                    return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.proc or not self.file:
+            return None
+        self.file.flush()
+        with open(self.file.name) as f:
+            rows = [r.strip().split(", ") for r in f if r.strip()]
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for k, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(k)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_problem(T, P, cfg):
+    c = P.CONFIGS[cfg]
+    t = T.TopOpt(c["nel"], rmin=c["rmin"], mg_levels=c["levels"])
+    P.apply_bcs(t, P.bcs(cfg))
+    t.FEInitialize()
+    return t
+
+
+# -------------------------------------------------------------- our arm
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    import topopt3d_b200 as T
+    from topopt3d_b200 import problems as P
+
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    cfg = P.CONFIGS[CONFIG]
+    nel = cfg["nel"]
+    ne, nn = int(np.prod(nel)), int(np.prod([n + 1 for n in nel]))
+    x = P.design(CONFIG)
+
+    t = build_problem(T, P, CONFIG)
+    t.set_stream(stream.cuda_stream)
+    x_dev = torch.tensor(x, device=dev)
+    t.MatIntFnc(x_dev)
+    t0 = time.perf_counter()
+    t.FEAssemble()
+    torch.cuda.synchronize(dev)
+    setup_ms = (time.perf_counter() - t0) * 1e3
+
+    zeros_u = torch.zeros(3 * nn, dtype=torch.float64, device=dev)
+    dc = torch.zeros(ne, dtype=torch.float64, device=dev)
+    infos = []
+
+    def step(opts):
+        t.set("U", zeros_u)
+        info = t.FESolve(opts)
+        C, _, _ = t.compliance(out=dc)
+        infos.append((info, C))
+
+    def timed(opts, k, w, sample_clocks=False):
+        for _ in range(w):
+            step(opts)
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        infos.clear()
+        l0 = T.load().tpo_kernel_launches()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        sampler = ClockSampler(local) if sample_clocks else None
+        if sampler:
+            sampler.__enter__()
+        ev0.record(stream)
+        for _ in range(k):
+            step(opts)
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        if sampler:
+            sampler.__exit__(None, None, None)
+        barrier(world)
+        ms = ev0.elapsed_time(ev1)
+        launches = T.load().tpo_kernel_launches() - l0
+        return ms, launches, (sampler.summary() if sampler else None)
+
+    mixed = T.default_opts(precision=T.PREC_MIXED)
+    fp64 = T.default_opts(precision=T.PREC_FP64)
+    ms_mx, launches, clocks = timed(mixed, args.steps, args.warmup, sample_clocks=True)
+    info_mx = infos[-1]
+    ms_64, _, _ = timed(fp64, args.steps, args.warmup)
+    info_64 = infos[-1]
+    ms_mx = max_over_ranks(ms_mx, world)
+    ms_64 = max_over_ranks(ms_64, world)
+    value = world * args.steps / (ms_mx / 1e3)
+    value_64 = world * args.steps / (ms_64 / 1e3)
+
+    # roofline of the dominant kernel: the FP32 matrix-free apply, timed
+    # launch by launch on the library's stream with an L2 flush between
+    peak, peak_kind = measured_peaks()
+    u64 = torch.randn(3 * nn, dtype=torch.float64, device=dev)
+    y64 = torch.empty_like(u64)
+    u32, y32 = u64.float(), torch.empty(3 * nn, dtype=torch.float32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    lib = T.load()
+    import ctypes as C
+    durs = {}
+    for name in ("fp32", "fp64"):
+        ds = []
+        for i in range(12):
+            flush.fill_(float(i))          # evict u, y, E from L2
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            if name == "fp64":
+                t.apply(u64, y64, precision=T.PREC_FP64)
+            else:
+                rc = lib.tpo_apply_f32(t._h, C.c_void_p(u32.data_ptr()),
+                                       C.c_void_p(y32.data_ptr()))
+                assert rc == 0
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            ds.append(e0.elapsed_time(e1))
+        durs[name] = statistics.median(ds[2:])
+    bytes32 = 3 * nn * 4 * 2 + ne * 4 + nn          # u, y, E, fixed mask
+    bytes64 = 3 * nn * 8 * 2 + ne * 8 + nn
+    achieved32 = bytes32 / (durs["fp32"] * 1e-3) / 1e9
+    achieved64 = bytes64 / (durs["fp64"] * 1e-3) / 1e9
+    traffic = committed_traffic("apply_fine_fp32_cfg1.md")
+
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms_mx / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic: seeded uniform[0,1] densities (seed 1), r_min=1.5 filter",
+        "config": {"workload": "192x96x96 hex8 cantilever, 5,447,811 dof, mixed "
+                               "FP32/FP64 PCG + 5-level GMG to 1e-8",
+                   "n_elem": ne, "n_dof": 3 * nn, "levels": cfg["levels"],
+                   "l2": "working set > L2 (126 MB) per solve; apply timing flushes L2"},
+        "iterations": info_mx[0]["iterations"], "outer": info_mx[0]["outer"],
+        "relres": info_mx[0]["relres"], "compliance": info_mx[1],
+        "fp64": {"value": round(value_64, 4), "unit": UNIT,
+                 "ms_per_step": round(ms_64 / args.steps, 4),
+                 "iterations": info_64[0]["iterations"],
+                 "relres": info_64[0]["relres"], "compliance": info_64[1]},
+        "mixed_over_fp64": round(value / value_64, 4),
+        "setup_ms": round(setup_ms, 3),
+        "apply": {"fp32_ms": round(durs["fp32"], 5), "fp64_ms": round(durs["fp64"], 5),
+                  "fp32_gbs": round(achieved32, 1), "fp64_gbs": round(achieved64, 1),
+                  "bytes_fp32": bytes32, "bytes_fp64": bytes64},
+        "roofline": {"bound": "hbm", "achieved": round(achieved32, 1),
+                     "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved32 / peak, 4), "traffic": traffic,
+                     "kernel": "k_apply_fine<float>", "peak_kind": peak_kind},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    t.set_stream(None)
+
+    if not args.no_e2e:
+        line["e2e"] = run_e2e(args, T, P, t, x, world, dev, torch)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(sample_its=3)
+    return line
+
+
+def run_e2e(args, T, P, t, x, world, dev, torch):
+    """Whole design iterations through the C ABI with host buffers."""
+    ne, nn = t.nElem, t.nNode
+    x_h = torch.tensor(x, dtype=torch.float64).pin_memory()
+    dc_h = torch.zeros(ne, dtype=torch.float64).pin_memory()
+    u0 = np.zeros(3 * nn)
+    mixed = T.default_opts(precision=T.PREC_MIXED)
+
+    def step():
+        t.MatIntFnc(x_h)                 # H2D of the design
+        t.FEAssemble()
+        t.set("U", u0)
+        t.FESolve(mixed)
+        C, _, _ = t.compliance(out=dc_h)  # D2H of dC/dx (and C)
+        return C
+
+    for _ in range(args.warmup):
+        step()
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    t.FESolve  # noqa: B018 (keep the handle alive until timing ends)
+    torch.cuda.synchronize(dev)
+    el = max_over_ranks(time.perf_counter() - t0, world)
+    return {"value": round(world * args.steps / el, 4), "unit": UNIT,
+            "h2d_bytes_per_step": ne * 8 + 3 * nn * 8,
+            "d2h_bytes_per_step": ne * 8 + 8,
+            "includes": "design upload, MatIntFnc, FEAssemble/PCSetUp, mixed solve, "
+                        "compliance + dC/dx download"}
+
+
+# ------------------------------------------------------------ CPU baseline
+
+def cpu_baseline(sample_its=3, steps=None, warmup=0):
+    """The oracle's assembled FP64 PCG + GMG (OpenMP, all host threads) on
+    the same 192x96x96 problem.  Sample: `sample_its` PCG iterations per
+    step from U = 0; solves/s = 1 / (per-iteration time x iterations of the
+    full solve, measured once untimed)."""
+    from oracle import oracle as O
+    from topopt3d_b200 import problems as P
+    c = P.CONFIGS[CONFIG]
+    cores = os.cpu_count()
+    ref = O.Problem(c["nel"], rmin=c["rmin"], mg_levels=c["levels"])
+    P.apply_bcs(ref, P.bcs(CONFIG))
+    ref.set_design(P.design(CONFIG), 3.0, 1e-10)
+    t0 = time.perf_counter()
+    ref.assemble(O.default_opts())
+    setup_s = time.perf_counter() - t0
+    # iterations of the full solve (untimed)
+    t0 = time.perf_counter()
+    _, st, its_full, rr = ref.solve(opts=O.default_opts())
+    full_s = time.perf_counter() - t0
+
+    def sample():
+        o0 = O.default_opts(rtol=1e-300, maxit=0)
+        t0 = time.perf_counter()
+        ref.solve(opts=o0)
+        base = time.perf_counter() - t0
+        o = O.default_opts(rtol=1e-300, maxit=sample_its)
+        t0 = time.perf_counter()
+        ref.solve(opts=o)
+        return (time.perf_counter() - t0 - base) / sample_its
+
+    per_it = sample()
+    out = {"value": round(1.0 / (per_it * its_full), 6), "unit": UNIT,
+           "cores": cores, "kind": "port",
+           "sample": f"{sample_its} PCG+GMG iterations of the 192x96x96 problem "
+                     f"(assembled BSR SpMV, FP64, OpenMP) x {its_full} iterations of "
+                     f"the full solve; setup {setup_s:.1f} s and a full solve "
+                     f"({full_s:.1f} s, status {st}) untimed",
+           "per_iteration_s": per_it, "full_solve_s": full_s}
+    if steps:
+        for _ in range(warmup):
+            sample()
+        ts = [sample() for _ in range(steps)]
+        out["per_iteration_s"] = statistics.mean(ts)
+        out["value"] = round(1.0 / (out["per_iteration_s"] * its_full), 6)
+    return out
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the reference's FE path on the host cores.  The
+    reference (PETSc/SLEPc/ParMETIS/MPI/Eigen) cannot be built in this image,
+    so its CPU path runs as the oracle restatement."""
+    if rank != 0:
+        return None
+    cb = cpu_baseline(sample_its=2, steps=args.steps, warmup=min(args.warmup, 1))
+    return {"impl": "reference", "metric": METRIC, "value": cb["value"],
+            "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "192x96x96 hex8 cantilever, 5,447,811 dof, FP64 "
+                                   "PCG + 5-level GMG to 1e-8 (CPU)"},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_setup(args)
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+    else:
+        line = run_ours(args, rank, world, local)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,198 @@
+/*
+ * topopt_b200.h -- C ABI of the B200-native TopOpt3D finite-element path.
+ *
+ * One context (tpo_ctx) holds one structured hex8 problem on one GPU: the
+ * mesh, boundary conditions, density filter, SIMP material, the geometric
+ * multigrid hierarchy and the solution vectors, all resident in HBM.  Every
+ * entry point returns an int status: 0 = success, > 0 = the solver stopped
+ * without converging (iterations and residual are still reported),
+ * < 0 = error (see TPO_E_*); tpo_last_error() gives the message.  No entry
+ * point aborts the process.  A context is bound to the device that was
+ * current at tpo_create and must not be used from two host threads at once.
+ *
+ * Vectors use the reference numbering: element e = i + j*nx + k*nx*ny,
+ * node n = i + j*(nx+1) + k*(nx+1)*(ny+1), dof = 3*n + component.  Buffers
+ * are FP64 and caller-owned; `mem` selects host (TPO_MEM_HOST) or device
+ * (TPO_MEM_DEVICE) pointers.  Host buffers are copied inside the call.
+ *
+ * Each declaration names the darinpeetz/TopOpt3D member it replaces
+ * (file:line in that tree).
+ */
+#ifndef TOPOPT_B200_H
+#define TOPOPT_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define TPO_API __attribute__((visibility("default")))
+#else
+#define TPO_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TPO_OK 0
+#define TPO_NOT_CONVERGED 1
+#define TPO_E_ARG (-1)      /* invalid argument or call order */
+#define TPO_E_CUDA (-2)     /* CUDA runtime / library error */
+#define TPO_E_BREAKDOWN (-3)/* CG breakdown, non-finite residual, indefinite */
+#define TPO_E_UNSUPPORTED (-4)
+
+#define TPO_MEM_HOST 0
+#define TPO_MEM_DEVICE 1
+
+#define TPO_PREC_FP64 0     /* FP64 apply, smoother, transfers, CG */
+#define TPO_PREC_MIXED 1    /* FP32 inner PCG+GMG inside FP64 defect correction */
+
+#define TPO_BC_SUPPORT 0
+#define TPO_BC_LOAD 1
+
+typedef struct tpo_ctx tpo_ctx;
+
+typedef struct {
+  int32_t nel[3];     /* elements per dimension (NEL) */
+  double dx[3];       /* element edge lengths (Dimensions / NEL) */
+  double E0, nu;      /* Young's modulus and Poisson ratio (E0, Nu0) */
+  double rmin;        /* density-filter radius, absolute (RMin) */
+  int32_t mg_levels;  /* GMG levels incl. the finest (-kuf_pc_mg_levels);
+                         <= 0 selects floor(log2(min nel)) as the reference */
+} tpo_mesh_params;
+
+typedef struct {
+  double rtol;        /* ||F - K U|| <= rtol * ||F|| (KSP rtol 1e-8) */
+  int32_t maxit;      /* CG iterations (inner iterations in mixed form) */
+  int32_t precision;  /* TPO_PREC_FP64 or TPO_PREC_MIXED */
+  int32_t cheb_degree;/* Chebyshev steps per smoothing (2) */
+  double cheb_lo;     /* smoothing interval [lo, hi] * lambda_max(D^-1 A) */
+  double cheb_hi;
+  int32_t power_its;  /* power iterations for lambda_max at setup (15) */
+  double inner_rtol;  /* mixed form: relative drop per inner solve (1e-4) */
+  int32_t max_outer;  /* mixed form: defect-correction passes (10) */
+  int32_t use_graph;  /* capture the V-cycle/CG iteration in a CUDA graph */
+} tpo_solve_opts;
+
+typedef struct {
+  int32_t status;     /* as the return code */
+  int32_t iterations; /* CG iterations (sum over inner solves when mixed) */
+  int32_t outer;      /* defect-correction passes (1 in FP64 form) */
+  double relres;      /* final ||F - K U|| / ||F||, FP64 */
+  double solve_ms;    /* host wall time of the solve phase */
+  double setup_ms;    /* host wall time of the last FEAssemble/PCSetUp */
+} tpo_solve_info;
+
+/* fills the defaults used throughout (rtol 1e-8, maxit 500, FP64, Chebyshev
+ * degree 2 on [0.1, 1.1] * lambda, 15 power iterations, inner_rtol 1e-4,
+ * max_outer 10, graphs on) */
+TPO_API void tpo_default_solve_opts(tpo_solve_opts *opts);
+
+/* TopOpt::CreateMesh (RecMesh.cpp:426-728) on one device: structured box
+ * mesh, density filter (Filter.cpp:21-150), GMG level layout
+ * (Interpolation.cpp:31-169) and the element stiffness K0
+ * (FEAnalysis.cpp:869-1050). */
+TPO_API int tpo_create(const tpo_mesh_params *params, tpo_ctx **out);
+/* TopOpt::Clear (TopOpt.cpp:59-89) */
+TPO_API int tpo_destroy(tpo_ctx *ctx);
+TPO_API const char *tpo_last_error(const tpo_ctx *ctx);
+
+/* sizes: elements, nodes, levels actually built */
+TPO_API int tpo_sizes(const tpo_ctx *ctx, int64_t *n_elem, int64_t *n_node,
+              int32_t *n_levels);
+/* GMG level l (0 = finest): nodes per dimension */
+TPO_API int tpo_level_dims(const tpo_ctx *ctx, int32_t level, int32_t dims[3]);
+
+/* TopOpt::Set_BC (Inputs.cpp:105-223) for SUPPORT and LOAD: selects every
+ * node with sum_d ((x_d-c_d)/r_d)^2 <= 1 inside limits [lo0,hi0,lo1,hi1,
+ * lo2,hi2]; a support fixes each component whose value is non-zero, a load
+ * adds `values` to every selected node.  *n_selected receives the count. */
+TPO_API int tpo_add_bc(tpo_ctx *ctx, int32_t type, const double center[3],
+               const double radius[3], const double limits[6],
+               const double values[3], int64_t *n_selected);
+/* direct form: per-node fixed-component bitmask (bit c fixes component c)
+ * and load vector F (3*nNode); either may be NULL to keep the current one */
+TPO_API int tpo_set_bc(tpo_ctx *ctx, const uint8_t *fixmask, const double *F, int mem);
+TPO_API int tpo_get_bc(const tpo_ctx *ctx, uint8_t *fixmask, double *F, int mem);
+
+/* TopOpt::FEInitialize (FEAnalysis.cpp:215-424): freezes the BCs, uploads
+ * the fixed mask and F, allocates the solver state (U = 0). */
+TPO_API int tpo_fe_initialize(tpo_ctx *ctx);
+
+/* TopOpt::MatIntFnc (Material_Interpolation.cpp:20-140) with vdMin <= 0:
+ * rho = P x, E = eps + (1-eps) rho^p, dEdz = (1-eps) p rho^(p-1).
+ * The reference hard-codes eps = 1e-10 (:28). */
+TPO_API int tpo_mat_int_fnc(tpo_ctx *ctx, const double *x, double penal, double eps,
+                    int mem);
+/* set E (and optionally dEdz) directly, bypassing filter and SIMP */
+TPO_API int tpo_set_moduli(tpo_ctx *ctx, const double *E, const double *dEdz, int mem);
+
+/* TopOpt::FEAssemble + PCSetUp (FEAnalysis.cpp:432-490, :541-573): the
+ * matrix-free fine operator with the Dirichlet fixes, Galerkin coarse
+ * operators P^T A P on every level, Jacobi diagonals, Chebyshev bounds and
+ * the coarsest-level Cholesky factor. */
+TPO_API int tpo_fe_assemble(tpo_ctx *ctx, const tpo_solve_opts *opts);
+
+/* TopOpt::FESolve (FEAnalysis.cpp:507-732): PCG + GMG on K U = F from the
+ * context's current U (nonzero initial guess, :389). */
+TPO_API int tpo_fe_solve(tpo_ctx *ctx, const tpo_solve_opts *opts,
+                 tpo_solve_info *info);
+
+/* solve K U = b for nrhs right-hand sides (column-major, 3*nNode each);
+ * U holds the initial guesses and receives the solutions. */
+TPO_API int tpo_solve(tpo_ctx *ctx, const double *b, double *U, int32_t nrhs,
+              int mem, const tpo_solve_opts *opts, tpo_solve_info *info);
+
+/* y = K(rho) u on the finest level (the reference MatMult(K), with the
+ * MatZeroRowsColumns identity rows, FEAnalysis.cpp:473), nrhs columns;
+ * precision TPO_PREC_FP64 or TPO_PREC_MIXED (FP32 arithmetic). */
+TPO_API int tpo_apply(tpo_ctx *ctx, const double *u, double *y, int32_t nrhs,
+              int32_t precision, int mem);
+/* FP32 form of tpo_apply on device buffers only (3*nNode floats each): the
+ * matrix-free kernel alone, as used inside the mixed-precision solve. */
+TPO_API int tpo_apply_f32(tpo_ctx *ctx, const float *u, float *y);
+/* y = A_l u on GMG level l with the assembled Galerkin operator (l >= 1) */
+TPO_API int tpo_apply_level(tpo_ctx *ctx, int32_t level, const double *u, double *y,
+                    int mem);
+/* one application of the GMG V-cycle preconditioner z = M r (finest) */
+TPO_API int tpo_vcycle(tpo_ctx *ctx, const double *r, double *z, int32_t precision,
+               int mem);
+/* lambda_max(D^-1 A_l) estimate used by the Chebyshev smoother */
+TPO_API int tpo_level_lambda(const tpo_ctx *ctx, int32_t level, double *lambda);
+
+/* U, F, x, rho, E, dEdz accessors: which = "U","F","x","rho","E","dEdz" */
+TPO_API int tpo_get_vector(const tpo_ctx *ctx, const char *which, double *out, int mem);
+TPO_API int tpo_set_vector(tpo_ctx *ctx, const char *which, const double *in, int mem);
+
+/* Compliance::Function (Compliance.cpp:15-57) on the context's U:
+ * C = U.F and dC/dx = P^T(-dEdz .* u_e^T K0 u_e) (Chain_Filter,
+ * Material_Interpolation.cpp:150-187).  dCdx / dCdrho may be NULL. */
+TPO_API int tpo_compliance(tpo_ctx *ctx, double *C, double *dCdx, double *dCdrho,
+                   int mem);
+/* Volume::Function (Volume.cpp:15-41): V = sum(rho)/nElem, dV/dx */
+TPO_API int tpo_volume(tpo_ctx *ctx, double *V, double *dVdx, int mem);
+/* MatMult(P) (transpose = 0) or MatMultTranspose(P) (transpose = 1) */
+TPO_API int tpo_filter(tpo_ctx *ctx, const double *in, double *out, int32_t transpose,
+               int mem);
+
+/* MMA::OCsub (MMA.cpp:103-180) on the GPU, OCeta = 0.5: x (nElem) is
+ * updated in place; dfdx is clipped to <= 0 in place; returns Change. */
+TPO_API int tpo_oc_update(tpo_ctx *ctx, double *x, const double *xmin,
+                  const double *xmax, double *dfdx, double g,
+                  const double *dgdx, double move, double *change, int mem);
+
+/* block until all work of the context is done */
+TPO_API int tpo_sync(tpo_ctx *ctx);
+
+/* run the context's work on a caller stream (a cudaStream_t passed as
+ * void*); NULL restores the context's own stream.  No reference
+ * counterpart: it lets a host framework order and time the kernels. */
+TPO_API int tpo_set_stream(tpo_ctx *ctx, void *stream);
+
+/* number of kernels this library has launched in the process (graph
+ * launches count their kernel nodes).  No reference counterpart. */
+TPO_API int64_t tpo_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TOPOPT_B200_H */

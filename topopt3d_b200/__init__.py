@@ -1,0 +1,15 @@
+"""B200-native finite-element hot path of darinpeetz/TopOpt3D.
+
+The GPU library (``libtopopt_b200.so``, C ABI in ``include/topopt_b200.h``)
+implements the SIMP hex8 stiffness apply, the GMG-preconditioned CG solve
+(FP64 and mixed FP32/FP64), the compliance sensitivity and the density
+filter.  ``TopOpt`` mirrors the reference's call surface.
+"""
+from ._lib import (BC_LOAD, BC_SUPPORT, MEM_DEVICE, MEM_HOST, PREC_FP64,
+                   PREC_MIXED, SolveInfo, SolveOpts, default_opts, load)
+from .topopt import OC, Compliance, Function_Base, TopOpt, TopOptError, Volume
+
+__all__ = ["TopOpt", "TopOptError", "Compliance", "Volume", "Function_Base",
+           "OC", "SolveOpts", "SolveInfo", "default_opts", "load",
+           "PREC_FP64", "PREC_MIXED", "MEM_HOST", "MEM_DEVICE", "BC_SUPPORT",
+           "BC_LOAD"]

@@ -1,0 +1,73 @@
+"""Build the CUDA library libtopopt_b200.so in-tree for sm_100a.
+
+Used by ``__graft_entry__.build()`` and importable on its own:
+``python -m topopt3d_b200.build``.
+"""
+from __future__ import annotations
+
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libtopopt_b200.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
+         "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
+
+
+def sources():
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")) +
+                  glob.glob(os.path.join(CSRC, "*.cpp")))
+
+
+def needs_build() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = sources() + glob.glob(os.path.join(CSRC, "*.h")) + \
+        glob.glob(os.path.join(CSRC, "*.cuh")) + \
+        [os.path.join(HERE, "..", "include", "topopt_b200.h")]
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(verbose: bool = False, force: bool = False, jobs: int = 8) -> str:
+    if not force and not needs_build():
+        return LIB
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    objs, procs = [], []
+    for src in sources():
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        objs.append(obj)
+        cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj]
+        if verbose:
+            cmd.append("-Xptxas=-v")
+        procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE,
+                                            stderr=subprocess.STDOUT)))
+        if len(procs) >= jobs:
+            _wait(procs, verbose)
+            procs = []
+    _wait(procs, verbose)
+    link = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcusolver", "-lcublas"]
+    subprocess.run(link, check=True)
+    return LIB
+
+
+def _wait(procs, verbose):
+    for cmd, p in procs:
+        out, _ = p.communicate()
+        text = out.decode(errors="replace")
+        if p.returncode != 0:
+            sys.stderr.write(text)
+            raise RuntimeError("nvcc failed: " + " ".join(cmd))
+        if verbose and text:
+            sys.stderr.write(text)
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv, force=True))

@@ -1,0 +1,736 @@
+// The C ABI (include/topopt_b200.h): context life cycle, boundary
+// conditions, the TopOpt call surface and data movement between caller
+// buffers and the context's HBM-resident state.
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "solver.h"
+
+using tpo::Ctx;
+
+struct tpo_ctx {
+  Ctx c;
+};
+
+namespace tpo {
+std::atomic<long long> g_launches{0};
+}
+
+namespace {
+
+#define CK(call)                                                       \
+  do {                                                                 \
+    cudaError_t e_ = (call);                                           \
+    if (e_ != cudaSuccess) {                                           \
+      c.err = std::string(#call) + ": " + cudaGetErrorString(e_);      \
+      return TPO_E_CUDA;                                               \
+    }                                                                  \
+  } while (0)
+
+#define REQUIRE(cond, msg)   \
+  do {                       \
+    if (!(cond)) {           \
+      c.err = (msg);         \
+      return TPO_E_ARG;      \
+    }                        \
+  } while (0)
+
+template <typename T>
+int dalloc(Ctx &c, T **p, size_t n) {
+  if (*p) return TPO_OK;
+  CK(cudaMalloc(reinterpret_cast<void **>(p), sizeof(T) * std::max<size_t>(n, 1)));
+  CK(cudaMemsetAsync(*p, 0, sizeof(T) * std::max<size_t>(n, 1), c.stream));
+  return TPO_OK;
+}
+
+template <typename T>
+void dfree(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+// Eigen 3.3 LinSpaced (floating point) as used for the node coordinates
+// (RecMesh.cpp:582-597)
+double linspaced(double lo, double hi, int64_t n, int64_t i) {
+  if (n == 1) return hi;
+  const double step = (hi - lo) / static_cast<double>(n - 1);
+  if (std::fabs(hi) < std::fabs(lo))
+    return (i == 0) ? lo : hi - static_cast<double>(n - 1 - i) * step;
+  return (i == n - 1) ? hi : lo + static_cast<double>(i) * step;
+}
+
+int begin(tpo_ctx *ctx) {
+  if (!ctx) return TPO_E_ARG;
+  cudaError_t e = cudaSetDevice(ctx->c.device);
+  if (e != cudaSuccess) {
+    ctx->c.err = std::string("cudaSetDevice: ") + cudaGetErrorString(e);
+    return TPO_E_CUDA;
+  }
+  ctx->c.err.clear();
+  return TPO_OK;
+}
+
+int finish(Ctx &c, int rc) {
+  if (rc < 0) return rc;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    c.err = std::string("kernel launch: ") + cudaGetErrorString(e);
+    return TPO_E_CUDA;
+  }
+  return rc;
+}
+
+// device view of a caller buffer: device pointers pass through, host
+// buffers are staged into `buf`
+int stage_in(Ctx &c, const double *p, size_t n, int mem, double *buf,
+             const double **out) {
+  if (mem == TPO_MEM_DEVICE) {
+    *out = p;
+    return TPO_OK;
+  }
+  CK(cudaMemcpyAsync(buf, p, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream));
+  *out = buf;
+  return TPO_OK;
+}
+
+int copy_out(Ctx &c, double *dst, const double *src, size_t n, int mem) {
+  if (!dst) return TPO_OK;
+  if (dst == src) return TPO_OK;
+  CK(cudaMemcpyAsync(dst, src, sizeof(double) * n,
+                     mem == TPO_MEM_DEVICE ? cudaMemcpyDeviceToDevice
+                                           : cudaMemcpyDeviceToHost,
+                     c.stream));
+  if (mem != TPO_MEM_DEVICE) CK(cudaStreamSynchronize(c.stream));
+  return TPO_OK;
+}
+
+int check_mem(Ctx &c, int mem) {
+  REQUIRE(mem == TPO_MEM_HOST || mem == TPO_MEM_DEVICE, "mem must be TPO_MEM_HOST or TPO_MEM_DEVICE");
+  return TPO_OK;
+}
+
+int alloc_solver(Ctx &c) {
+  const size_t n0 = 3 * c.nn;
+  int rc = 0;
+#define A(p, n) \
+  if ((rc = dalloc(c, &(p), (n))) != TPO_OK) return rc
+  A(c.S0, 243 * c.nn);
+  for (int l = 0; l < c.L; ++l) {
+    tpo::Level &v = c.lev[l];
+    const size_t n = 3 * v.nn;
+    A(v.dinv64, n);
+    A(v.dinv32, n);
+    A(v.r64, n); A(v.d64, n); A(v.a64, n);
+    A(v.r32, n); A(v.d32, n); A(v.a32, n);
+    if (l > 0) {
+      A(v.b64, n); A(v.x64, n); A(v.b32, n); A(v.x32, n);
+      A(v.S64, 243 * v.nn);
+      if (l + 1 < c.L) A(v.S32, 243 * v.nn);
+    }
+  }
+  const int64_t nc = 3 * c.lev[c.L - 1].nn;
+  A(c.Adense, (size_t)(nc * nc));
+  A(c.Ainv, (size_t)(nc * nc));
+  A(c.r64, n0); A(c.z64, n0); A(c.p64, n0); A(c.q64, n0); A(c.w64, n0);
+  A(c.r32, n0); A(c.z32, n0); A(c.p32, n0); A(c.q32, n0); A(c.x32, n0);
+#undef A
+  return TPO_OK;
+}
+
+void free_all(Ctx &c) {
+  tpo::invalidate_graphs(c);
+  for (tpo::Level &v : c.lev) {
+    dfree(v.S64); dfree(v.S32); dfree(v.dinv64); dfree(v.dinv32);
+    dfree(v.b64); dfree(v.x64); dfree(v.r64); dfree(v.d64); dfree(v.a64);
+    dfree(v.b32); dfree(v.x32); dfree(v.r32); dfree(v.d32); dfree(v.a32);
+  }
+  dfree(c.fix); dfree(c.F); dfree(c.U); dfree(c.x); dfree(c.rho);
+  dfree(c.E64); dfree(c.dEdz); dfree(c.E32); dfree(c.S0); dfree(c.K0lex);
+  dfree(c.Ainv); dfree(c.Adense); dfree(c.solver_work); dfree(c.dev_info);
+  dfree(c.finv); dfree(c.taps_d);
+  dfree(c.r64); dfree(c.z64); dfree(c.p64); dfree(c.q64); dfree(c.w64);
+  dfree(c.r32); dfree(c.z32); dfree(c.p32); dfree(c.q32); dfree(c.x32);
+  dfree(c.scal); dfree(c.part); dfree(c.ticket); dfree(c.tmpe); dfree(c.tmpe2);
+  dfree(c.io_a); dfree(c.io_b);
+  dfree(c.oc_ws);
+  if (c.scal_h) cudaFreeHost(c.scal_h);
+  c.scal_h = nullptr;
+  if (c.cusolver) cusolverDnDestroy(static_cast<cusolverDnHandle_t>(c.cusolver));
+  c.cusolver = nullptr;
+  if (c.own_stream) cudaStreamDestroy(c.own_stream);
+  c.own_stream = c.stream = nullptr;
+}
+
+double *vec_ptr(Ctx &c, const char *which, size_t *n) {
+  if (!which) return nullptr;
+  if (!std::strcmp(which, "U")) { *n = 3 * c.nn; return c.U; }
+  if (!std::strcmp(which, "F")) { *n = 3 * c.nn; return c.F; }
+  if (!std::strcmp(which, "x")) { *n = c.ne; return c.x; }
+  if (!std::strcmp(which, "rho")) { *n = c.ne; return c.rho; }
+  if (!std::strcmp(which, "E")) { *n = c.ne; return c.E64; }
+  if (!std::strcmp(which, "dEdz")) { *n = c.ne; return c.dEdz; }
+  return nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+void tpo_default_solve_opts(tpo_solve_opts *o) {
+  if (!o) return;
+  o->rtol = 1e-8;
+  o->maxit = 500;
+  o->precision = TPO_PREC_FP64;
+  o->cheb_degree = 2;
+  o->cheb_lo = 0.1;
+  o->cheb_hi = 1.1;
+  o->power_its = 15;
+  o->inner_rtol = 1e-4;
+  o->max_outer = 10;
+  o->use_graph = 1;
+}
+
+const char *tpo_last_error(const tpo_ctx *ctx) {
+  return ctx ? ctx->c.err.c_str() : "null context";
+}
+
+int tpo_create(const tpo_mesh_params *p, tpo_ctx **out) {
+  if (!p || !out) return TPO_E_ARG;
+  *out = nullptr;
+  for (int d = 0; d < 3; ++d)
+    if (p->nel[d] < 1 || !(p->dx[d] > 0)) return TPO_E_ARG;
+  if (!(p->E0 > 0) || !(p->nu > -1.0 && p->nu < 0.5) || !(p->rmin > 0))
+    return TPO_E_ARG;
+  tpo_ctx *ctx = new tpo_ctx();
+  Ctx &c = ctx->c;
+  c.prm = *p;
+  for (int d = 0; d < 3; ++d) c.nel[d] = p->nel[d];
+  c.ne = (int64_t)c.nel[0] * c.nel[1] * c.nel[2];
+  c.nn = (int64_t)(c.nel[0] + 1) * (c.nel[1] + 1) * (c.nel[2] + 1);
+  if (3 * c.nn >= (int64_t)1 << 31) {
+    delete ctx;
+    return TPO_E_UNSUPPORTED;
+  }
+  // levels: floor(log2(min nel)) unless given (RecMesh.cpp:552-557), cut
+  // when a level has <= 10 dofs (Interpolation.cpp:61-69)
+  int L = p->mg_levels;
+  if (L <= 0) {
+    const int mn = std::min(c.nel[0], std::min(c.nel[1], c.nel[2]));
+    L = (int)std::log2((double)mn);
+  }
+  if (L < 1) L = 1;
+  int dims[3] = {c.nel[0] + 1, c.nel[1] + 1, c.nel[2] + 1};
+  c.lev.clear();
+  for (int l = 0; l < L; ++l) {
+    tpo::Level v;
+    std::memcpy(v.dims, dims, sizeof(dims));
+    v.nn = (int64_t)dims[0] * dims[1] * dims[2];
+    c.lev.push_back(v);
+    for (int d = 0; d < 3; ++d) dims[d] = (dims[d] + 1) / 2;
+    if (l + 1 < L && 3LL * dims[0] * dims[1] * dims[2] <= 10) {
+      L = l + 2;
+    }
+  }
+  c.L = (int)c.lev.size();
+  const int64_t ncoarse = 3 * c.lev[c.L - 1].nn;
+  if (ncoarse > 12000) {
+    c.err = "coarsest level too large for the dense solve; use more levels";
+    delete ctx;
+    return TPO_E_UNSUPPORTED;
+  }
+  int rc = tpo::build_element_constants(c);
+  if (rc != TPO_OK) {
+    delete ctx;
+    return rc;
+  }
+  if (!tpo::build_filter_taps(c.nel, p->dx, p->rmin, c.taps)) {
+    delete ctx;
+    return TPO_E_UNSUPPORTED;
+  }
+  c.fix_h.assign(c.nn, 0);
+  c.F_h.assign(3 * c.nn, 0.0);
+  if (cudaGetDevice(&c.device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c.own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return TPO_E_CUDA;
+  }
+  c.stream = c.own_stream;
+  auto fail = [&](int code) {
+    free_all(c);
+    delete ctx;
+    return code;
+  };
+  const size_t nio = std::max<size_t>(3 * c.nn, c.ne);
+#define A(p, n) \
+  if (dalloc(c, &(p), (n)) != TPO_OK) return fail(TPO_E_CUDA)
+  A(c.taps_d, 1);
+  A(c.finv, c.ne); A(c.K0lex, 576);
+  A(c.x, c.ne); A(c.rho, c.ne); A(c.E64, c.ne); A(c.dEdz, c.ne); A(c.E32, c.ne);
+  A(c.fix, c.nn); A(c.F, 3 * c.nn); A(c.U, 3 * c.nn);
+  A(c.scal, 16); A(c.part, tpo::kRedBlocks); A(c.ticket, 1);
+  A(c.tmpe, c.ne); A(c.tmpe2, c.ne); A(c.dev_info, 1);
+  A(c.io_a, nio); A(c.io_b, nio);
+#undef A
+  if (cudaMallocHost(&c.scal_h, 16 * sizeof(double)) != cudaSuccess)
+    return fail(TPO_E_CUDA);
+  static constexpr int kLexToLocal[8] = {0, 1, 3, 2, 4, 5, 7, 6};
+  double Kl[576];
+  for (int a = 0; a < 8; ++a)
+    for (int b = 0; b < 8; ++b)
+      for (int r = 0; r < 3; ++r)
+        for (int q = 0; q < 3; ++q)
+          Kl[24 * (3 * a + r) + 3 * b + q] =
+              c.K0[24 * (3 * kLexToLocal[a] + r) + 3 * kLexToLocal[b] + q];
+  if (cudaMemcpyAsync(c.K0lex, Kl, sizeof(Kl), cudaMemcpyHostToDevice, c.stream) != cudaSuccess ||
+      cudaMemcpyAsync(c.taps_d, &c.taps, sizeof(c.taps), cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
+    return fail(TPO_E_CUDA);
+  tpo::launch_filter_rowsum(c, c.stream);
+  if (cudaStreamSynchronize(c.stream) != cudaSuccess || cudaGetLastError() != cudaSuccess)
+    return fail(TPO_E_CUDA);
+  *out = ctx;
+  return TPO_OK;
+}
+
+int tpo_destroy(tpo_ctx *ctx) {
+  if (!ctx) return TPO_OK;
+  cudaSetDevice(ctx->c.device);
+  if (ctx->c.stream) cudaStreamSynchronize(ctx->c.stream);
+  free_all(ctx->c);
+  delete ctx;
+  return TPO_OK;
+}
+
+int tpo_sizes(const tpo_ctx *ctx, int64_t *n_elem, int64_t *n_node,
+              int32_t *n_levels) {
+  if (!ctx) return TPO_E_ARG;
+  if (n_elem) *n_elem = ctx->c.ne;
+  if (n_node) *n_node = ctx->c.nn;
+  if (n_levels) *n_levels = ctx->c.L;
+  return TPO_OK;
+}
+
+int tpo_level_dims(const tpo_ctx *ctx, int32_t level, int32_t dims[3]) {
+  if (!ctx || !dims || level < 0 || level >= ctx->c.L) return TPO_E_ARG;
+  for (int d = 0; d < 3; ++d) dims[d] = ctx->c.lev[level].dims[d];
+  return TPO_OK;
+}
+
+int tpo_add_bc(tpo_ctx *ctx, int32_t type, const double center[3],
+               const double radius[3], const double limits[6],
+               const double values[3], int64_t *n_selected) {
+  if (!ctx) return TPO_E_ARG;
+  Ctx &c = ctx->c;
+  c.err.clear();
+  REQUIRE(center && radius && limits && values, "null BC argument");
+  REQUIRE(type == TPO_BC_SUPPORT || type == TPO_BC_LOAD, "unknown BC type");
+  // Set_BC node selection (Inputs.cpp:116-124), nodes in increasing order
+  const int64_t N[3] = {c.nel[0] + 1, c.nel[1] + 1, c.nel[2] + 1};
+  int64_t cnt = 0;
+  for (int64_t n = 0; n < c.nn; ++n) {
+    const int64_t idx[3] = {n % N[0], (n / N[0]) % N[1], n / (N[0] * N[1])};
+    double dist = 0;
+    bool valid = true;
+    for (int d = 0; d < 3; ++d) {
+      const double xd = linspaced(0.0, c.prm.dx[d] * c.nel[d], N[d], idx[d]);
+      const double t = (xd - center[d]) / radius[d];
+      dist += t * t;
+      valid = valid && xd >= limits[2 * d] && xd <= limits[2 * d + 1];
+    }
+    if (!(valid && dist <= 1)) continue;
+    ++cnt;
+    for (int d = 0; d < 3; ++d) {
+      if (type == TPO_BC_SUPPORT) {
+        if (values[d] != 0) c.fix_h[n] |= (uint8_t)(1u << d);
+      } else {
+        c.F_h[3 * n + d] += values[d];   // FEAnalysis.cpp:352-355
+      }
+    }
+  }
+  if (n_selected) *n_selected = cnt;
+  if (c.initialized) {
+    cudaSetDevice(c.device);
+    CK(cudaMemcpyAsync(c.fix, c.fix_h.data(), c.nn, cudaMemcpyHostToDevice, c.stream));
+    CK(cudaMemcpyAsync(c.F, c.F_h.data(), sizeof(double) * 3 * c.nn, cudaMemcpyHostToDevice, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    c.assembled = false;
+  }
+  return TPO_OK;
+}
+
+int tpo_set_bc(tpo_ctx *ctx, const uint8_t *fixmask, const double *F, int mem) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = check_mem(c, mem)) return rc;
+  const cudaMemcpyKind k = mem == TPO_MEM_DEVICE ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost;
+  if (fixmask) CK(cudaMemcpy(c.fix_h.data(), fixmask, c.nn, k));
+  if (F) CK(cudaMemcpy(c.F_h.data(), F, sizeof(double) * 3 * c.nn, k));
+  if (c.initialized) {
+    CK(cudaMemcpyAsync(c.fix, c.fix_h.data(), c.nn, cudaMemcpyHostToDevice, c.stream));
+    CK(cudaMemcpyAsync(c.F, c.F_h.data(), sizeof(double) * 3 * c.nn, cudaMemcpyHostToDevice, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    c.assembled = false;
+  }
+  return TPO_OK;
+}
+
+int tpo_get_bc(const tpo_ctx *cctx, uint8_t *fixmask, double *F, int mem) {
+  tpo_ctx *ctx = const_cast<tpo_ctx *>(cctx);
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = check_mem(c, mem)) return rc;
+  const cudaMemcpyKind k = mem == TPO_MEM_DEVICE ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost;
+  if (fixmask) CK(cudaMemcpy(fixmask, c.fix_h.data(), c.nn, k));
+  if (F) CK(cudaMemcpy(F, c.F_h.data(), sizeof(double) * 3 * c.nn, k));
+  return TPO_OK;
+}
+
+int tpo_fe_initialize(tpo_ctx *ctx) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = alloc_solver(c)) return rc;
+  CK(cudaMemcpyAsync(c.fix, c.fix_h.data(), c.nn, cudaMemcpyHostToDevice, c.stream));
+  CK(cudaMemcpyAsync(c.F, c.F_h.data(), sizeof(double) * 3 * c.nn, cudaMemcpyHostToDevice, c.stream));
+  CK(cudaMemsetAsync(c.U, 0, sizeof(double) * 3 * c.nn, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  c.initialized = true;
+  c.assembled = false;
+  return TPO_OK;
+}
+
+int tpo_mat_int_fnc(tpo_ctx *ctx, const double *x, double penal, double eps,
+                    int mem) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = check_mem(c, mem)) return rc;
+  REQUIRE(x, "null design vector");
+  REQUIRE(penal > 0 && eps >= 0 && eps < 1, "invalid penalty or eps");
+  if (mem == TPO_MEM_DEVICE)
+    CK(cudaMemcpyAsync(c.x, x, sizeof(double) * c.ne, cudaMemcpyDeviceToDevice, c.stream));
+  else
+    CK(cudaMemcpyAsync(c.x, x, sizeof(double) * c.ne, cudaMemcpyHostToDevice, c.stream));
+  tpo::launch_filter(c, c.x, c.rho, false, c.stream);   // rho = P x (:35)
+  tpo::launch_simp(c, penal, eps, c.stream);
+  c.have_material = true;
+  c.assembled = false;
+  return finish(c, TPO_OK);
+}
+
+int tpo_set_moduli(tpo_ctx *ctx, const double *E, const double *dEdz, int mem) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = check_mem(c, mem)) return rc;
+  REQUIRE(E, "null E");
+  const cudaMemcpyKind k = mem == TPO_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  CK(cudaMemcpyAsync(c.E64, E, sizeof(double) * c.ne, k, c.stream));
+  if (dEdz) CK(cudaMemcpyAsync(c.dEdz, dEdz, sizeof(double) * c.ne, k, c.stream));
+  tpo::launch_d2f(c.ne, c.E64, c.E32, c.stream);
+  CK(cudaStreamSynchronize(c.stream));
+  c.have_material = true;
+  c.assembled = false;
+  return finish(c, TPO_OK);
+}
+
+int tpo_fe_assemble(tpo_ctx *ctx, const tpo_solve_opts *opts) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  REQUIRE(c.initialized, "tpo_fe_initialize must be called first");
+  REQUIRE(c.have_material, "no material: call tpo_mat_int_fnc or tpo_set_moduli");
+  tpo_solve_opts o;
+  if (opts) o = *opts; else tpo_default_solve_opts(&o);
+  REQUIRE(o.cheb_degree >= 1 && o.cheb_hi > o.cheb_lo && o.cheb_lo >= 0 && o.power_its >= 1,
+          "invalid smoother options");
+  return finish(c, tpo::setup_hierarchy(c, o));
+}
+
+static int validate_solve(Ctx &c, const tpo_solve_opts &o) {
+  REQUIRE(c.assembled, "tpo_fe_assemble must be called first");
+  REQUIRE(o.rtol > 0 && o.maxit >= 0, "invalid rtol/maxit");
+  REQUIRE(o.precision == TPO_PREC_FP64 || o.precision == TPO_PREC_MIXED, "invalid precision");
+  REQUIRE(o.cheb_degree == c.setup_opts.cheb_degree && o.cheb_lo == c.setup_opts.cheb_lo &&
+              o.cheb_hi == c.setup_opts.cheb_hi,
+          "smoother options differ from those given to tpo_fe_assemble");
+  REQUIRE(o.precision == TPO_PREC_FP64 || (o.inner_rtol > 0 && o.inner_rtol < 1 && o.max_outer >= 1),
+          "invalid mixed-precision options");
+  return TPO_OK;
+}
+
+int tpo_fe_solve(tpo_ctx *ctx, const tpo_solve_opts *opts, tpo_solve_info *info) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  tpo_solve_opts o;
+  if (opts) o = *opts; else { tpo_default_solve_opts(&o); o.cheb_degree = c.setup_opts.cheb_degree; }
+  if (int rc = validate_solve(c, o)) return rc;
+  return finish(c, tpo::solve(c, o, c.F, c.U, info));
+}
+
+int tpo_solve(tpo_ctx *ctx, const double *b, double *U, int32_t nrhs, int mem,
+              const tpo_solve_opts *opts, tpo_solve_info *info) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = check_mem(c, mem)) return rc;
+  REQUIRE(b && U && nrhs >= 1, "invalid solve arguments");
+  tpo_solve_opts o;
+  if (opts) o = *opts; else tpo_default_solve_opts(&o);
+  if (int rc = validate_solve(c, o)) return rc;
+  const size_t n = 3 * c.nn;
+  int worst = TPO_OK;
+  tpo_solve_info acc{};
+  for (int j = 0; j < nrhs; ++j) {
+    const double *bj = b + j * n;
+    double *uj = U + j * n;
+    const double *db = nullptr;
+    double *du = uj;
+    if (int rc = stage_in(c, bj, n, mem, c.io_a, &db)) return rc;
+    if (mem != TPO_MEM_DEVICE) {
+      CK(cudaMemcpyAsync(c.io_b, uj, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream));
+      du = c.io_b;
+    }
+    tpo_solve_info one{};
+    const int rc = tpo::solve(c, o, db, du, &one);
+    if (rc < 0) return finish(c, rc);
+    if (int rc2 = copy_out(c, uj, du, n, mem)) return rc2;
+    if (rc != TPO_OK && worst == TPO_OK) worst = rc;
+    acc.iterations += one.iterations;
+    acc.outer += one.outer;
+    acc.relres = std::max(acc.relres, one.relres);
+    acc.solve_ms += one.solve_ms;
+  }
+  acc.status = worst;
+  acc.setup_ms = c.setup_ms;
+  if (info) *info = acc;
+  return finish(c, worst);
+}
+
+int tpo_apply(tpo_ctx *ctx, const double *u, double *y, int32_t nrhs,
+              int32_t precision, int mem) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = check_mem(c, mem)) return rc;
+  REQUIRE(u && y && nrhs >= 1, "invalid apply arguments");
+  REQUIRE(c.initialized && c.have_material, "mesh not initialised or no material");
+  REQUIRE(precision == TPO_PREC_FP64 || precision == TPO_PREC_MIXED, "invalid precision");
+  const size_t n = 3 * c.nn;
+  for (int j = 0; j < nrhs; ++j) {
+    const double *du = nullptr;
+    if (int rc = stage_in(c, u + j * n, n, mem, c.io_a, &du)) return rc;
+    double *dy = (mem == TPO_MEM_DEVICE) ? y + j * n : c.io_b;
+    if (precision == TPO_PREC_FP64) {
+      tpo::launch_apply_fine<double>(c, c.E64, du, nullptr, dy, c.stream);
+    } else {
+      tpo::launch_d2f(n, du, c.r32, c.stream);
+      tpo::launch_apply_fine<float>(c, c.E32, c.r32, nullptr, c.q32, c.stream);
+      tpo::launch_f2d(n, c.q32, dy, c.stream);
+    }
+    if (int rc = copy_out(c, y + j * n, dy, n, mem)) return rc;
+  }
+  return finish(c, TPO_OK);
+}
+
+int tpo_apply_f32(tpo_ctx *ctx, const float *u, float *y) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  REQUIRE(u && y && u != y, "invalid apply arguments");
+  REQUIRE(c.initialized && c.have_material, "mesh not initialised or no material");
+  tpo::launch_apply_fine<float>(c, c.E32, u, nullptr, y, c.stream);
+  return finish(c, TPO_OK);
+}
+
+int tpo_apply_level(tpo_ctx *ctx, int32_t level, const double *u, double *y,
+                    int mem) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = check_mem(c, mem)) return rc;
+  REQUIRE(c.assembled, "tpo_fe_assemble must be called first");
+  REQUIRE(level >= 0 && level < c.L && u && y, "invalid level or buffer");
+  const size_t n = 3 * c.lev[level].nn;
+  const double *du = nullptr;
+  if (int rc = stage_in(c, u, n, mem, c.io_a, &du)) return rc;
+  double *dy = (mem == TPO_MEM_DEVICE) ? y : c.io_b;
+  if (level == 0)
+    tpo::launch_apply_fine<double>(c, c.E64, du, nullptr, dy, c.stream);
+  else
+    tpo::launch_apply_stencil<double>(c.lev[level], c.lev[level].S64, du, nullptr, dy, c.stream);
+  if (int rc = copy_out(c, y, dy, n, mem)) return rc;
+  return finish(c, TPO_OK);
+}
+
+int tpo_vcycle(tpo_ctx *ctx, const double *r, double *z, int32_t precision, int mem) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = check_mem(c, mem)) return rc;
+  REQUIRE(c.assembled, "tpo_fe_assemble must be called first");
+  REQUIRE(r && z, "null buffer");
+  const size_t n = 3 * c.nn;
+  const double *dr = nullptr;
+  if (int rc = stage_in(c, r, n, mem, c.io_a, &dr)) return rc;
+  double *dz = (mem == TPO_MEM_DEVICE) ? z : c.io_b;
+  if (int rc = tpo::vcycle_apply(c, c.setup_opts, precision, dr, dz)) return rc;
+  if (int rc = copy_out(c, z, dz, n, mem)) return rc;
+  return finish(c, TPO_OK);
+}
+
+int tpo_level_lambda(const tpo_ctx *ctx, int32_t level, double *lambda) {
+  if (!ctx || !lambda || level < 0 || level >= ctx->c.L) return TPO_E_ARG;
+  *lambda = ctx->c.lev[level].lam;
+  return TPO_OK;
+}
+
+int tpo_get_vector(const tpo_ctx *cctx, const char *which, double *out, int mem) {
+  tpo_ctx *ctx = const_cast<tpo_ctx *>(cctx);
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = check_mem(c, mem)) return rc;
+  size_t n = 0;
+  double *p = vec_ptr(c, which, &n);
+  REQUIRE(p && out, "unknown vector name or null buffer");
+  CK(cudaMemcpyAsync(out, p, sizeof(double) * n,
+                     mem == TPO_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                     c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  return TPO_OK;
+}
+
+int tpo_set_vector(tpo_ctx *ctx, const char *which, const double *in, int mem) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = check_mem(c, mem)) return rc;
+  size_t n = 0;
+  double *p = vec_ptr(c, which, &n);
+  REQUIRE(p && in, "unknown vector name or null buffer");
+  CK(cudaMemcpyAsync(p, in, sizeof(double) * n,
+                     mem == TPO_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                     c.stream));
+  if (p == c.E64) {
+    // new moduli invalidate the hierarchy
+    tpo::launch_d2f(c.ne, c.E64, c.E32, c.stream);
+    c.have_material = true;
+    c.assembled = false;
+  }
+  CK(cudaStreamSynchronize(c.stream));
+  return finish(c, TPO_OK);
+}
+
+int tpo_compliance(tpo_ctx *ctx, double *C, double *dCdx, double *dCdrho, int mem) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = check_mem(c, mem)) return rc;
+  REQUIRE(c.initialized && c.have_material, "mesh not initialised or no material");
+  const int64_t n = 3 * c.nn;
+  if (C) {
+    tpo::launch_dot<double>(c, n, c.U, c.F, c.scal + 8, nullptr, c.stream);  // :19
+    CK(cudaMemcpyAsync(c.scal_h + 8, c.scal + 8, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  }
+  if (dCdx || dCdrho) {
+    tpo::launch_sensitivity(c, c.U, c.tmpe, c.stream);                      // :37-46
+    if (dCdrho)
+      if (int rc = copy_out(c, dCdrho, c.tmpe, c.ne, mem)) return rc;
+    if (dCdx) {
+      tpo::launch_filter(c, c.tmpe, c.tmpe2, true, c.stream);              // :51
+      if (int rc = copy_out(c, dCdx, c.tmpe2, c.ne, mem)) return rc;
+    }
+  }
+  CK(cudaStreamSynchronize(c.stream));
+  if (C) *C = c.scal_h[8];
+  return finish(c, TPO_OK);
+}
+
+int tpo_volume(tpo_ctx *ctx, double *V, double *dVdx, int mem) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = check_mem(c, mem)) return rc;
+  REQUIRE(c.have_material, "no material");
+  if (V) {
+    tpo::launch_fill(c.ne, c.tmpe2, 1.0, c.stream);
+    tpo::launch_dot<double>(c, c.ne, c.rho, c.tmpe2, c.scal + 9, nullptr, c.stream);
+    CK(cudaMemcpyAsync(c.scal_h + 9, c.scal + 9, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  }
+  if (dVdx) {
+    tpo::launch_filter_adj_uniform(c, 1.0 / (double)c.ne, c.tmpe, c.stream);
+    if (int rc = copy_out(c, dVdx, c.tmpe, c.ne, mem)) return rc;
+  }
+  CK(cudaStreamSynchronize(c.stream));
+  if (V) *V = c.scal_h[9] / (double)c.ne;
+  return finish(c, TPO_OK);
+}
+
+int tpo_filter(tpo_ctx *ctx, const double *in, double *out, int32_t transpose, int mem) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = check_mem(c, mem)) return rc;
+  REQUIRE(in && out, "null buffer");
+  const double *din = nullptr;
+  if (int rc = stage_in(c, in, c.ne, mem, c.io_a, &din)) return rc;
+  double *dout = (mem == TPO_MEM_DEVICE) ? out : c.io_b;
+  REQUIRE(din != dout, "filter input and output must differ");
+  tpo::launch_filter(c, din, dout, transpose != 0, c.stream);
+  if (int rc = copy_out(c, out, dout, c.ne, mem)) return rc;
+  return finish(c, TPO_OK);
+}
+
+int tpo_oc_update(tpo_ctx *ctx, double *x, const double *xmin, const double *xmax,
+                  double *dfdx, double g, const double *dgdx, double move,
+                  double *change, int mem) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = check_mem(c, mem)) return rc;
+  REQUIRE(x && xmin && xmax && dfdx && dgdx, "null OC argument");
+  const int64_t n = c.ne;
+  if (!c.oc_ws) CK(cudaMalloc(&c.oc_ws, sizeof(double) * 6 * n));
+  double *dx = c.oc_ws, *dxold = dx + n, *dmin = dx + 2 * n, *dmax = dx + 3 * n,
+         *ddf = dx + 4 * n, *ddg = dx + 5 * n;
+  const cudaMemcpyKind k = mem == TPO_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  CK(cudaMemcpyAsync(dxold, x, sizeof(double) * n, k, c.stream));
+  CK(cudaMemcpyAsync(dmin, xmin, sizeof(double) * n, k, c.stream));
+  CK(cudaMemcpyAsync(dmax, xmax, sizeof(double) * n, k, c.stream));
+  CK(cudaMemcpyAsync(ddf, dfdx, sizeof(double) * n, k, c.stream));
+  CK(cudaMemcpyAsync(ddg, dgdx, sizeof(double) * n, k, c.stream));
+  tpo::launch_oc_clip(n, ddf, c.stream);
+  // bisection on the Lagrange multiplier (MMA.cpp:136-161)
+  double l1 = 0, l2 = 1e6;
+  while (l2 - l1 > 1e-4) {
+    const double lmid = 0.5 * (l1 + l2);
+    tpo::launch_oc_step(c, n, dx, dxold, dmin, dmax, ddf, ddg, move, lmid, c.scal + 10, c.stream);
+    CK(cudaMemcpyAsync(c.scal_h + 10, c.scal + 10, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    if (g + c.scal_h[10] > 0) l1 = lmid; else l2 = lmid;
+  }
+  tpo::launch_oc_finish(c, n, dx, dxold, dmin, dmax, c.scal + 11, c.stream);
+  CK(cudaMemcpyAsync(c.scal_h + 11, c.scal + 11, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  const cudaMemcpyKind ko = mem == TPO_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  CK(cudaMemcpyAsync(x, dx, sizeof(double) * n, ko, c.stream));
+  CK(cudaMemcpyAsync(dfdx, ddf, sizeof(double) * n, ko, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  if (change) *change = c.scal_h[11];
+  return finish(c, TPO_OK);
+}
+
+int tpo_sync(tpo_ctx *ctx) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  CK(cudaStreamSynchronize(c.stream));
+  return finish(c, TPO_OK);
+}
+
+int tpo_set_stream(tpo_ctx *ctx, void *stream) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  cudaStream_t next = stream ? static_cast<cudaStream_t>(stream) : c.own_stream;
+  if (next != c.stream) {
+    // order the switch: the new stream waits for work already issued
+    cudaEvent_t ev;
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(ev, c.stream));
+    CK(cudaStreamWaitEvent(next, ev, 0));
+    CK(cudaEventDestroy(ev));
+    c.stream = next;
+  }
+  return TPO_OK;
+}
+
+int64_t tpo_kernel_launches(void) { return tpo::g_launches.load(); }
+
+}  // extern "C"

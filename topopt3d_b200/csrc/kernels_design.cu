@@ -1,0 +1,274 @@
+// Design-side kernels: the density filter (forward and transpose, matrix
+// free), SIMP interpolation, the compliance sensitivity and the OC update.
+#include <math_constants.h>
+
+#include "modal.cuh"
+
+namespace tpo {
+
+namespace {
+
+int grid_for(int64_t n, int threads) {
+  int64_t g = (n + threads - 1) / threads;
+  if (g > 148 * 32) g = 148 * 32;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+// row sums of the raw filter (Filter.cpp:136-147): finv = 1 / sum_j W_ij,
+// summed in increasing column order
+__global__ void k_filter_rowsum(int nx, int ny, int nz,
+                                const FilterTaps *__restrict__ taps,
+                                double *finv) {
+  const int64_t ne = (int64_t)nx * ny * nz;
+  const int nt = taps->n;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int i = e % nx, j = (e / nx) % ny, k = e / ((int64_t)nx * ny);
+    double s = 0;
+    for (int t = 0; t < nt; ++t) {
+      const int a = i + taps->off[t][0], b = j + taps->off[t][1], c = k + taps->off[t][2];
+      if (a < 0 || a >= nx || b < 0 || b >= ny || c < 0 || c >= nz) continue;
+      s += taps->w[t];
+    }
+    finv[e] = 1.0 / s;
+  }
+}
+
+// rho_i = sum_j (W_ij * finv_i) x_j  (MatMult(P), Material_Interpolation.cpp:35)
+__global__ void k_filter_fwd(int nx, int ny, int nz,
+                             const FilterTaps *__restrict__ taps,
+                             const double *__restrict__ finv,
+                             const double *__restrict__ in,
+                             double *__restrict__ out) {
+  const int64_t ne = (int64_t)nx * ny * nz;
+  const int nt = taps->n;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int i = e % nx, j = (e / nx) % ny, k = e / ((int64_t)nx * ny);
+    const double fi = finv[e];
+    double s = 0;
+    for (int t = 0; t < nt; ++t) {
+      const int a = i + taps->off[t][0], b = j + taps->off[t][1], c = k + taps->off[t][2];
+      if (a < 0 || a >= nx || b < 0 || b >= ny || c < 0 || c >= nz) continue;
+      s += (taps->w[t] * fi) * in[((int64_t)c * ny + b) * nx + a];
+    }
+    out[e] = s;
+  }
+}
+
+// out_j = sum_i (W_ij * finv_i) g_i over rows i in increasing order
+// (MatMultTranspose(P), Material_Interpolation.cpp:160,180)
+__global__ void k_filter_adj(int nx, int ny, int nz,
+                             const FilterTaps *__restrict__ taps,
+                             const double *__restrict__ finv,
+                             const double *__restrict__ in, double uniform,
+                             double *__restrict__ out) {
+  const int64_t ne = (int64_t)nx * ny * nz;
+  const int nt = taps->n;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int i = e % nx, j = (e / nx) % ny, k = e / ((int64_t)nx * ny);
+    double s = 0;
+    for (int t = nt - 1; t >= 0; --t) {
+      const int a = i - taps->off[t][0], b = j - taps->off[t][1], c = k - taps->off[t][2];
+      if (a < 0 || a >= nx || b < 0 || b >= ny || c < 0 || c >= nz) continue;
+      const int64_t r = ((int64_t)c * ny + b) * nx + a;
+      s += (taps->w[t] * finv[r]) * (in ? in[r] : uniform);
+    }
+    out[e] = s;
+  }
+}
+
+// PETSc VecPow special cases (used by MatIntFnc)
+__device__ __forceinline__ double vecpow(double v, double p) {
+  if (p == 1.0) return v;
+  if (p == -1.0) return 1.0 / v;
+  if (p == 0.0) return (v == v) ? 1.0 : v;
+  if (p == 0.5) return v >= 0 ? sqrt(v) : CUDART_INF;
+  if (p == -0.5) return v >= 0 ? 1.0 / sqrt(v) : CUDART_INF;
+  if (p == 2.0) return v * v;
+  if (p == -2.0) return 1.0 / (v * v);
+  return v >= 0 ? pow(v, p) : CUDART_INF;
+}
+
+// Material_Interpolation.cpp:40-75 with vdMin <= 0 (y = 1, z = rho)
+__global__ void k_simp(int64_t ne, const double *__restrict__ rho, double penal,
+                       double eps, double *E, double *dEdz, float *E32) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const double z = rho[e];
+    double d = vecpow(z, penal - 1);
+    const double es = d * z;
+    d = d * penal;
+    dEdz[e] = d * (1 - eps);
+    const double Ee = eps + (1 - eps) * es;
+    E[e] = Ee;
+    E32[e] = static_cast<float>(Ee);
+  }
+}
+
+// dc_e = -dEdz_e * u_e^T K0 u_e (Compliance.cpp:37-46)
+__global__ void k_sensitivity(int nelx, int nely, int nelz,
+                              const double *__restrict__ U,
+                              const double *__restrict__ dEdz, double *dc,
+                              const Kh<double> kh) {
+  const int Nx = nelx + 1, Ny = nely + 1;
+  const int64_t ne = (int64_t)nelx * nely * nelz;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int i = e % nelx, j = (e / nelx) % nely, k = e / ((int64_t)nelx * nely);
+    double v[8][3];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+      const int64_t n = ((int64_t)(k + (l >> 2)) * Ny + (j + ((l >> 1) & 1))) * Nx +
+                        (i + (l & 1));
+#pragma unroll
+      for (int c = 0; c < 3; ++c) v[l][c] = U[3 * n + c];
+    }
+    dc[e] = -dEdz[e] * element_energy(v, kh);
+  }
+}
+
+__global__ void k_oc_clip(int64_t n, double *dfdx) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    if (dfdx[i] > 0) dfdx[i] = 0;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// one bisection trial of MMA::OCsub (MMA.cpp:139-160): candidate x and
+// per-block partial sums of dgdx . (x - xold)
+__global__ void k_oc_step(int64_t n, double *x, const double *xold,
+                          const double *xmin, const double *xmax,
+                          const double *dfdx, const double *dgdx, double move,
+                          double lmid, double *part) {
+  __shared__ double sh[32];
+  double s = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double B = pow(-dfdx[i] / dgdx[i] / lmid, 0.5);
+    const double xo = xold[i], lo = xmin[i], hi = xmax[i];
+    const double step = move * (hi - lo);
+    double v = lo + (xo - lo) * B;
+    v = fmin(v, xo + step);
+    v = fmin(v, hi);
+    v = fmax(v, xo - step);
+    v = fmax(v, lo);
+    x[i] = v;
+    s += dgdx[i] * (v - xo);
+  }
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+    s = warp_sum(s);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+  }
+}
+
+__global__ void k_sum_parts(int nparts, const double *part, double *out) {
+  __shared__ double sh[32];
+  double s = 0;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += part[i];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+    s = warp_sum(s);
+    if (threadIdx.x == 0) *out = s;
+  }
+}
+
+// x < 1e-6 -> 0 (MMA.cpp:166-173), then Change = max |x - xold| / (xmax - xmin)
+__global__ void k_oc_finish(int64_t n, double *x, const double *xold,
+                            const double *xmin, const double *xmax,
+                            unsigned long long *out) {
+  double m = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double v = x[i];
+    if (v < 1e-6) {
+      v = 0;
+      x[i] = 0;
+    }
+    m = fmax(m, fabs((v - xold[i]) / (xmax[i] - xmin[i])));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+}  // namespace
+
+void launch_filter_rowsum(const Ctx &c, cudaStream_t s) {
+  count_launch();
+  k_filter_rowsum<<<grid_for(c.ne, 256), 256, 0, s>>>(c.nel[0], c.nel[1],
+                                                       c.nel[2], c.taps_d, c.finv);
+}
+
+void launch_filter(const Ctx &c, const double *in, double *out, bool transpose,
+                   cudaStream_t s) {
+  count_launch();
+  if (transpose)
+    k_filter_adj<<<grid_for(c.ne, 256), 256, 0, s>>>(
+        c.nel[0], c.nel[1], c.nel[2], c.taps_d, c.finv, in, 0.0, out);
+  else
+    k_filter_fwd<<<grid_for(c.ne, 256), 256, 0, s>>>(
+        c.nel[0], c.nel[1], c.nel[2], c.taps_d, c.finv, in, out);
+}
+
+void launch_filter_adj_uniform(const Ctx &c, double value, double *out,
+                               cudaStream_t s) {
+  count_launch();
+  k_filter_adj<<<grid_for(c.ne, 256), 256, 0, s>>>(
+      c.nel[0], c.nel[1], c.nel[2], c.taps_d, c.finv, nullptr, value, out);
+}
+
+void launch_simp(const Ctx &c, double penal, double eps, cudaStream_t s) {
+  count_launch();
+  k_simp<<<grid_for(c.ne, 256), 256, 0, s>>>(c.ne, c.rho, penal, eps, c.E64,
+                                              c.dEdz, c.E32);
+}
+
+void launch_sensitivity(const Ctx &c, const double *U, double *dc,
+                        cudaStream_t s) {
+  count_launch();
+  k_sensitivity<<<grid_for(c.ne, 128), 128, 0, s>>>(c.nel[0], c.nel[1], c.nel[2],
+                                                     U, c.dEdz, dc, c.kh64);
+}
+
+void launch_oc_clip(int64_t n, double *dfdx, cudaStream_t s) {
+  count_launch();
+  k_oc_clip<<<grid_for(n, 256), 256, 0, s>>>(n, dfdx);
+}
+
+void launch_oc_step(const Ctx &c, int64_t n, double *x, const double *xold,
+                    const double *xmin, const double *xmax, const double *dfdx,
+                    const double *dgdx, double move, double lmid, double *out,
+                    cudaStream_t s) {
+  count_launch();
+  count_launch();   // k_oc_step + k_sum_parts
+  k_oc_step<<<kRedBlocks, 256, 0, s>>>(n, x, xold, xmin, xmax, dfdx, dgdx, move,
+                                       lmid, c.part);
+  k_sum_parts<<<1, 256, 0, s>>>(kRedBlocks, c.part, out);
+}
+
+void launch_oc_finish(const Ctx &c, int64_t n, double *x, const double *xold,
+                      const double *xmin, const double *xmax, double *out,
+                      cudaStream_t s) {
+  count_launch();
+  (void)c;
+  cudaMemsetAsync(out, 0, sizeof(double), s);
+  k_oc_finish<<<grid_for(n, 256), 256, 0, s>>>(
+      n, x, xold, xmin, xmax, reinterpret_cast<unsigned long long *>(out));
+}
+
+}  // namespace tpo

@@ -1,0 +1,412 @@
+// Geometric multigrid kernels: Galerkin coarse operators, stencil operator
+// on the coarse levels, trilinear transfers, Chebyshev/Jacobi smoother
+// updates and the dense coarsest-level solve.
+//
+// Level layout (Interpolation.cpp:31-169): a coarse node sits on every even
+// fine node index; level l+1 has (N_l + 1) / 2 nodes per dimension,
+// numbered lexicographically.  The prolongation weight of coarse node c for
+// fine node f is prod_d w_d with w_d = 1 (f_d = 2c_d) or 1/2 (|f_d - 2c_d| =
+// 1), each row normalised to sum 1 (Interpolation.cpp:330-347).  The
+// normalisation factorises per dimension, so weights are computed on the
+// fly from the indices; no interpolation matrix is stored.
+//
+// Coarse operators are A_{l+1} = P^T A_l P (PCMG Galerkin,
+// FEAnalysis.cpp:412), stored as 27-point 3x3-block stencils in SoA form
+// S[(nb*9 + 3r + s) * nn + node].
+#include "tpo_internal.h"
+
+namespace tpo {
+
+namespace {
+
+int grid_for(int64_t n, int threads, int64_t cap = 148 * 32) {
+  int64_t g = (n + threads - 1) / threads;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+// normalised 1-D prolongation weight of coarse index c for fine index f
+// (fine extent Nf)
+__device__ __forceinline__ double pw1(int f, int c, int Nf) {
+  const int d = f - 2 * c;
+  if (d < -1 || d > 1) return 0.0;
+  if (d == 0) return 1.0;
+  // odd f: neighbours (f-1)/2 always, (f+1)/2 if f+1 <= Nf-1
+  return (f + 1 <= Nf - 1) ? 0.5 : 1.0;
+}
+
+// A_c(I, I+delta) = sum_f sum_g P(f,I) A_f(f,g) P(g,I+delta); one thread
+// per (coarse node, delta) block.  Fine nodes f run over the support of I
+// and g over the stencil of f intersected with the support of J, both in
+// increasing index order.
+__global__ void k_galerkin(int fx, int fy, int fz, int cx, int cy, int cz,
+                           const double *__restrict__ Sf,
+                           double *__restrict__ Sc) {
+  const int64_t nnf = (int64_t)fx * fy * fz, nnc = (int64_t)cx * cy * cz;
+  const int64_t total = nnc * 27;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int nb = (int)(t / nnc);
+    const int64_t I = t - (int64_t)nb * nnc;
+    const int ix = I % cx, iy = (I / cx) % cy, iz = I / ((int64_t)cx * cy);
+    const int jx = ix + nb % 3 - 1, jy = iy + (nb / 3) % 3 - 1, jz = iz + nb / 9 - 1;
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (jx >= 0 && jx < cx && jy >= 0 && jy < cy && jz >= 0 && jz < cz) {
+      for (int az = -1; az <= 1; ++az) {
+        const int gzf = 2 * iz + az;
+        if (gzf < 0 || gzf >= fz) continue;
+        const double wiz = pw1(gzf, iz, fz);
+        if (wiz == 0.0) continue;
+        for (int ay = -1; ay <= 1; ++ay) {
+          const int gyf = 2 * iy + ay;
+          if (gyf < 0 || gyf >= fy) continue;
+          const double wiy = pw1(gyf, iy, fy);
+          if (wiy == 0.0) continue;
+          for (int ax = -1; ax <= 1; ++ax) {
+            const int gxf = 2 * ix + ax;
+            if (gxf < 0 || gxf >= fx) continue;
+            const double wix = pw1(gxf, ix, fx);
+            if (wix == 0.0) continue;
+            const double wI = wix * wiy * wiz;
+            const int64_t f = ((int64_t)gzf * fy + gyf) * fx + gxf;
+            for (int ez = -1; ez <= 1; ++ez) {
+              const int hz = gzf + ez;
+              if (hz < 0 || hz >= fz) continue;
+              const double wjz = pw1(hz, jz, fz);
+              if (wjz == 0.0) continue;
+              for (int ey = -1; ey <= 1; ++ey) {
+                const int hy = gyf + ey;
+                if (hy < 0 || hy >= fy) continue;
+                const double wjy = pw1(hy, jy, fy);
+                if (wjy == 0.0) continue;
+                for (int ex = -1; ex <= 1; ++ex) {
+                  const int hx = gxf + ex;
+                  if (hx < 0 || hx >= fx) continue;
+                  const double wjx = pw1(hx, jx, fx);
+                  if (wjx == 0.0) continue;
+                  const double w = wI * (wjx * wjy * wjz);
+                  const int fnb = (ez + 1) * 9 + (ey + 1) * 3 + (ex + 1);
+                  const double *blk = Sf + (int64_t)fnb * 9 * nnf + f;
+#pragma unroll
+                  for (int q = 0; q < 9; ++q) acc[q] += w * blk[q * nnf];
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) Sc[(int64_t)(nb * 9 + q) * nnc + I] = acc[q];
+  }
+}
+
+template <typename T, bool RESID>
+__global__ void k_apply_stencil(int nx, int ny, int nz, const T *__restrict__ S,
+                                const T *__restrict__ u, const T *__restrict__ b,
+                                T *__restrict__ y) {
+  const int64_t nn = (int64_t)nx * ny * nz;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
+       n += (int64_t)gridDim.x * blockDim.x) {
+    const int i = n % nx, j = (n / nx) % ny, k = n / ((int64_t)nx * ny);
+    T a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll
+    for (int nb = 0; nb < 27; ++nb) {
+      const int mi = i + nb % 3 - 1, mj = j + (nb / 3) % 3 - 1, mk = k + nb / 9 - 1;
+      if (mi < 0 || mi >= nx || mj < 0 || mj >= ny || mk < 0 || mk >= nz) continue;
+      const int64_t m = ((int64_t)mk * ny + mj) * nx + mi;
+      const T u0 = u[3 * m], u1 = u[3 * m + 1], u2 = u[3 * m + 2];
+      const T *s = S + (int64_t)nb * 9 * nn + n;
+      a0 += s[0] * u0 + s[nn] * u1 + s[2 * nn] * u2;
+      a1 += s[3 * nn] * u0 + s[4 * nn] * u1 + s[5 * nn] * u2;
+      a2 += s[6 * nn] * u0 + s[7 * nn] * u1 + s[8 * nn] * u2;
+    }
+    if (RESID) {
+      a0 = b[3 * n] - a0;
+      a1 = b[3 * n + 1] - a1;
+      a2 = b[3 * n + 2] - a2;
+    }
+    y[3 * n] = a0;
+    y[3 * n + 1] = a1;
+    y[3 * n + 2] = a2;
+  }
+}
+
+__global__ void k_stencil_diag(int64_t nn, const double *__restrict__ S,
+                               double *dinv64, float *dinv32) {
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
+       n += (int64_t)gridDim.x * blockDim.x) {
+    for (int c = 0; c < 3; ++c) {
+      const double d = S[(int64_t)(13 * 9 + 4 * c) * nn + n];
+      dinv64[3 * n + c] = 1.0 / d;
+      dinv32[3 * n + c] = static_cast<float>(1.0 / d);
+    }
+  }
+}
+
+// b_c = P^T r_f
+template <typename T>
+__global__ void k_restrict(int fx, int fy, int fz, int cx, int cy, int cz,
+                           const T *__restrict__ rf, T *__restrict__ bc) {
+  const int64_t nnc = (int64_t)cx * cy * cz;
+  for (int64_t I = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; I < nnc;
+       I += (int64_t)gridDim.x * blockDim.x) {
+    const int ix = I % cx, iy = (I / cx) % cy, iz = I / ((int64_t)cx * cy);
+    T s0 = 0, s1 = 0, s2 = 0;
+    for (int az = -1; az <= 1; ++az) {
+      const int gz = 2 * iz + az;
+      if (gz < 0 || gz >= fz) continue;
+      const double wz = pw1(gz, iz, fz);
+      if (wz == 0.0) continue;
+      for (int ay = -1; ay <= 1; ++ay) {
+        const int gy = 2 * iy + ay;
+        if (gy < 0 || gy >= fy) continue;
+        const double wy = pw1(gy, iy, fy);
+        if (wy == 0.0) continue;
+        for (int ax = -1; ax <= 1; ++ax) {
+          const int gx = 2 * ix + ax;
+          if (gx < 0 || gx >= fx) continue;
+          const double wx = pw1(gx, ix, fx);
+          if (wx == 0.0) continue;
+          const T w = static_cast<T>(wx * wy * wz);
+          const int64_t f = ((int64_t)gz * fy + gy) * fx + gx;
+          s0 += w * rf[3 * f];
+          s1 += w * rf[3 * f + 1];
+          s2 += w * rf[3 * f + 2];
+        }
+      }
+    }
+    bc[3 * I] = s0;
+    bc[3 * I + 1] = s1;
+    bc[3 * I + 2] = s2;
+  }
+}
+
+// x_f += P x_c
+template <typename T>
+__global__ void k_prolong_add(int fx, int fy, int fz, int cx, int cy, int cz,
+                              const T *__restrict__ xc, T *__restrict__ xf) {
+  const int64_t nnf = (int64_t)fx * fy * fz;
+  for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < nnf;
+       f += (int64_t)gridDim.x * blockDim.x) {
+    const int gx = f % fx, gy = (f / fx) % fy, gz = f / ((int64_t)fx * fy);
+    T s0 = 0, s1 = 0, s2 = 0;
+    for (int cz2 = (gz - 1 + 1) / 2; 2 * cz2 <= gz + 1 && cz2 < cz; ++cz2) {
+      const double wz = pw1(gz, cz2, fz);
+      if (wz == 0.0) continue;
+      for (int cy2 = (gy - 1 + 1) / 2; 2 * cy2 <= gy + 1 && cy2 < cy; ++cy2) {
+        const double wy = pw1(gy, cy2, fy);
+        if (wy == 0.0) continue;
+        for (int cx2 = (gx - 1 + 1) / 2; 2 * cx2 <= gx + 1 && cx2 < cx; ++cx2) {
+          const double wx = pw1(gx, cx2, fx);
+          if (wx == 0.0) continue;
+          const T w = static_cast<T>(wx * wy * wz);
+          const int64_t I = ((int64_t)cz2 * cy + cy2) * cx + cx2;
+          s0 += w * xc[3 * I];
+          s1 += w * xc[3 * I + 1];
+          s2 += w * xc[3 * I + 2];
+        }
+      }
+    }
+    xf[3 * f] += s0;
+    xf[3 * f + 1] += s1;
+    xf[3 * f + 2] += s2;
+  }
+}
+
+__global__ void k_to_dense(int nx, int ny, int nz, const double *__restrict__ S,
+                           double *__restrict__ A) {
+  const int64_t nn = (int64_t)nx * ny * nz, n3 = 3 * nn;
+  const int64_t total = nn * 27 * 9;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int q = (int)(t / nn);
+    const int64_t n = t - (int64_t)q * nn;
+    const int nb = q / 9, rs = q % 9, r = rs / 3, s = rs % 3;
+    const int i = n % nx, j = (n / nx) % ny, k = n / ((int64_t)nx * ny);
+    const int mi = i + nb % 3 - 1, mj = j + (nb / 3) % 3 - 1, mk = k + nb / 9 - 1;
+    if (mi < 0 || mi >= nx || mj < 0 || mj >= ny || mk < 0 || mk >= nz) continue;
+    const int64_t m = ((int64_t)mk * ny + mj) * nx + mi;
+    A[(3 * n + r) * n3 + 3 * m + s] = S[t];
+  }
+}
+
+// x = Ainv b, one warp per row, FP64 accumulation
+template <typename T>
+__global__ void k_coarse_gemv(int64_t n, const double *__restrict__ A,
+                              const T *__restrict__ b, T *__restrict__ x) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t row = warp; row < n; row += nwarps) {
+    const double *a = A + row * n;
+    double s = 0;
+    for (int64_t k = lane; k < n; k += 32) s += a[k] * static_cast<double>(b[k]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) x[row] = static_cast<T>(s);
+  }
+}
+
+// Chebyshev start: r = D^-1 (b or the residual already in r), d = r/theta,
+// x (+)= d
+template <typename T>
+__global__ void k_cheb_init(int64_t n, const T *__restrict__ dinv,
+                            const T *__restrict__ b, T *__restrict__ r,
+                            T *__restrict__ d, T *__restrict__ x, T inv_theta,
+                            bool zero_guess) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const T ri = dinv[i] * (zero_guess ? b[i] : r[i]);
+    const T di = ri * inv_theta;
+    r[i] = ri;
+    d[i] = di;
+    x[i] = zero_guess ? di : x[i] + di;
+  }
+}
+
+// r -= D^-1 A d ; d = c1 d + c2 r ; x += d
+template <typename T>
+__global__ void k_cheb_step(int64_t n, const T *__restrict__ dinv,
+                            const T *__restrict__ Ad, T *__restrict__ r,
+                            T *__restrict__ d, T *__restrict__ x, T c1, T c2) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const T ri = r[i] - dinv[i] * Ad[i];
+    const T di = c1 * d[i] + c2 * ri;
+    r[i] = ri;
+    d[i] = di;
+    x[i] += di;
+  }
+}
+
+}  // namespace
+
+template <typename T>
+void launch_apply_stencil(const Level &v, const T *S, const T *u, const T *b,
+                          T *y, cudaStream_t s) {
+  count_launch();
+  const int g = grid_for(v.nn, 128);
+  if (b)
+    k_apply_stencil<T, true><<<g, 128, 0, s>>>(v.dims[0], v.dims[1], v.dims[2],
+                                               S, u, b, y);
+  else
+    k_apply_stencil<T, false><<<g, 128, 0, s>>>(v.dims[0], v.dims[1], v.dims[2],
+                                                S, u, b, y);
+}
+template void launch_apply_stencil<double>(const Level &, const double *,
+                                           const double *, const double *,
+                                           double *, cudaStream_t);
+template void launch_apply_stencil<float>(const Level &, const float *,
+                                          const float *, const float *, float *,
+                                          cudaStream_t);
+
+void launch_galerkin(const Level &fine, const double *Sf, const Level &coarse,
+                     double *Sc, cudaStream_t s) {
+  count_launch();
+  k_galerkin<<<grid_for(coarse.nn * 27, 128, 1 << 20), 128, 0, s>>>(
+      fine.dims[0], fine.dims[1], fine.dims[2], coarse.dims[0], coarse.dims[1],
+      coarse.dims[2], Sf, Sc);
+}
+
+void launch_stencil_diag(const Level &v, const double *S, double *dinv64,
+                         float *dinv32, cudaStream_t s) {
+  count_launch();
+  k_stencil_diag<<<grid_for(v.nn, 256), 256, 0, s>>>(v.nn, S, dinv64, dinv32);
+}
+
+template <typename T>
+void launch_restrict(const Level &fine, const Level &coarse, const T *rf,
+                     T *bc, cudaStream_t s) {
+  count_launch();
+  k_restrict<T><<<grid_for(coarse.nn, 128), 128, 0, s>>>(
+      fine.dims[0], fine.dims[1], fine.dims[2], coarse.dims[0], coarse.dims[1],
+      coarse.dims[2], rf, bc);
+}
+template void launch_restrict<double>(const Level &, const Level &,
+                                      const double *, double *, cudaStream_t);
+template void launch_restrict<float>(const Level &, const Level &,
+                                     const float *, float *, cudaStream_t);
+
+template <typename T>
+void launch_prolong_add(const Level &fine, const Level &coarse, const T *xc,
+                        T *xf, cudaStream_t s) {
+  count_launch();
+  k_prolong_add<T><<<grid_for(fine.nn, 128), 128, 0, s>>>(
+      fine.dims[0], fine.dims[1], fine.dims[2], coarse.dims[0], coarse.dims[1],
+      coarse.dims[2], xc, xf);
+}
+template void launch_prolong_add<double>(const Level &, const Level &,
+                                         const double *, double *,
+                                         cudaStream_t);
+template void launch_prolong_add<float>(const Level &, const Level &,
+                                        const float *, float *, cudaStream_t);
+
+void launch_to_dense(const Level &v, const double *S, double *A,
+                     cudaStream_t s) {
+  count_launch();
+  const int64_t n3 = 3 * v.nn;
+  cudaMemsetAsync(A, 0, sizeof(double) * n3 * n3, s);
+  k_to_dense<<<grid_for(v.nn * 243, 256), 256, 0, s>>>(v.dims[0], v.dims[1],
+                                                       v.dims[2], S, A);
+}
+
+namespace {
+__global__ void k_eye(int64_t n, double *A) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * n;
+       t += (int64_t)gridDim.x * blockDim.x)
+    A[t] = (t / n == t % n) ? 1.0 : 0.0;
+}
+}  // namespace
+
+void launch_eye(int64_t n, double *A, cudaStream_t s) {
+  count_launch();
+  k_eye<<<grid_for(n * n, 256), 256, 0, s>>>(n, A);
+}
+
+template <typename T>
+void launch_coarse_gemv(int64_t n, const double *Ainv, const T *b, T *x,
+                        cudaStream_t s) {
+  count_launch();
+  const int64_t warps = n;
+  const int threads = 256;
+  int64_t blocks = (warps * 32 + threads - 1) / threads;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  k_coarse_gemv<T><<<(int)blocks, threads, 0, s>>>(n, Ainv, b, x);
+}
+template void launch_coarse_gemv<double>(int64_t, const double *,
+                                         const double *, double *,
+                                         cudaStream_t);
+template void launch_coarse_gemv<float>(int64_t, const double *, const float *,
+                                        float *, cudaStream_t);
+
+template <typename T>
+void launch_cheb_init(int64_t n, const T *dinv, const T *b, T *r, T *d, T *x,
+                      double inv_theta, bool zero_guess, cudaStream_t s) {
+  count_launch();
+  k_cheb_init<T><<<grid_for(n, 256), 256, 0, s>>>(
+      n, dinv, b, r, d, x, static_cast<T>(inv_theta), zero_guess);
+}
+template void launch_cheb_init<double>(int64_t, const double *, const double *,
+                                       double *, double *, double *, double,
+                                       bool, cudaStream_t);
+template void launch_cheb_init<float>(int64_t, const float *, const float *,
+                                      float *, float *, float *, double, bool,
+                                      cudaStream_t);
+
+template <typename T>
+void launch_cheb_step(int64_t n, const T *dinv, const T *Ad, T *r, T *d, T *x,
+                      double c1, double c2, cudaStream_t s) {
+  count_launch();
+  k_cheb_step<T><<<grid_for(n, 256), 256, 0, s>>>(
+      n, dinv, Ad, r, d, x, static_cast<T>(c1), static_cast<T>(c2));
+}
+template void launch_cheb_step<double>(int64_t, const double *, const double *,
+                                       double *, double *, double *, double,
+                                       double, cudaStream_t);
+template void launch_cheb_step<float>(int64_t, const float *, const float *,
+                                      float *, float *, float *, double, double,
+                                      cudaStream_t);
+
+}  // namespace tpo

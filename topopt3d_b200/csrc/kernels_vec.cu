@@ -1,0 +1,259 @@
+// Vector kernels of the Krylov solvers.  Every reduction accumulates in FP64
+// and is deterministic: a fixed grid of kRedBlocks blocks writes one partial
+// each in a fixed order, and the last block to finish (ticket counter) sums
+// the partials in a fixed tree order and writes the result to a device
+// scalar, so the CG recurrences never round-trip through the host.
+#include "tpo_internal.h"
+
+namespace tpo {
+
+namespace {
+
+constexpr int kRedThreads = 256;
+
+int grid_for(int64_t n, int threads) {
+  int64_t g = (n + threads - 1) / threads;
+  if (g > 148 * 32) g = 148 * 32;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  v = 0;
+  if (threadIdx.x < 32) {
+    v = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  }
+  __syncthreads();
+  return v;   // valid in thread 0
+}
+
+// partial -> last block -> *out (previous *out moved to *shift_to if set)
+__device__ __forceinline__ void finish_reduction(double v, double *part,
+                                                 unsigned int *ticket,
+                                                 double *out, double *shift_to) {
+  __shared__ double sh[32];
+  __shared__ bool last;
+  v = block_sum(v, sh);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = v;
+    __threadfence();
+    last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double s = 0;
+  for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x)
+    s += ((volatile double *)part)[i];
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) {
+    if (shift_to) *shift_to = *out;
+    *out = s;
+    *ticket = 0u;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads)
+    k_dot(int64_t n, const T *__restrict__ a, const T *__restrict__ b,
+          double *part, unsigned int *ticket, double *out, double *shift_to) {
+  double s = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    s += static_cast<double>(a[i]) * static_cast<double>(b[i]);
+  finish_reduction(s, part, ticket, out, shift_to);
+}
+
+// p = z (first) or p = z + (rho / rho_old) p
+template <typename T>
+__global__ void k_cg_p(int64_t n, const T *__restrict__ z, T *__restrict__ p,
+                       const double *__restrict__ scal, bool first) {
+  const T beta = first ? T(0) : static_cast<T>(scal[0] / scal[1]);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = first ? z[i] : z[i] + beta * p[i];
+}
+
+// x += alpha p ; r -= alpha q ; rr = r.r   with alpha = rho / (p.q)
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads)
+    k_cg_update(int64_t n, T *__restrict__ x, T *__restrict__ r,
+                const T *__restrict__ p, const T *__restrict__ q,
+                const double *__restrict__ scal, double *part,
+                unsigned int *ticket, double *rr) {
+  const double alpha_d = scal[0] / scal[2];
+  const T alpha = static_cast<T>(alpha_d);
+  double s = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    x[i] += alpha * p[i];
+    const T ri = r[i] - alpha * q[i];
+    r[i] = ri;
+    s += static_cast<double>(ri) * static_cast<double>(ri);
+  }
+  finish_reduction(s, part, ticket, rr, nullptr);
+}
+
+__device__ __forceinline__ double start_value(uint64_t i) {
+  // splitmix64 of the dof index mapped to [-1, 1)
+  uint64_t z = i + 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z = z ^ (z >> 31);
+  return (double)(z >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+}
+
+__global__ void k_power_start(int64_t n, double *a) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = start_value((uint64_t)i);
+}
+
+// a = w / sqrt(nrm2)   (w may alias a)
+__global__ void k_power_normalize(int64_t n, double *a, const double *w,
+                                  const double *nrm2) {
+  const double s = sqrt(*nrm2);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = w[i] / s;
+}
+
+__global__ void k_scale_diag(int64_t n, double *w, const double *dinv) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    w[i] *= dinv[i];
+}
+
+// b = float(a / sqrt(*nrm2))
+__global__ void k_to_f32_scaled(int64_t n, const double *a, const double *nrm2,
+                                float *b) {
+  const double s = 1.0 / sqrt(*nrm2);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = static_cast<float>(a[i] * s);
+}
+
+// U += sqrt(*nrm2) * double(d)
+__global__ void k_axpy_f32(int64_t n, double *U, const float *d,
+                           const double *nrm2) {
+  const double s = sqrt(*nrm2);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    U[i] += s * static_cast<double>(d[i]);
+}
+
+__global__ void k_d2f(int64_t n, const double *a, float *b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = static_cast<float>(a[i]);
+}
+
+__global__ void k_f2d(int64_t n, const float *a, double *b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = static_cast<double>(a[i]);
+}
+
+__global__ void k_fill(int64_t n, double *a, double v) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = v;
+}
+
+}  // namespace
+
+template <typename T>
+void launch_dot(const Ctx &c, int64_t n, const T *a, const T *b, double *out,
+                double *shift_to, cudaStream_t s) {
+  count_launch();
+  k_dot<T><<<kRedBlocks, kRedThreads, 0, s>>>(n, a, b, c.part, c.ticket, out,
+                                               shift_to);
+}
+template void launch_dot<double>(const Ctx &, int64_t, const double *,
+                                 const double *, double *, double *,
+                                 cudaStream_t);
+template void launch_dot<float>(const Ctx &, int64_t, const float *,
+                                const float *, double *, double *,
+                                cudaStream_t);
+
+template <typename T>
+void launch_cg_p(int64_t n, const T *z, T *p, const double *scal, bool first,
+                 cudaStream_t s) {
+  count_launch();
+  k_cg_p<T><<<grid_for(n, 256), 256, 0, s>>>(n, z, p, scal, first);
+}
+template void launch_cg_p<double>(int64_t, const double *, double *,
+                                  const double *, bool, cudaStream_t);
+template void launch_cg_p<float>(int64_t, const float *, float *,
+                                 const double *, bool, cudaStream_t);
+
+template <typename T>
+void launch_cg_update(const Ctx &c, int64_t n, T *x, T *r, const T *p,
+                      const T *q, const double *scal, double *rr,
+                      cudaStream_t s) {
+  count_launch();
+  k_cg_update<T><<<kRedBlocks, kRedThreads, 0, s>>>(n, x, r, p, q, scal, c.part,
+                                                     c.ticket, rr);
+}
+template void launch_cg_update<double>(const Ctx &, int64_t, double *,
+                                       double *, const double *,
+                                       const double *, const double *,
+                                       double *, cudaStream_t);
+template void launch_cg_update<float>(const Ctx &, int64_t, float *, float *,
+                                      const float *, const float *,
+                                      const double *, double *, cudaStream_t);
+
+void launch_power_start(int64_t n, double *a, cudaStream_t s) {
+  count_launch();
+  k_power_start<<<grid_for(n, 256), 256, 0, s>>>(n, a);
+}
+
+void launch_power_normalize(int64_t n, double *a, const double *w,
+                            const double *dinv, const double *nrm2,
+                            cudaStream_t s) {
+  count_launch();
+  (void)dinv;
+  k_power_normalize<<<grid_for(n, 256), 256, 0, s>>>(n, a, w, nrm2);
+}
+
+void launch_scale_diag(int64_t n, double *w, const double *dinv,
+                       cudaStream_t s) {
+  count_launch();
+  k_scale_diag<<<grid_for(n, 256), 256, 0, s>>>(n, w, dinv);
+}
+
+void launch_to_f32_scaled(int64_t n, const double *a, const double *scal,
+                          float *b, cudaStream_t s) {
+  count_launch();
+  k_to_f32_scaled<<<grid_for(n, 256), 256, 0, s>>>(n, a, scal, b);
+}
+
+void launch_axpy_f32(int64_t n, double *U, const float *d, const double *scal,
+                     cudaStream_t s) {
+  count_launch();
+  k_axpy_f32<<<grid_for(n, 256), 256, 0, s>>>(n, U, d, scal);
+}
+
+void launch_d2f(int64_t n, const double *a, float *b, cudaStream_t s) {
+  count_launch();
+  k_d2f<<<grid_for(n, 256), 256, 0, s>>>(n, a, b);
+}
+
+void launch_f2d(int64_t n, const float *a, double *b, cudaStream_t s) {
+  count_launch();
+  k_f2d<<<grid_for(n, 256), 256, 0, s>>>(n, a, b);
+}
+
+void launch_fill(int64_t n, double *a, double v, cudaStream_t s) {
+  count_launch();
+  k_fill<<<grid_for(n, 256), 256, 0, s>>>(n, a, v);
+}
+
+}  // namespace tpo

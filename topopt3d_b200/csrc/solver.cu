@@ -1,0 +1,397 @@
+// Host orchestration of the FE solve: GMG set-up (PCSetUp), the V-cycle,
+// FP64 PCG and the mixed FP32/FP64 defect-correction solve.
+//
+// Reference behaviour restated here (FEAnalysis.cpp:387-416, :541-573,
+// :673): KSP CG, nonzero initial guess, convergence on the unpreconditioned
+// residual ||b - K u|| <= rtol ||b||, PCMG with Galerkin coarse operators,
+// Chebyshev/Jacobi smoothing and a direct (here Cholesky) coarse solve.
+#include <cusolverDn.h>
+
+#include <chrono>
+#include <cmath>
+
+#include "solver.h"
+
+namespace tpo {
+
+namespace {
+
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(
+             std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+struct Cheb {
+  double inv_theta, sigma, delta, rho0;
+};
+
+Cheb cheb_of(double lam, const tpo_solve_opts &o) {
+  const double a = o.cheb_lo * lam, b = o.cheb_hi * lam;
+  const double theta = 0.5 * (b + a), delta = 0.5 * (b - a);
+  const double sigma = theta / delta;
+  return {1.0 / theta, sigma, delta, 1.0 / sigma};
+}
+
+template <typename T>
+struct LV {
+  T *b, *x, *r, *d, *a;
+  const T *S, *dinv;
+};
+
+LV<double> lv(Level &v, double *) {
+  return {v.b64, v.x64, v.r64, v.d64, v.a64, v.S64, v.dinv64};
+}
+LV<float> lv(Level &v, float *) {
+  return {v.b32, v.x32, v.r32, v.d32, v.a32, v.S32, v.dinv32};
+}
+
+const double *fineE(const Ctx &c, double *) { return c.E64; }
+const float *fineE(const Ctx &c, float *) { return c.E32; }
+
+template <typename T>
+void level_apply(Ctx &c, int l, const T *u, const T *b, T *y, cudaStream_t s) {
+  if (l == 0)
+    launch_apply_fine<T>(c, fineE(c, (T *)nullptr), u, b, y, s);
+  else
+    launch_apply_stencil<T>(c.lev[l], lv(c.lev[l], (T *)nullptr).S, u, b, y, s);
+}
+
+template <typename T>
+void vcycle_rec(Ctx &c, int l, const T *b, T *x, const tpo_solve_opts &o,
+                cudaStream_t s) {
+  if (l == c.L - 1) {
+    launch_coarse_gemv<T>(c.nc, c.Ainv, b, x, s);
+    return;
+  }
+  Level &v = c.lev[l];
+  LV<T> w = lv(v, (T *)nullptr);
+  const int64_t n = 3 * v.nn;
+  const Cheb ch = cheb_of(v.lam, o);
+  // pre-smoothing from a zero guess
+  launch_cheb_init<T>(n, w.dinv, b, w.r, w.d, x, ch.inv_theta, true, s);
+  double rho = ch.rho0;
+  for (int k = 1; k < o.cheb_degree; ++k) {
+    level_apply<T>(c, l, w.d, nullptr, w.a, s);
+    const double rn = 1.0 / (2.0 * ch.sigma - rho);
+    launch_cheb_step<T>(n, w.dinv, w.a, w.r, w.d, x, rn * rho, 2.0 * rn / ch.delta, s);
+    rho = rn;
+  }
+  // residual, restriction, coarse correction, prolongation
+  level_apply<T>(c, l, x, b, w.a, s);
+  Level &cv = c.lev[l + 1];
+  LV<T> cw = lv(cv, (T *)nullptr);
+  launch_restrict<T>(v, cv, w.a, cw.b, s);
+  vcycle_rec<T>(c, l + 1, cw.b, cw.x, o, s);
+  launch_prolong_add<T>(v, cv, cw.x, x, s);
+  // post-smoothing from the corrected x
+  level_apply<T>(c, l, x, b, w.r, s);
+  launch_cheb_init<T>(n, w.dinv, b, w.r, w.d, x, ch.inv_theta, false, s);
+  rho = ch.rho0;
+  for (int k = 1; k < o.cheb_degree; ++k) {
+    level_apply<T>(c, l, w.d, nullptr, w.a, s);
+    const double rn = 1.0 / (2.0 * ch.sigma - rho);
+    launch_cheb_step<T>(n, w.dinv, w.a, w.r, w.d, x, rn * rho, 2.0 * rn / ch.delta, s);
+    rho = rn;
+  }
+}
+
+// one CG iteration after the first (p = z + beta p): V-cycle, rho, p, q,
+// pq, update.  Kept free of host synchronisation so it can be captured.
+template <typename T>
+void cg_body(Ctx &c, int64_t n, T *x, T *r, T *z, T *p, T *q,
+             const tpo_solve_opts &o, bool first, cudaStream_t s) {
+  double *sc = c.scal;
+  vcycle_rec<T>(c, 0, r, z, o, s);
+  launch_dot<T>(c, n, r, z, sc + 0, sc + 1, s);
+  launch_cg_p<T>(n, z, p, sc, first, s);
+  launch_apply_fine<T>(c, fineE(c, (T *)nullptr), p, nullptr, q, s);
+  launch_dot<T>(c, n, p, q, sc + 2, nullptr, s);
+  launch_cg_update<T>(c, n, x, r, p, q, sc, sc + 3, s);
+}
+
+#define CK(call)                                                       \
+  do {                                                                 \
+    cudaError_t e_ = (call);                                           \
+    if (e_ != cudaSuccess) {                                           \
+      c.err = std::string(#call) + ": " + cudaGetErrorString(e_);      \
+      return TPO_E_CUDA;                                               \
+    }                                                                  \
+  } while (0)
+
+int readback(Ctx &c, int count) {
+  CK(cudaMemcpyAsync(c.scal_h, c.scal, sizeof(double) * count,
+                     cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  return TPO_OK;
+}
+
+// PCG on the fine operator in precision T.  x holds the initial guess and
+// r must already hold b - K x; ||r||^2 is in scal[3] on the host mirror.
+// target_rr is the squared residual norm at which to stop.
+template <typename T>
+int pcg_loop(Ctx &c, const tpo_solve_opts &o, T *x, T *r, T *z, T *p, T *q,
+             double target_rr, int maxit, int *its) {
+  cudaStream_t s = c.stream;
+  const int64_t n = 3 * c.nn;
+  cudaGraphExec_t &g = (sizeof(T) == 8) ? c.graph64 : c.graph32;
+  const void *&gx = (sizeof(T) == 8) ? c.graph64_x : c.graph32_x;
+  long long &gnodes = (sizeof(T) == 8) ? c.graph64_nodes : c.graph32_nodes;
+  int k = 0;
+  int status = TPO_NOT_CONVERGED;
+  if (c.scal_h[3] <= target_rr) {
+    *its = 0;
+    return TPO_OK;
+  }
+  while (k < maxit) {
+    const bool first = (k == 0);
+    if (!first && o.use_graph) {
+      if (!g || gx != (const void *)x) {
+        if (g) {
+          cudaGraphExecDestroy(g);
+          g = nullptr;
+        }
+        cudaGraph_t graph;
+        const long long before = g_launches.load();
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        cg_body<T>(c, n, x, r, z, p, q, o, false, s);
+        CK(cudaStreamEndCapture(s, &graph));
+        // captured launches run when the graph is launched, not now
+        gnodes = g_launches.load() - before;
+        count_launch(-gnodes);
+        CK(cudaGraphInstantiate(&g, graph, 0));
+        CK(cudaGraphDestroy(graph));
+        gx = x;
+      }
+      CK(cudaGraphLaunch(g, s));
+      count_launch(gnodes);
+    } else {
+      cg_body<T>(c, n, x, r, z, p, q, o, first, s);
+    }
+    CK(cudaGetLastError());
+    ++k;
+    if (int rc = readback(c, 4)) return rc;
+    const double rho = c.scal_h[0], pq = c.scal_h[2], rr = c.scal_h[3];
+    if (!(rho > 0) || !(pq > 0) || !std::isfinite(rr)) {
+      status = TPO_E_BREAKDOWN;
+      c.err = "CG breakdown (indefinite preconditioner/operator or non-finite residual)";
+      break;
+    }
+    if (rr <= target_rr) {
+      status = TPO_OK;
+      break;
+    }
+  }
+  *its = k;
+  return status;
+}
+
+}  // namespace
+
+void invalidate_graphs(Ctx &c) {
+  if (c.graph64) cudaGraphExecDestroy(c.graph64);
+  if (c.graph32) cudaGraphExecDestroy(c.graph32);
+  c.graph64 = c.graph32 = nullptr;
+  c.graph64_x = c.graph32_x = nullptr;
+}
+
+int estimate_lambda(Ctx &c, int l, int its, double *lam) {
+  Level &v = c.lev[l];
+  const int64_t n = 3 * v.nn;
+  cudaStream_t s = c.stream;
+  double *a = v.d64, *w = v.a64;
+  launch_power_start(n, a, s);
+  launch_dot<double>(c, n, a, a, c.scal + 6, nullptr, s);
+  launch_power_normalize(n, a, a, nullptr, c.scal + 6, s);
+  for (int k = 0; k < its; ++k) {
+    level_apply<double>(c, l, a, nullptr, w, s);
+    launch_scale_diag(n, w, v.dinv64, s);
+    launch_dot<double>(c, n, w, w, c.scal + 6, nullptr, s);
+    launch_power_normalize(n, a, w, nullptr, c.scal + 6, s);
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(c.scal_h + 6, c.scal + 6, sizeof(double),
+                     cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  *lam = std::sqrt(c.scal_h[6]);
+  return TPO_OK;
+}
+
+int setup_hierarchy(Ctx &c, const tpo_solve_opts &o) {
+  const double t0 = now_ms();
+  cudaStream_t s = c.stream;
+  invalidate_graphs(c);
+  // fine level: Jacobi diagonal and the assembled stencil for Galerkin
+  launch_fine_diag(c, c.lev[0].dinv64, c.lev[0].dinv32, s);
+  if (c.L > 1 || true) launch_fine_stencil(c, c.S0, s);
+  for (int l = 0; l + 1 < c.L; ++l) {
+    const double *Sf = (l == 0) ? c.S0 : c.lev[l].S64;
+    launch_galerkin(c.lev[l], Sf, c.lev[l + 1], c.lev[l + 1].S64, s);
+    launch_stencil_diag(c.lev[l + 1], c.lev[l + 1].S64, c.lev[l + 1].dinv64,
+                        c.lev[l + 1].dinv32, s);
+    if (l + 1 < c.L - 1)
+      launch_d2f(243 * c.lev[l + 1].nn, c.lev[l + 1].S64, c.lev[l + 1].S32, s);
+  }
+  CK(cudaGetLastError());
+  // coarsest level: dense Cholesky, then the explicit inverse for a
+  // bandwidth-parallel GEMV inside the V-cycle
+  Level &cl = c.lev[c.L - 1];
+  const double *Sc = (c.L == 1) ? c.S0 : cl.S64;
+  const int64_t nc = 3 * cl.nn;
+  c.nc = nc;
+  launch_to_dense(cl, Sc, c.Adense, s);
+  launch_eye(nc, c.Ainv, s);
+  CK(cudaGetLastError());
+  cusolverDnHandle_t h = static_cast<cusolverDnHandle_t>(c.cusolver);
+  if (!h) {
+    if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) {
+      c.err = "cusolverDnCreate failed";
+      return TPO_E_CUDA;
+    }
+    c.cusolver = h;
+  }
+  cusolverDnSetStream(h, s);
+  int lwork = 0;
+  if (cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, (int)nc, c.Adense,
+                                  (int)nc, &lwork) != CUSOLVER_STATUS_SUCCESS) {
+    c.err = "cusolverDnDpotrf_bufferSize failed";
+    return TPO_E_CUDA;
+  }
+  if ((size_t)lwork > c.solver_work_n) {
+    if (c.solver_work) cudaFree(c.solver_work);
+    c.solver_work = nullptr;
+    CK(cudaMalloc(&c.solver_work, sizeof(double) * (size_t)lwork));
+    c.solver_work_n = lwork;
+  }
+  if (cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, (int)nc, c.Adense, (int)nc,
+                       c.solver_work, lwork, c.dev_info) != CUSOLVER_STATUS_SUCCESS ||
+      cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, (int)nc, (int)nc, c.Adense,
+                       (int)nc, c.Ainv, (int)nc, c.dev_info) != CUSOLVER_STATUS_SUCCESS) {
+    c.err = "coarse Cholesky factorisation failed";
+    return TPO_E_CUDA;
+  }
+  int info_h = 0;
+  CK(cudaMemcpyAsync(&info_h, c.dev_info, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (info_h != 0) {
+    c.err = "coarsest operator is not positive definite (potrf info " +
+            std::to_string(info_h) + ")";
+    return TPO_E_BREAKDOWN;
+  }
+  // Chebyshev bounds
+  for (int l = 0; l + 1 < c.L; ++l) {
+    double lam = 0;
+    if (int rc = estimate_lambda(c, l, o.power_its, &lam)) return rc;
+    c.lev[l].lam = lam;
+  }
+  c.setup_opts = o;
+  c.assembled = true;
+  c.setup_ms = now_ms() - t0;
+  return TPO_OK;
+}
+
+int vcycle_apply(Ctx &c, const tpo_solve_opts &o, int precision,
+                 const double *r, double *z) {
+  cudaStream_t s = c.stream;
+  const int64_t n = 3 * c.nn;
+  if (precision == TPO_PREC_FP64) {
+    vcycle_rec<double>(c, 0, r, z, o, s);
+  } else {
+    launch_d2f(n, r, c.r32, s);
+    vcycle_rec<float>(c, 0, c.r32, c.z32, o, s);
+    launch_f2d(n, c.z32, z, s);
+  }
+  CK(cudaGetLastError());
+  return TPO_OK;
+}
+
+// Solve K x = b; x holds the initial guess (device pointers, 3*nn each).
+int solve(Ctx &c, const tpo_solve_opts &o, const double *b, double *x,
+          tpo_solve_info *info) {
+  const double t0 = now_ms();
+  cudaStream_t s = c.stream;
+  const int64_t n = 3 * c.nn;
+  double *sc = c.scal;
+  int its_total = 0, outer = 0, status = TPO_NOT_CONVERGED;
+  double bn = 0, rn = 0;
+
+  launch_dot<double>(c, n, b, b, sc + 4, nullptr, s);
+  launch_apply_fine<double>(c, c.E64, x, b, c.r64, s);
+  launch_dot<double>(c, n, c.r64, c.r64, sc + 5, nullptr, s);
+  CK(cudaGetLastError());
+  if (int rc = readback(c, 6)) return rc;
+  bn = std::sqrt(c.scal_h[4]);
+  rn = std::sqrt(c.scal_h[5]);
+  const double target = o.rtol * bn;
+  if (bn == 0.0) {
+    CK(cudaMemsetAsync(x, 0, sizeof(double) * n, s));
+    status = TPO_OK;
+    rn = 0;
+  } else if (rn <= target) {
+    status = TPO_OK;
+  } else if (o.precision == TPO_PREC_FP64) {
+    // r = b - K x already in r64 and ||r||^2 in scal[5]
+    c.scal_h[3] = c.scal_h[5];
+    CK(cudaMemcpyAsync(sc + 3, sc + 5, sizeof(double), cudaMemcpyDeviceToDevice, s));
+    int its = 0;
+    status = pcg_loop<double>(c, o, x, c.r64, c.z64, c.p64, c.q64,
+                              target * target, o.maxit, &its);
+    its_total = its;
+    outer = 1;
+    // report the true residual
+    launch_apply_fine<double>(c, c.E64, x, b, c.r64, s);
+    launch_dot<double>(c, n, c.r64, c.r64, sc + 5, nullptr, s);
+    if (int rc = readback(c, 6)) return rc;
+    rn = std::sqrt(c.scal_h[5]);
+  } else {
+    // mixed: FP32 PCG+GMG on K d = r/||r|| inside FP64 defect correction
+    while (outer < o.max_outer) {
+      if (rn <= target) {
+        status = TPO_OK;
+        break;
+      }
+      if (its_total >= o.maxit) break;
+      launch_to_f32_scaled(n, c.r64, sc + 5, c.r32, s);
+      CK(cudaMemsetAsync(c.x32, 0, sizeof(float) * n, s));
+      launch_dot<float>(c, n, c.r32, c.r32, sc + 3, nullptr, s);
+      if (int rc = readback(c, 4)) return rc;
+      const double tgt = o.inner_rtol * o.inner_rtol * c.scal_h[3];
+      int its = 0;
+      const int st = pcg_loop<float>(c, o, c.x32, c.r32, c.z32, c.p32, c.q32,
+                                     tgt, o.maxit - its_total, &its);
+      its_total += its;
+      ++outer;
+      launch_axpy_f32(n, x, c.x32, sc + 5, s);
+      launch_apply_fine<double>(c, c.E64, x, b, c.r64, s);
+      launch_dot<double>(c, n, c.r64, c.r64, sc + 5, nullptr, s);
+      if (int rc = readback(c, 6)) return rc;
+      const double rn_new = std::sqrt(c.scal_h[5]);
+      if (st == TPO_E_BREAKDOWN && !(rn_new < rn)) {
+        status = TPO_E_BREAKDOWN;
+        rn = rn_new;
+        break;
+      }
+      rn = rn_new;
+      if (!std::isfinite(rn)) {
+        status = TPO_E_BREAKDOWN;
+        c.err = "non-finite residual in defect correction";
+        break;
+      }
+    }
+    if (rn <= target) status = TPO_OK;
+  }
+  CK(cudaGetLastError());
+  if (info) {
+    info->status = status;
+    info->iterations = its_total;
+    info->outer = outer;
+    info->relres = bn > 0 ? rn / bn : 0.0;
+    info->solve_ms = now_ms() - t0;
+    info->setup_ms = c.setup_ms;
+  }
+  if (status == TPO_NOT_CONVERGED && c.err.empty())
+    c.err = "solver reached its iteration limit";
+  return status;
+}
+
+}  // namespace tpo

@@ -1,0 +1,16 @@
+// Host-side solver entry points shared by the C ABI layer.
+#pragma once
+
+#include "tpo_internal.h"
+
+namespace tpo {
+
+void invalidate_graphs(Ctx &c);
+int estimate_lambda(Ctx &c, int level, int its, double *lam);
+int setup_hierarchy(Ctx &c, const tpo_solve_opts &o);
+int vcycle_apply(Ctx &c, const tpo_solve_opts &o, int precision,
+                 const double *r, double *z);
+int solve(Ctx &c, const tpo_solve_opts &o, const double *b, double *x,
+          tpo_solve_info *info);
+
+}  // namespace tpo

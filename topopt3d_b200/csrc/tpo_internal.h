@@ -1,0 +1,241 @@
+// Internal declarations of the B200 TopOpt3D FE library: the context, the
+// per-level state and the kernel launchers.  Nothing here is part of the
+// C ABI (include/topopt_b200.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/topopt_b200.h"
+
+namespace tpo {
+
+// ---------------------------------------------------------------------------
+// The element stiffness in the 2x2x2 Hadamard (modal) basis.
+//
+// Nodal values of one element in lexicographic corner order l = bx+2by+4bz
+// are transformed per component by the unnormalised butterfly
+//   uh[q] = sum_l s(l,q) u[l],  s(l,q) = prod_{d in q} (bit d of l ? +1 : -1)
+// (q = mode bitmask over x,y,z).  With Kh = T K0 T^T / 64 the element matvec
+// is y = T^T Kh T u.  Kh couples only these blocks of (mode q, component c)
+// pairs (true for any box element and isotropic D); the 45 constants are
+// stored block by block, row-major:
+//   0: 3x3 {(1,0),(2,1),(4,2)}   normal strains
+//   1: 2x2 {(1,1),(2,0)}         shear xy
+//   2: 2x2 {(1,2),(4,0)}         shear xz
+//   3: 2x2 {(2,2),(4,1)}         shear yz
+//   4: 2x2 {(3,0),(6,2)}         bilinear modes
+//   5: 2x2 {(3,1),(5,2)}
+//   6: 2x2 {(6,1),(5,0)}
+//   7: 3x3 {(3,2),(6,0),(5,1)}
+//   8: 3 x 1x1 {(7,0)},{(7,1)},{(7,2)}
+// ---------------------------------------------------------------------------
+constexpr int kNumKh = 45;
+
+template <typename T>
+struct Kh {
+  T v[kNumKh];
+};
+
+// diagonal of K0 in lexicographic corner order (24 values) for the Jacobi
+// diagonal of the fine operator
+template <typename T>
+struct K0Diag {
+  T v[24];
+};
+
+// density filter template: offsets and raw weights 1 - d/R (Filter.cpp:43-52)
+constexpr int kMaxFilterTaps = 512;
+
+struct FilterTaps {
+  int n;
+  int8_t off[kMaxFilterTaps][3];
+  double w[kMaxFilterTaps];
+};
+
+struct Level {
+  int dims[3] = {0, 0, 0};
+  int64_t nn = 0;
+  // Galerkin operator as a 27-point 3x3-block stencil, SoA:
+  // S[(nb*9 + 3r + s) * nn + node], nb = (dk+1)*9 + (dj+1)*3 + (di+1)
+  double *S64 = nullptr;
+  float *S32 = nullptr;
+  double *dinv64 = nullptr;
+  float *dinv32 = nullptr;
+  double lam = 0.0;
+  // V-cycle work vectors (3*nn each)
+  double *b64 = nullptr, *x64 = nullptr, *r64 = nullptr, *d64 = nullptr,
+         *a64 = nullptr;
+  float *b32 = nullptr, *x32 = nullptr, *r32 = nullptr, *d32 = nullptr,
+        *a32 = nullptr;
+};
+
+struct Ctx {
+  tpo_mesh_params prm{};
+  int nel[3] = {0, 0, 0};
+  int64_t ne = 0, nn = 0;
+  int L = 0;
+  std::vector<Level> lev;
+  int device = 0;
+  cudaStream_t stream = nullptr;      // stream all work is issued on
+  cudaStream_t own_stream = nullptr;  // the context's own stream
+  std::string err;
+
+  // element constants
+  double K0[576];
+  Kh<double> kh64{};
+  Kh<float> kh32{};
+  K0Diag<double> kd64{};
+
+  // host-side boundary conditions
+  std::vector<uint8_t> fix_h;
+  std::vector<double> F_h;
+  bool initialized = false;
+  bool have_material = false;
+  bool assembled = false;
+  tpo_solve_opts setup_opts{};
+  double setup_ms = 0.0;
+
+  // device state
+  uint8_t *fix = nullptr;   // per-node fixed-component bitmask
+  double *F = nullptr, *U = nullptr;
+  double *x = nullptr, *rho = nullptr, *E64 = nullptr, *dEdz = nullptr;
+  float *E32 = nullptr;
+  double *S0 = nullptr;     // fine-level assembled stencil (setup only)
+  double *K0lex = nullptr;  // K0 in lexicographic corner order (576)
+  double *Ainv = nullptr;   // dense inverse of the coarsest operator
+  int64_t nc = 0;
+
+  // filter
+  FilterTaps taps{};
+  FilterTaps *taps_d = nullptr;
+  double *finv = nullptr;   // 1 / row sum per element
+
+  // solver work (fine level, FP64 and FP32)
+  double *r64 = nullptr, *z64 = nullptr, *p64 = nullptr, *q64 = nullptr,
+         *w64 = nullptr;
+  float *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *q32 = nullptr,
+        *x32 = nullptr;
+  double *scal = nullptr;   // device scalars
+  double *scal_h = nullptr; // pinned host mirror
+  double *part = nullptr;   // reduction partials
+  unsigned int *ticket = nullptr;
+  double *tmpe = nullptr, *tmpe2 = nullptr;   // element-sized scratch
+  double *io_a = nullptr, *io_b = nullptr;    // staging for host buffers
+  double *oc_ws = nullptr;                    // OC update workspace (6 nElem)
+  size_t io_bytes = 0;
+
+  // coarse factorisation
+  void *cusolver = nullptr;
+  double *Adense = nullptr;     // coarsest operator, dense (factorised in place)
+  double *solver_work = nullptr;
+  size_t solver_work_n = 0;
+  int *dev_info = nullptr;
+
+  // CUDA graphs of the CG iteration bodies
+  cudaGraphExec_t graph64 = nullptr, graph32 = nullptr;
+  const void *graph64_x = nullptr, *graph32_x = nullptr;
+  long long graph64_nodes = 0, graph32_nodes = 0;
+};
+
+// --------------------------- kernel launchers ------------------------------
+
+// process-wide count of kernel launches (tpo_kernel_launches)
+extern std::atomic<long long> g_launches;
+inline void count_launch(long long n = 1) {
+  g_launches.fetch_add(n, std::memory_order_relaxed);
+}
+
+constexpr int kRedBlocks = 592;   // 4 x 148 SMs: fixed grid for reductions
+
+// fine matrix-free operator: y = M K M u + (1-M) u, or y = b - (that)
+template <typename T>
+void launch_apply_fine(const Ctx &c, const T *E, const T *u, const T *b, T *y,
+                       cudaStream_t s);
+void launch_fine_diag(const Ctx &c, double *dinv64, float *dinv32,
+                      cudaStream_t s);
+void launch_fine_stencil(const Ctx &c, double *S, cudaStream_t s);
+
+// stencil levels
+template <typename T>
+void launch_apply_stencil(const Level &v, const T *S, const T *u, const T *b,
+                          T *y, cudaStream_t s);
+void launch_galerkin(const Level &fine, const double *Sf, const Level &coarse,
+                     double *Sc, cudaStream_t s);
+void launch_stencil_diag(const Level &v, const double *S, double *dinv64,
+                         float *dinv32, cudaStream_t s);
+template <typename T>
+void launch_restrict(const Level &fine, const Level &coarse, const T *rf,
+                     T *bc, cudaStream_t s);
+template <typename T>
+void launch_prolong_add(const Level &fine, const Level &coarse, const T *xc,
+                        T *xf, cudaStream_t s);
+void launch_to_dense(const Level &v, const double *S, double *A,
+                     cudaStream_t s);
+void launch_eye(int64_t n, double *A, cudaStream_t s);
+template <typename T>
+void launch_coarse_gemv(int64_t n, const double *Ainv, const T *b, T *x,
+                        cudaStream_t s);
+
+// Chebyshev smoother pieces
+template <typename T>
+void launch_cheb_init(int64_t n, const T *dinv, const T *b, T *r, T *d, T *x,
+                      double inv_theta, bool zero_guess, cudaStream_t s);
+template <typename T>
+void launch_cheb_step(int64_t n, const T *dinv, const T *Ad, T *r, T *d, T *x,
+                      double c1, double c2, cudaStream_t s);
+
+// vectors and reductions (FP64 accumulation; results in device scalars)
+template <typename T>
+void launch_dot(const Ctx &c, int64_t n, const T *a, const T *b, double *out,
+                double *shift_to, cudaStream_t s);
+template <typename T>
+void launch_cg_p(int64_t n, const T *z, T *p, const double *scal, bool first,
+                 cudaStream_t s);
+template <typename T>
+void launch_cg_update(const Ctx &c, int64_t n, T *x, T *r, const T *p,
+                      const T *q, const double *scal, double *rr,
+                      cudaStream_t s);
+void launch_power_normalize(int64_t n, double *a, const double *w,
+                            const double *dinv, const double *nrm2,
+                            cudaStream_t s);
+void launch_power_start(int64_t n, double *a, cudaStream_t s);
+void launch_scale_diag(int64_t n, double *w, const double *dinv,
+                       cudaStream_t s);
+void launch_to_f32_scaled(int64_t n, const double *a, const double *scal,
+                          float *b, cudaStream_t s);
+void launch_axpy_f32(int64_t n, double *U, const float *d, const double *scal,
+                     cudaStream_t s);
+void launch_d2f(int64_t n, const double *a, float *b, cudaStream_t s);
+void launch_f2d(int64_t n, const float *a, double *b, cudaStream_t s);
+void launch_fill(int64_t n, double *a, double v, cudaStream_t s);
+
+// design-side kernels
+void launch_filter_rowsum(const Ctx &c, cudaStream_t s);
+void launch_filter(const Ctx &c, const double *in, double *out, bool transpose,
+                   cudaStream_t s);
+// P^T applied to the constant vector `value`
+void launch_filter_adj_uniform(const Ctx &c, double value, double *out,
+                               cudaStream_t s);
+void launch_simp(const Ctx &c, double penal, double eps, cudaStream_t s);
+void launch_sensitivity(const Ctx &c, const double *U, double *dc,
+                        cudaStream_t s);
+void launch_oc_step(const Ctx &c, int64_t n, double *x, const double *xold,
+                    const double *xmin, const double *xmax, const double *dfdx,
+                    const double *dgdx, double move, double lmid, double *out,
+                    cudaStream_t s);
+void launch_oc_clip(int64_t n, double *dfdx, cudaStream_t s);
+void launch_oc_finish(const Ctx &c, int64_t n, double *x, const double *xold,
+                      const double *xmin, const double *xmax, double *out,
+                      cudaStream_t s);
+
+// host-side element constants (element.cpp)
+int build_element_constants(Ctx &c);
+bool build_filter_taps(const int nel[3], const double dx[3], double R,
+                       FilterTaps &taps);
+
+}  // namespace tpo

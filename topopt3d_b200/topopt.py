@@ -1,0 +1,397 @@
+"""Python mirror of the darinpeetz/TopOpt3D call surface over the C ABI.
+
+``TopOpt`` keeps the reference member names (TopOpt.h:210-292):
+``Set_BC``, ``FEInitialize``, ``MatIntFnc``, ``FEAssemble``, ``FESolve``,
+``Chain_Filter``; ``Compliance`` and ``Volume`` follow ``Function_Base``
+(Functions.h:16-91) with ``Compute`` and ``Function_Call``; ``OC`` follows
+``MMA::Update`` for a single constraint (MMA.cpp:62-180).  Where the
+reference returns a non-zero PetscErrorCode these methods raise
+``TopOptError``; solver non-convergence is reported, as KUF_reason is, in
+``last_solve`` without raising.
+
+Vectors are numpy arrays (host) or torch CUDA float64 tensors (device);
+every call runs on the GPU through libtopopt_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+
+
+class TopOptError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def _is_torch(a):
+    return type(a).__module__.startswith("torch")
+
+
+def _buf(a, n=None, writable=False):
+    """(pointer, mem flag, keepalive) for a numpy array or torch tensor."""
+    if a is None:
+        return None, L.MEM_HOST, None
+    if _is_torch(a):
+        import torch
+        if a.dtype != torch.float64 or not a.is_contiguous():
+            raise TypeError("device buffers must be contiguous float64 tensors")
+        if n is not None and a.numel() < n:
+            raise ValueError(f"buffer has {a.numel()} values, need {n}")
+        mem = L.MEM_DEVICE if a.is_cuda else L.MEM_HOST
+        return C.c_void_p(a.data_ptr()), mem, a
+    arr = np.ascontiguousarray(a, dtype=np.float64)
+    if writable and arr is not a:
+        raise TypeError("output numpy arrays must be contiguous float64")
+    if n is not None and arr.size < n:
+        raise ValueError(f"buffer has {arr.size} values, need {n}")
+    return arr.ctypes.data_as(C.c_void_p), L.MEM_HOST, arr
+
+
+class TopOpt:
+    """One structured hex8 TopOpt problem resident on one GPU."""
+
+    SUPPORT = L.BC_SUPPORT
+    LOAD = L.BC_LOAD
+
+    def __init__(self, nel, dx=(1.0, 1.0, 1.0), E0=1.0, Nu0=0.3, rmin=1.5,
+                 mg_levels=0):
+        self._lib = L.load()
+        p = L.MeshParams((C.c_int32 * 3)(*[int(t) for t in nel]),
+                         (C.c_double * 3)(*[float(t) for t in dx]),
+                         float(E0), float(Nu0), float(rmin), int(mg_levels))
+        h = C.c_void_p()
+        rc = self._lib.tpo_create(C.byref(p), C.byref(h))
+        if rc != 0:
+            raise TopOptError(rc, "tpo_create failed (invalid mesh or no GPU)")
+        self._h = h
+        ne, nn, nl = C.c_int64(), C.c_int64(), C.c_int32()
+        self._lib.tpo_sizes(h, C.byref(ne), C.byref(nn), C.byref(nl))
+        self.nel = tuple(int(t) for t in nel)
+        self.nElem, self.nNode, self.mg_levels = ne.value, nn.value, nl.value
+        self.penal = 3.0
+        self.eps = 1e-10           # Material_Interpolation.cpp:28
+        self.opts = L.default_opts()
+        self.last_solve = None
+        self.function_list = []
+
+    # -- plumbing ---------------------------------------------------------
+    def _check(self, rc, what):
+        if rc < 0:
+            msg = self._lib.tpo_last_error(self._h).decode(errors="replace")
+            raise TopOptError(rc, f"{what}: {msg}")
+        return rc
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.tpo_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def level_dims(self, level):
+        d = (C.c_int32 * 3)()
+        self._check(self._lib.tpo_level_dims(self._h, level, d), "level_dims")
+        return tuple(d)
+
+    # -- boundary conditions (Inputs.cpp:105-223) --------------------------
+    def Set_BC(self, center, radius, limits, values, TYPE):
+        n = C.c_int64()
+        arr = lambda v, k: (C.c_double * k)(*[float(t) for t in v])
+        self._check(self._lib.tpo_add_bc(self._h, int(TYPE), arr(center, 3),
+                                         arr(radius, 3), arr(limits, 6),
+                                         arr(values, 3), C.byref(n)), "Set_BC")
+        return n.value
+
+    def set_bc_arrays(self, fixmask=None, F=None):
+        fm = None if fixmask is None else np.ascontiguousarray(fixmask, np.uint8)
+        fp, mem, keep = _buf(F, 3 * self.nNode)
+        self._check(self._lib.tpo_set_bc(
+            self._h, None if fm is None else fm.ctypes.data_as(C.c_void_p),
+            fp, mem if F is not None else L.MEM_HOST), "set_bc")
+
+    def get_bc(self):
+        fm = np.zeros(self.nNode, np.uint8)
+        F = np.zeros(3 * self.nNode)
+        self._check(self._lib.tpo_get_bc(self._h, fm.ctypes.data_as(C.c_void_p),
+                                         F.ctypes.data_as(C.c_void_p),
+                                         L.MEM_HOST), "get_bc")
+        return fm, F
+
+    # -- FE ----------------------------------------------------------------
+    def FEInitialize(self):
+        self._check(self._lib.tpo_fe_initialize(self._h), "FEInitialize")
+
+    def MatIntFnc(self, design):
+        p, mem, keep = _buf(design, self.nElem)
+        self._check(self._lib.tpo_mat_int_fnc(self._h, p, self.penal, self.eps,
+                                              mem), "MatIntFnc")
+
+    def set_moduli(self, E, dEdz=None):
+        p, mem, k1 = _buf(E, self.nElem)
+        q, _, k2 = _buf(dEdz, self.nElem)
+        self._check(self._lib.tpo_set_moduli(self._h, p, q, mem), "set_moduli")
+
+    def FEAssemble(self, opts=None):
+        if opts is not None:
+            self.opts = opts
+        self._check(self._lib.tpo_fe_assemble(self._h, C.byref(self.opts)),
+                    "FEAssemble")
+
+    def FESolve(self, opts=None):
+        info = L.SolveInfo()
+        o = opts or self.opts
+        rc = self._check(self._lib.tpo_fe_solve(self._h, C.byref(o),
+                                                C.byref(info)), "FESolve")
+        self.KUF_reason = rc
+        self.last_solve = info.as_dict()
+        return self.last_solve
+
+    def solve(self, b, U, nrhs=1, opts=None):
+        """Solve K U = b for nrhs column-major right-hand sides."""
+        info = L.SolveInfo()
+        bp, mem, k1 = _buf(b, 3 * self.nNode * nrhs)
+        up, mem2, k2 = _buf(U, 3 * self.nNode * nrhs, writable=True)
+        if mem != mem2:
+            raise ValueError("b and U must both be host or both be device")
+        self._check(self._lib.tpo_solve(self._h, bp, up, nrhs, mem,
+                                        C.byref(opts or self.opts),
+                                        C.byref(info)), "solve")
+        return info.as_dict()
+
+    def apply(self, u, y, nrhs=1, precision=L.PREC_FP64):
+        up, mem, k1 = _buf(u, 3 * self.nNode * nrhs)
+        yp, mem2, k2 = _buf(y, 3 * self.nNode * nrhs, writable=True)
+        self._check(self._lib.tpo_apply(self._h, up, yp, nrhs, precision, mem),
+                    "apply")
+        return y
+
+    def apply_level(self, level, u, y):
+        up, mem, k1 = _buf(u)
+        yp, _, k2 = _buf(y, writable=True)
+        self._check(self._lib.tpo_apply_level(self._h, level, up, yp, mem),
+                    "apply_level")
+        return y
+
+    def vcycle(self, r, z, precision=L.PREC_FP64):
+        rp, mem, k1 = _buf(r, 3 * self.nNode)
+        zp, _, k2 = _buf(z, 3 * self.nNode, writable=True)
+        self._check(self._lib.tpo_vcycle(self._h, rp, zp, precision, mem),
+                    "vcycle")
+        return z
+
+    def level_lambda(self, level):
+        v = C.c_double()
+        self._check(self._lib.tpo_level_lambda(self._h, level, C.byref(v)),
+                    "level_lambda")
+        return v.value
+
+    def get(self, which, out=None):
+        n = 3 * self.nNode if which in ("U", "F") else self.nElem
+        out = np.zeros(n) if out is None else out
+        p, mem, keep = _buf(out, n, writable=True)
+        self._check(self._lib.tpo_get_vector(self._h, which.encode(), p, mem),
+                    f"get {which}")
+        return out
+
+    def set(self, which, values):
+        n = 3 * self.nNode if which in ("U", "F") else self.nElem
+        p, mem, keep = _buf(values, n)
+        self._check(self._lib.tpo_set_vector(self._h, which.encode(), p, mem),
+                    f"set {which}")
+
+    @property
+    def U(self):
+        return self.get("U")
+
+    @property
+    def F(self):
+        return self.get("F")
+
+    @property
+    def rho(self):
+        return self.get("rho")
+
+    @property
+    def E(self):
+        return self.get("E")
+
+    @property
+    def dEdz(self):
+        return self.get("dEdz")
+
+    # -- filter chain (Material_Interpolation.cpp:150-187) -----------------
+    def filter(self, v, out=None, transpose=False):
+        out = np.zeros(self.nElem) if out is None else out
+        ip, mem, k1 = _buf(v, self.nElem)
+        op, _, k2 = _buf(out, self.nElem, writable=True)
+        self._check(self._lib.tpo_filter(self._h, ip, op, int(bool(transpose)),
+                                         mem), "filter")
+        return out
+
+    def Chain_Filter(self, dfdV=None, dfdE=None):
+        """In-place chain rule through the density filter (vdMin <= 0)."""
+        for v in (dfdV, dfdE):
+            if v is not None:
+                tmp = self.filter(v, transpose=True)
+                v[...] = tmp
+        return dfdV, dfdE
+
+    def compliance(self, gradient=True, want_drho=False, out=None):
+        """C = U.F and dC/dx; `out` may be a host or device float64 buffer
+        that receives dC/dx."""
+        c = C.c_double()
+        if out is not None:
+            dx = out
+        else:
+            dx = np.zeros(self.nElem) if gradient else None
+        dr = np.zeros(self.nElem) if want_drho else None
+        p, mem, keep = _buf(dx, self.nElem, writable=True)
+        if dr is not None and mem != L.MEM_HOST:
+            raise ValueError("want_drho needs a host output buffer")
+        self._check(self._lib.tpo_compliance(
+            self._h, C.byref(c), p,
+            None if dr is None else dr.ctypes.data_as(C.c_void_p),
+            mem), "compliance")
+        return c.value, dx, dr
+
+    def set_stream(self, stream_handle):
+        """Issue all work on a caller cudaStream_t (int handle) or None."""
+        self._check(self._lib.tpo_set_stream(
+            self._h, None if stream_handle is None else C.c_void_p(stream_handle)),
+            "set_stream")
+
+    def volume(self, gradient=True):
+        v = C.c_double()
+        dv = np.zeros(self.nElem) if gradient else None
+        self._check(self._lib.tpo_volume(
+            self._h, C.byref(v),
+            None if dv is None else dv.ctypes.data_as(C.c_void_p), L.MEM_HOST),
+            "volume")
+        return v.value, dv
+
+
+# -- functions (Functions.h:16-91, Functions.cpp:39-109) --------------------
+class Function_Base:
+    def __init__(self, values, min_val, max_val, objective=True,
+                 calc_gradient=True):
+        self.weights = list(values)
+        self.min_val, self.max_val = float(min_val), float(max_val)
+        self.objective = bool(objective)
+        self.calc_gradient = bool(calc_gradient)
+        self.values = [0.0] * len(self.weights)
+        self.gradients = None
+        self.value, self.gradient = 0.0, None
+
+    def Function(self, topOpt):  # pragma: no cover - abstract
+        raise NotImplementedError
+
+    def Compute(self, topOpt):
+        """Functions.cpp:39-62: weighted, normalised value and gradient."""
+        self.Function(topOpt)
+        w = self.weights[0]
+        rng = self.max_val - self.min_val
+        if self.objective:
+            value = w * (self.values[0] - self.min_val)
+            grad = None if self.gradients is None else w * self.gradients
+        else:
+            value = (self.values[0] - self.min_val) - w
+            grad = self.gradients
+        self.value = value / rng
+        self.gradient = None if grad is None else grad / rng
+
+    @staticmethod
+    def Function_Call(topOpt):
+        """Functions.cpp:77-109 -> (f, dfdx, g, dgdx) over all functions."""
+        f, dfdx, g, dgdx = 0.0, np.zeros(topOpt.nElem), [], []
+        for fn in topOpt.function_list:
+            fn.Compute(topOpt)
+            if fn.objective:
+                f += fn.value
+                dfdx += fn.gradient
+            else:
+                g.append(fn.value)
+                dgdx.append(fn.gradient)
+        dg = np.stack(dgdx, axis=1) if dgdx else np.zeros((topOpt.nElem, 0))
+        return f, dfdx, np.array(g), dg
+
+
+class Compliance(Function_Base):
+    """Compliance.cpp:15-57"""
+
+    def Function(self, topOpt):
+        c, dcdx, _ = topOpt.compliance(gradient=self.calc_gradient)
+        self.values[0] = c
+        self.gradients = dcdx
+
+
+class Volume(Function_Base):
+    """Volume.cpp:15-41"""
+
+    def __init__(self, values, min_val, max_val, objective=True,
+                 calc_gradient=True):
+        # constraint values are pre-scaled by the range (Inputs.cpp:554-557)
+        if not objective:
+            values = [v * (max_val - min_val) for v in values]
+        super().__init__(values, min_val, max_val, objective, calc_gradient)
+
+    def Function(self, topOpt):
+        v, dv = topOpt.volume(gradient=self.calc_gradient)
+        self.values[0] = v
+        self.gradients = dv
+
+
+@dataclass
+class OC:
+    """MMA::Update for m < 2 constraints, i.e. the OC branch (MMA.cpp:87-94,
+    103-180), computed on the GPU."""
+    n: int
+    move: float = 0.5            # MMA default move (MMA.h:21) / Step_Limit
+    xmin: np.ndarray = None
+    xmax: np.ndarray = None
+    miniter: int = 0
+    maxiter: int = 50
+    minchange: float = 0.0
+    iter: int = 0
+    Change: float = 1.0
+    xval: np.ndarray = field(default=None)
+
+    def __post_init__(self):
+        if self.xmin is None:
+            self.xmin = np.zeros(self.n)
+        if self.xmax is None:
+            self.xmax = np.ones(self.n)
+
+    def Update(self, topOpt, dfdx, g, dgdx):
+        if g.size != 1:
+            raise TopOptError(-4, "the GPU update implements the OC branch (one constraint)")
+        x = np.ascontiguousarray(self.xval, np.float64)
+        df = np.ascontiguousarray(dfdx, np.float64)
+        dg = np.ascontiguousarray(dgdx[:, 0], np.float64)
+        ch = C.c_double()
+        lib = topOpt._lib
+        topOpt._check(lib.tpo_oc_update(
+            topOpt._h, x.ctypes.data_as(C.c_void_p),
+            self.xmin.ctypes.data_as(C.c_void_p),
+            self.xmax.ctypes.data_as(C.c_void_p), df.ctypes.data_as(C.c_void_p),
+            float(g[0]), dg.ctypes.data_as(C.c_void_p), float(self.move),
+            C.byref(ch), L.MEM_HOST), "OC update")
+        self.xval = x
+        self.Change = ch.value
+        return x
+
+    def Check(self):
+        """MMA.h:83-85"""
+        if (self.iter > self.miniter) and (self.Change < self.minchange):
+            return True
+        self.iter += 1
+        return self.iter >= self.maxiter
