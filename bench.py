@@ -127,7 +127,7 @@ class ClockSampler:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=self.file, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -185,7 +185,9 @@ def run_ours(args, rank, world, local):
     from topopt3d_b200 import problems as P
 
     dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream(dev)
+    # a non-default stream: handle 0 would select the library's own stream
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     cfg = P.CONFIGS[CONFIG]
     nel = cfg["nel"]
     ne, nn = int(np.prod(nel)), int(np.prod([n + 1 for n in nel]))

@@ -68,7 +68,9 @@ typedef struct {
   double cheb_lo;     /* smoothing interval [lo, hi] * lambda_max(D^-1 A) */
   double cheb_hi;
   int32_t power_its;  /* power iterations for lambda_max at setup (15) */
-  double inner_rtol;  /* mixed form: relative drop per inner solve (1e-4) */
+  double inner_rtol;  /* mixed form: floor of the relative drop asked of one
+                         FP32 inner solve (1e-5); each pass asks for the drop
+                         that reaches rtol with a 3x margin, if larger */
   int32_t max_outer;  /* mixed form: defect-correction passes (10) */
   int32_t use_graph;  /* capture the V-cycle/CG iteration in a CUDA graph */
 } tpo_solve_opts;
@@ -83,7 +85,7 @@ typedef struct {
 } tpo_solve_info;
 
 /* fills the defaults used throughout (rtol 1e-8, maxit 500, FP64, Chebyshev
- * degree 2 on [0.1, 1.1] * lambda, 15 power iterations, inner_rtol 1e-4,
+ * degree 2 on [0.1, 1.1] * lambda, 15 power iterations, inner_rtol 1e-5,
  * max_outer 10, graphs on) */
 TPO_API void tpo_default_solve_opts(tpo_solve_opts *opts);
 

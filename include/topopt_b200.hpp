@@ -1,0 +1,180 @@
+// topopt_b200.hpp -- header-only C++ mirror of the darinpeetz/TopOpt3D
+// finite-element call surface over the C ABI in topopt_b200.h.
+//
+// A reference caller keeps its call sequence (Main.cpp:138-169):
+//
+//   tpo::TopOpt t({nx, ny, nz}, {dx, dy, dz}, E0, Nu0, rmin, levels);
+//   t.Set_BC(center, radius, limits, values, tpo::SUPPORT);   // Inputs.cpp:105
+//   t.FEInitialize();                                          // FEAnalysis.cpp:215
+//   t.MatIntFnc(x);                     // Material_Interpolation.cpp:20
+//   t.FEAssemble();                     // FEAnalysis.cpp:432
+//   t.FESolve();                        // FEAnalysis.cpp:507
+//   tpo::Compliance c({1.0}, 0, 1, true);
+//   c.Compute(t);                       // Functions.cpp:39
+//
+// Methods return the library status as the reference returns a
+// PetscErrorCode: 0 on success, negative on error (message in
+// last_error()), positive when the solver stopped without converging
+// (KUF_reason, FEAnalysis.cpp:677).  Vectors are std::vector<double> on the
+// host in the reference numbering.
+#ifndef TOPOPT_B200_HPP
+#define TOPOPT_B200_HPP
+
+#include <array>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "topopt_b200.h"
+
+namespace tpo {
+
+enum BCTYPE { SUPPORT = TPO_BC_SUPPORT, LOAD = TPO_BC_LOAD };
+
+class TopOpt {
+ public:
+  TopOpt(std::array<int, 3> nel, std::array<double, 3> dx, double E0,
+         double Nu0, double rmin, int mg_levels = 0) {
+    tpo_mesh_params p{};
+    for (int d = 0; d < 3; ++d) {
+      p.nel[d] = nel[d];
+      p.dx[d] = dx[d];
+    }
+    p.E0 = E0;
+    p.nu = Nu0;
+    p.rmin = rmin;
+    p.mg_levels = mg_levels;
+    status_ = tpo_create(&p, &ctx_);
+    if (ctx_) tpo_sizes(ctx_, &nElem, &nNode, &levels);
+    tpo_default_solve_opts(&opts);
+  }
+  ~TopOpt() { tpo_destroy(ctx_); }
+  TopOpt(const TopOpt &) = delete;
+  TopOpt &operator=(const TopOpt &) = delete;
+
+  bool ok() const { return ctx_ != nullptr && status_ >= 0; }
+  std::string last_error() const {
+    return ctx_ ? tpo_last_error(ctx_) : "context creation failed";
+  }
+  tpo_ctx *handle() { return ctx_; }
+
+  int Set_BC(std::array<double, 3> center, std::array<double, 3> radius,
+             std::array<double, 6> limits, std::array<double, 3> values,
+             BCTYPE type) {
+    int64_t n = 0;
+    return tpo_add_bc(ctx_, type, center.data(), radius.data(), limits.data(),
+                      values.data(), &n);
+  }
+  int FEInitialize() { return tpo_fe_initialize(ctx_); }
+  int MatIntFnc(const std::vector<double> &design) {
+    return tpo_mat_int_fnc(ctx_, design.data(), penal, eps, TPO_MEM_HOST);
+  }
+  int FEAssemble() { return tpo_fe_assemble(ctx_, &opts); }
+  int FESolve() {
+    KUF_reason = tpo_fe_solve(ctx_, &opts, &info);
+    return KUF_reason < 0 ? KUF_reason : 0;
+  }
+  // Chain_Filter (Material_Interpolation.cpp:150-187) with vdMin <= 0:
+  // dfdV <- P^T dfdV and dfdE <- P^T dfdE, in place; either may be null
+  int Chain_Filter(std::vector<double> *dfdV, std::vector<double> *dfdE) {
+    for (std::vector<double> *v : {dfdV, dfdE}) {
+      if (!v) continue;
+      std::vector<double> out(v->size());
+      int rc = tpo_filter(ctx_, v->data(), out.data(), 1, TPO_MEM_HOST);
+      if (rc) return rc;
+      v->swap(out);
+    }
+    return 0;
+  }
+  std::vector<double> get(const char *which) const {
+    const bool nodal = which[0] == 'U' || which[0] == 'F';
+    std::vector<double> out(nodal ? 3 * nNode : nElem);
+    tpo_get_vector(ctx_, which, out.data(), TPO_MEM_HOST);
+    return out;
+  }
+
+  int64_t nElem = 0, nNode = 0;
+  int32_t levels = 0;
+  double penal = 3.0;
+  double eps = 1e-10;            // Material_Interpolation.cpp:28
+  tpo_solve_opts opts{};
+  tpo_solve_info info{};
+  int KUF_reason = 0;
+
+ private:
+  tpo_ctx *ctx_ = nullptr;
+  int status_ = 0;
+};
+
+// Function_Base (Functions.h:16-63, Functions.cpp:39-62)
+class Function_Base {
+ public:
+  Function_Base(std::vector<double> values, double min_val, double max_val,
+                bool objective, bool calc_gradient = true)
+      : weights(std::move(values)), min_val(min_val), max_val(max_val),
+        objective(objective), calc_gradient(calc_gradient) {}
+  virtual ~Function_Base() = default;
+
+  int Compute(TopOpt &t) {
+    int rc = Function(t);
+    if (rc) return rc;
+    const double w = weights.empty() ? 1.0 : weights[0];
+    const double range = max_val - min_val;
+    value = (objective ? w : 1.0) * (values0 - min_val) - (objective ? 0.0 : w);
+    value /= range;
+    gradient.resize(gradients.size());
+    for (size_t i = 0; i < gradients.size(); ++i)
+      gradient[i] = (objective ? w : 1.0) * gradients[i] / range;
+    return 0;
+  }
+
+  std::vector<double> weights;
+  double min_val, max_val;
+  bool objective, calc_gradient;
+  double values0 = 0.0, value = 0.0;
+  std::vector<double> gradients, gradient;
+
+ protected:
+  virtual int Function(TopOpt &t) = 0;
+};
+
+// Compliance::Function (Compliance.cpp:15-57)
+class Compliance : public Function_Base {
+ public:
+  using Function_Base::Function_Base;
+
+ protected:
+  int Function(TopOpt &t) override {
+    gradients.assign(calc_gradient ? t.nElem : 0, 0.0);
+    return tpo_compliance(t.handle(), &values0,
+                          calc_gradient ? gradients.data() : nullptr, nullptr,
+                          TPO_MEM_HOST);
+  }
+};
+
+// Volume::Function (Volume.cpp:15-41); constraint values are pre-scaled by
+// the range as the input parser does (Inputs.cpp:554-557)
+class Volume : public Function_Base {
+ public:
+  Volume(std::vector<double> values, double min_val, double max_val,
+         bool objective, bool calc_gradient = true)
+      : Function_Base(scale(values, min_val, max_val, objective), min_val,
+                      max_val, objective, calc_gradient) {}
+
+ protected:
+  static std::vector<double> scale(std::vector<double> v, double lo, double hi,
+                                   bool objective) {
+    if (!objective)
+      for (double &x : v) x *= hi - lo;
+    return v;
+  }
+  int Function(TopOpt &t) override {
+    gradients.assign(calc_gradient ? t.nElem : 0, 0.0);
+    return tpo_volume(t.handle(), &values0,
+                      calc_gradient ? gradients.data() : nullptr, TPO_MEM_HOST);
+  }
+};
+
+}  // namespace tpo
+
+#endif  // TOPOPT_B200_HPP

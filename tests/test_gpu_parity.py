@@ -14,7 +14,17 @@ from topopt3d_b200 import problems as P
 pytestmark = pytest.mark.gpu
 
 
-def pair(T, O, nel, levels=2, rmin=1.5, spec=None, x=None, seed=0, assemble=True):
+def levels_for(nel, max_coarse_nodes=2000):
+    """GMG levels until the coarsest grid has at most max_coarse_nodes."""
+    dims, L = [n + 1 for n in nel], 1
+    while np.prod(dims) > max_coarse_nodes:
+        dims = [(d + 1) // 2 for d in dims]
+        L += 1
+    return L
+
+
+def pair(T, O, nel, levels=None, rmin=1.5, spec=None, x=None, seed=0, assemble=True):
+    levels = levels_for(nel) if levels is None else levels
     spec = P.cantilever_bcs(nel) if spec is None else spec
     ne = int(np.prod(nel))
     x = np.random.default_rng(seed).uniform(0.05, 1.0, ne) if x is None else x
@@ -85,15 +95,6 @@ def test_filter_and_matint(T, oracle):
         assert rel(t.rho, rho_o) < 1e-14
         assert rel(t.E, E_o) < 1e-14
         assert rel(t.dEdz, dE_o) < 1e-14
-
-
-def levels_for(nel, max_coarse_nodes=2000):
-    """GMG levels until the coarsest grid has at most max_coarse_nodes."""
-    dims, L = [n + 1 for n in nel], 1
-    while np.prod(dims) > max_coarse_nodes:
-        dims = [(d + 1) // 2 for d in dims]
-        L += 1
-    return L
 
 
 @pytest.mark.parametrize("nel", [(1, 1, 1), (2, 1, 1), (5, 3, 2), (12, 6, 6),

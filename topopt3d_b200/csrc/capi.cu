@@ -8,6 +8,7 @@
 #include <cstring>
 #include <string>
 
+#include "coarse.h"
 #include "solver.h"
 
 using tpo::Ctx;
@@ -128,6 +129,7 @@ int alloc_solver(Ctx &c) {
     A(v.r32, n); A(v.d32, n); A(v.a32, n);
     if (l > 0) {
       A(v.b64, n); A(v.x64, n); A(v.b32, n); A(v.x32, n);
+      A(v.e64, n); A(v.w64, n); A(v.e32, n); A(v.w32, n);
       A(v.S64, 243 * v.nn);
       if (l + 1 < c.L) A(v.S32, 243 * v.nn);
     }
@@ -147,6 +149,7 @@ void free_all(Ctx &c) {
     dfree(v.S64); dfree(v.S32); dfree(v.dinv64); dfree(v.dinv32);
     dfree(v.b64); dfree(v.x64); dfree(v.r64); dfree(v.d64); dfree(v.a64);
     dfree(v.b32); dfree(v.x32); dfree(v.r32); dfree(v.d32); dfree(v.a32);
+    dfree(v.e64); dfree(v.w64); dfree(v.e32); dfree(v.w32);
   }
   dfree(c.fix); dfree(c.F); dfree(c.U); dfree(c.x); dfree(c.rho);
   dfree(c.E64); dfree(c.dEdz); dfree(c.E32); dfree(c.S0); dfree(c.K0lex);
@@ -189,7 +192,7 @@ void tpo_default_solve_opts(tpo_solve_opts *o) {
   o->cheb_lo = 0.1;
   o->cheb_hi = 1.1;
   o->power_its = 15;
-  o->inner_rtol = 1e-4;
+  o->inner_rtol = 1e-5;
   o->max_outer = 10;
   o->use_graph = 1;
 }
@@ -236,6 +239,15 @@ int tpo_create(const tpo_mesh_params *p, tpo_ctx **out) {
     }
   }
   c.L = (int)c.lev.size();
+  // the small levels and the dense coarsest solve run in one persistent
+  // kernel: from the first level (>= 1) with at most kPersistentMaxNodes
+  c.ps = c.L - 1;
+  for (int l = 1; l < c.L; ++l)
+    if (c.lev[l].nn <= tpo::kPersistentMaxNodes) {
+      c.ps = l;
+      break;
+    }
+  if (c.L - c.ps - 1 > tpo::kMaxCoarseLevels) c.ps = c.L - 1 - tpo::kMaxCoarseLevels;
   const int64_t ncoarse = 3 * c.lev[c.L - 1].nn;
   if (ncoarse > 12000) {
     c.err = "coarsest level too large for the dense solve; use more levels";

@@ -1,121 +1,11 @@
-// Fine-level matrix-free stiffness operator and its set-up companions.
-//
-// apply: y = M K(rho) M u + (1 - M) u, K = sum_e E_e K0 (FEAnalysis.cpp:
-// 443-468) with the Dirichlet rows/columns replaced by identity
-// (MatZeroRowsColumns, :473).  M is the per-node fixed-component mask.
-//
-// Layout in HBM: u, y interleaved per node (dof 3n+c, reference order);
-// E per element in reference element order; fix as one byte per node.
-//
-// Kernel structure: a CTA owns a TX x TY column of elements and marches up
-// the z axis one element layer at a time.  Each step stages the next node
-// plane of u (with a one-node halo) in shared memory with row-contiguous,
-// coalesced loads, every thread applies E_e K0 to its element in the modal
-// basis (~210 FP ops instead of the dense 1152), and the element results
-// are gathered per node with warp shuffles along x and one shared-memory
-// exchange along y -- no atomics.  Threads on
-// the low x/y edge of the tile only supply halo elements, so a CTA owns
-// (TX-1) x (TY-1) output node columns.  The contribution of the element
-// layer below each node plane is carried in registers between steps.
+// Set-up companions of the fine-level operator: the Jacobi diagonal and the
+// assembled 27-point stencil used only to form the Galerkin coarse
+// operators.  The matrix-free apply itself is in kernels_apply_staged.cu.
 #include "modal.cuh"
 
 namespace tpo {
 
 namespace {
-
-constexpr int kTX = 32;
-constexpr int kTY = 8;
-
-template <typename T, bool RESID>
-__global__ void __launch_bounds__(kTX *kTY)
-    k_apply_fine(int nelx, int nely, int nelz, int zchunk,
-                 const T *__restrict__ E, const uint8_t *__restrict__ fix,
-                 const T *__restrict__ u, const T *__restrict__ b,
-                 T *__restrict__ y, const Kh<T> kh) {
-  const int Nx = nelx + 1, Ny = nely + 1, Nz = nelz + 1;
-  __shared__ T su[2][3][kTY + 1][kTX + 1];
-  __shared__ T sy[6][kTY][kTX];
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
-  const int X0 = blockIdx.x * (kTX - 1) - 1, Y0 = blockIdx.y * (kTY - 1) - 1;
-  const int zs = blockIdx.z * zchunk;
-  const int ze = min(zs + zchunk, Nz);
-  const int ex = X0 + tx, ey = Y0 + ty;
-  const bool exy = ex >= 0 && ex < nelx && ey >= 0 && ey < nely;
-  const bool owner = tx >= 1 && ty >= 1 && ex < Nx && ey < Ny;
-  const int64_t plane = (int64_t)Nx * Ny;
-
-  auto load_plane = [&](int z, int buf) {
-    for (int k = tid; k < 3 * (kTX + 1) * (kTY + 1); k += kTX * kTY) {
-      const int row = k / (3 * (kTX + 1));
-      const int rem = k - row * 3 * (kTX + 1);
-      const int xi = rem / 3, c = rem - 3 * xi;
-      const int gx = X0 + xi, gy = Y0 + row;
-      T v = T(0);
-      if (z >= 0 && z < Nz && gx >= 0 && gx < Nx && gy >= 0 && gy < Ny) {
-        const int64_t n = z * plane + (int64_t)gy * Nx + gx;
-        if (!((__ldg(fix + n) >> c) & 1)) v = __ldg(u + 3 * n + c);
-      }
-      su[buf][c][row][xi] = v;
-    }
-  };
-
-  T acc[3] = {T(0), T(0), T(0)};
-  load_plane(zs - 1, (zs - 1) & 1);
-  for (int ez = zs - 1; ez < ze; ++ez) {
-    load_plane(ez + 1, (ez + 1) & 1);
-    __syncthreads();
-    T v[8][3];
-    const int pb = ez & 1, pt = (ez + 1) & 1;
-#pragma unroll
-    for (int l = 0; l < 8; ++l) {
-      const int bx = l & 1, by = (l >> 1) & 1, p = (l >> 2) ? pt : pb;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) v[l][c] = su[p][c][ty + by][tx + bx];
-    }
-    const bool ev = exy && ez >= 0 && ez < nelz;
-    const T Ee = ev ? __ldg(E + ((int64_t)ez * nely + ey) * nelx + ex) : T(0);
-    element_apply(v, Ee, kh);
-    // Gather per node (tx, ty) = corner 0/4 of its own element, corner 1/5 of
-    // the -x element, 2/6 of the -y element, 3/7 of the -x-y element.  A warp
-    // is one tile row, so the -x contributions move by shuffle; each thread
-    // pre-sums (own 2/6 + left neighbour's 3/7) for the row above and passes
-    // it through shared memory.  Lane 0 receives its own value from the
-    // shuffle; lane-0 results only reach non-owner threads.
-    T bot[3], top[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const T l3 = __shfl_up_sync(0xffffffffu, v[3][c], 1);
-      const T l7 = __shfl_up_sync(0xffffffffu, v[7][c], 1);
-      const T l1 = __shfl_up_sync(0xffffffffu, v[1][c], 1);
-      const T l5 = __shfl_up_sync(0xffffffffu, v[5][c], 1);
-      sy[c][ty][tx] = v[2][c] + l3;
-      sy[3 + c][ty][tx] = v[6][c] + l7;
-      bot[c] = v[0][c] + l1;
-      top[c] = v[4][c] + l5;
-    }
-    __syncthreads();
-    if (owner) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        bot[c] += sy[c][ty - 1][tx];
-        top[c] += sy[3 + c][ty - 1][tx];
-      }
-      if (ez >= zs) {
-        const int64_t n = ez * plane + (int64_t)ey * Nx + ex;
-        const uint8_t f = __ldg(fix + n);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          T val = acc[c] + bot[c];
-          if ((f >> c) & 1) val = __ldg(u + 3 * n + c);
-          if (RESID) val = __ldg(b + 3 * n + c) - val;
-          y[3 * n + c] = val;
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < 3; ++c) acc[c] = top[c];
-    }
-  }
-}
 
 // Jacobi diagonal of the fine operator: sum_e E_e K0_ii, identity on fixed
 // dofs, non-positive diagonals set to 1 (FEAnalysis.cpp:476-484)
@@ -207,36 +97,6 @@ int grid_for(int64_t n, int threads) {
 }
 
 }  // namespace
-
-template <typename T>
-void launch_apply_fine(const Ctx &c, const T *E, const T *u, const T *b, T *y,
-                       cudaStream_t s) {
-  count_launch();
-  const int Nx = c.nel[0] + 1, Ny = c.nel[1] + 1, Nz = c.nel[2] + 1;
-  dim3 block(kTX, kTY);
-  const int gx = (Nx + kTX - 2) / (kTX - 1), gy = (Ny + kTY - 2) / (kTY - 1);
-  // z chunks: enough CTAs for ~4 per SM, each marching >= 8 planes
-  int chunks = (4 * 148 + gx * gy - 1) / (gx * gy);
-  if (chunks > (Nz + 7) / 8) chunks = (Nz + 7) / 8;
-  if (chunks < 1) chunks = 1;
-  const int zchunk = (Nz + chunks - 1) / chunks;
-  dim3 grid(gx, gy, (Nz + zchunk - 1) / zchunk);
-  const Kh<T> &kh = *reinterpret_cast<const Kh<T> *>(
-      sizeof(T) == 8 ? (const void *)&c.kh64 : (const void *)&c.kh32);
-  if (b)
-    k_apply_fine<T, true><<<grid, block, 0, s>>>(c.nel[0], c.nel[1], c.nel[2],
-                                                 zchunk, E, c.fix, u, b, y, kh);
-  else
-    k_apply_fine<T, false><<<grid, block, 0, s>>>(c.nel[0], c.nel[1], c.nel[2],
-                                                  zchunk, E, c.fix, u, b, y, kh);
-}
-
-template void launch_apply_fine<double>(const Ctx &, const double *,
-                                        const double *, const double *,
-                                        double *, cudaStream_t);
-template void launch_apply_fine<float>(const Ctx &, const float *,
-                                       const float *, const float *, float *,
-                                       cudaStream_t);
 
 void launch_fine_diag(const Ctx &c, double *dinv64, float *dinv32,
                       cudaStream_t s) {

@@ -1,0 +1,286 @@
+// Fine-level matrix-free stiffness operator, staged form.
+//
+//   y = M K(rho) M u + (1 - M) u          (MODE 0)
+//   y = b - [M K(rho) M u + (1 - M) u]    (MODE 1)
+//
+// K = sum_e E_e K0 (FEAnalysis.cpp:443-468), Dirichlet rows/columns replaced
+// by identity (MatZeroRowsColumns, FEAnalysis.cpp:473); M masks the fixed
+// components.  u, y, b are interleaved per node (dof 3n+c), E per element.
+//
+// The element matvec is y_e = T^T Kh T u_e in the 2x2x2 Hadamard basis
+// (tpo_internal.h).  T factorises into an x, a y and a z butterfly, and on a
+// structured grid the x butterfly of one x-edge is shared by the 4 elements
+// around that edge and the y butterfly of one xy-face by the 2 elements
+// above and below it.  So each stage is computed once per grid item:
+//
+//   node u  --x-->  x-edge (s, d)  --y-->  xy-face (4 modes)  --z-->  element
+//   (7 modes) -> E Kh -> element --z^T--> face contributions, summed over the
+//   two elements sharing the face --y^T--> edge contributions, summed over
+//   the two faces sharing the edge --x^T--> node contributions, summed over
+//   the two edges sharing the node.
+//
+// This needs ~165 FP operations per element instead of ~210 for a separate
+// butterfly per element (and 1152 for the dense 24x24 product).
+//
+// Thread (tx, ty) of a 32 x TY CTA owns the grid column (gx, gy) = tile
+// origin + (tx, ty): its node, the x-edge to gx+1, the xy-face spanning
+// (gx..gx+1, gy..gy+1) and the element column above that face; the CTA
+// marches up z.  x-neighbours exchange values by warp shuffles (a warp is
+// one tile row), y-neighbours through shared memory with one barrier per
+// plane.  Lane 0 and row 0 are the halo: the CTA writes nodes tx >= 1,
+// ty >= 1.  Lane 31 and row TY-1 load one extra node (column/row) so every
+// face of the tile is complete.  Node values of the next plane are
+// prefetched into registers one plane ahead.  The pipeline: at step p the
+// plane p is loaded into edges and faces, element layer p-1 is applied, the
+// faces of plane p-1 are complete, and nodes of plane p-2 are written.
+#include "modal.cuh"
+
+namespace tpo {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+template <typename T>
+struct NodeReg {
+  T v[3];
+  unsigned f;
+};
+
+template <typename T>
+__device__ __forceinline__ void fetch_node(const T *__restrict__ u,
+                                           const uint8_t *__restrict__ fix,
+                                           int gx, int gy, int z, int Nx, int Ny,
+                                           int Nz, NodeReg<T> &r) {
+  if (gx >= 0 && gx < Nx && gy >= 0 && gy < Ny && z >= 0 && z < Nz) {
+    const int64_t n = ((int64_t)z * Ny + gy) * Nx + gx;
+    r.f = __ldg(fix + n);
+    r.v[0] = __ldg(u + 3 * n);
+    r.v[1] = __ldg(u + 3 * n + 1);
+    r.v[2] = __ldg(u + 3 * n + 2);
+  } else {
+    r.f = 7u;   // outside the mesh: contributes zero
+    r.v[0] = r.v[1] = r.v[2] = T(0);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T masked(const NodeReg<T> &r, int c) {
+  return ((r.f >> c) & 1u) ? T(0) : r.v[c];
+}
+
+template <typename T, int TY, int MODE>
+__global__ void __launch_bounds__(32 * TY)
+    k_apply_staged(int nelx, int nely, int nelz, int zchunk,
+                   const T *__restrict__ E, const uint8_t *__restrict__ fix,
+                   const T *__restrict__ u, const T *__restrict__ b,
+                   T *__restrict__ y, const Kh<T> kh) {
+  const int Nx = nelx + 1, Ny = nely + 1, Nz = nelz + 1;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int gx = (int)blockIdx.x * 31 - 1 + tx;
+  const int gy = (int)blockIdx.y * (TY - 1) - 1 + ty;
+  const int zs = (int)blockIdx.z * zchunk;
+  const int ze = min(zs + zchunk, Nz);
+  const bool lane31 = (tx == 31);
+  const bool lastrow = (ty == TY - 1);
+  const bool exy = gx >= 0 && gx < nelx && gy >= 0 && gy < nely;
+
+  // dynamic shared memory (the FP64 tiles exceed the 48 KB static limit):
+  // se = x-edge (s, d) per row plus the extra row, sc = upper-edge
+  // contributions, both double-buffered by plane parity
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T(*se)[6][TY + 1][32] = reinterpret_cast<T(*)[6][TY + 1][32]>(smem_raw);
+  T(*sc)[6][TY][32] = reinterpret_cast<T(*)[6][TY][32]>(
+      smem_raw + sizeof(T) * 2 * 6 * (TY + 1) * 32);
+
+  NodeReg<T> n0, n1, n2, n3;   // next plane: own, +x, +y, +x+y
+  n1.f = n2.f = n3.f = 7u;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) n1.v[c] = n2.v[c] = n3.v[c] = T(0);
+  T nE = T(0);
+  auto fetch = [&](int z) {
+    fetch_node(u, fix, gx, gy, z, Nx, Ny, Nz, n0);
+    if (lane31) fetch_node(u, fix, gx + 1, gy, z, Nx, Ny, Nz, n1);
+    if (lastrow) {
+      fetch_node(u, fix, gx, gy + 1, z, Nx, Ny, Nz, n2);
+      if (lane31) fetch_node(u, fix, gx + 1, gy + 1, z, Nx, Ny, Nz, n3);
+    }
+    // element layer z-1 is applied when plane z is the top plane
+    const int ez = z - 1;
+    nE = (exy && ez >= 0 && ez < nelz)
+             ? __ldg(E + ((int64_t)ez * nely + gy) * nelx + gx)
+             : T(0);
+  };
+
+  T Fprev[4][3], ctop[4][3], les[3], led[3];
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) Fprev[m][c] = ctop[m][c] = T(0);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) les[c] = led[c] = T(0);
+
+  fetch(zs - 1);
+  for (int p = zs - 1; p <= ze + 1; ++p) {
+    // ---- plane p: take the prefetched values, prefetch plane p + 1
+    T cu[3], cr[3], cq[3], crq[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      cu[c] = masked(n0, c);
+      cr[c] = masked(n1, c);
+      cq[c] = masked(n2, c);
+      crq[c] = masked(n3, c);
+    }
+    const T Ee = nE;
+    if (p + 1 <= ze + 1) fetch(p + 1);
+    const int buf = p & 1;
+
+    // ---- x-edges of plane p: s = u(x+1) + u(x), d = u(x+1) - u(x)
+    T s0[3], d0[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      T r = __shfl_down_sync(kFull, cu[c], 1);
+      if (lane31) r = cr[c];
+      s0[c] = r + cu[c];
+      d0[c] = r - cu[c];
+      se[buf][c][ty][tx] = s0[c];
+      se[buf][3 + c][ty][tx] = d0[c];
+    }
+    if (lastrow) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        T r = __shfl_down_sync(kFull, cq[c], 1);
+        if (lane31) r = crq[c];
+        se[buf][c][TY][tx] = r + cq[c];
+        se[buf][3 + c][TY][tx] = r - cq[c];
+      }
+    }
+    __syncthreads();
+
+    // ---- xy-face of plane p: modes (1, x, y, xy)
+    T Fp[4][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const T s1 = se[buf][c][ty + 1][tx], d1 = se[buf][3 + c][ty + 1][tx];
+      Fp[0][c] = s0[c] + s1;
+      Fp[1][c] = d0[c] + d1;
+      Fp[2][c] = s1 - s0[c];
+      Fp[3][c] = d1 - d0[c];
+    }
+
+    // ---- nodes of plane p-2: complete the edge, transpose the x stage
+    if (p - 2 >= zs && p - 2 < ze) {
+      T val[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        T es = les[c], ed = led[c];
+        if (ty > 0) {
+          es += sc[buf ^ 1][c][ty - 1][tx];
+          ed += sc[buf ^ 1][3 + c][ty - 1][tx];
+        }
+        const T right = es + ed;
+        const T left = __shfl_up_sync(kFull, right, 1);
+        val[c] = (es - ed) + left;
+      }
+      if (tx >= 1 && ty >= 1 && gx < Nx && gy < Ny) {
+        const int64_t n = ((int64_t)(p - 2) * Ny + gy) * Nx + gx;
+        const unsigned f = __ldg(fix + n);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          T r = val[c];
+          if ((f >> c) & 1u) r = __ldg(u + 3 * n + c);
+          if (MODE == 1) r = __ldg(b + 3 * n + c) - r;
+          y[3 * n + c] = r;
+        }
+      }
+    }
+
+    // ---- element layer p-1 between faces p-1 (Fprev) and p (Fp)
+    T top[4][3], bot[4][3];
+    if (p - 1 >= zs - 1 && p - 1 < ze) {
+      T v[8][3], o[8][3];
+#pragma unroll
+      for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          v[m][c] = (Fp[m][c] + Fprev[m][c]) * Ee;
+          v[m + 4][c] = (Fp[m][c] - Fprev[m][c]) * Ee;
+        }
+      modal_couple(v, o, kh);
+#pragma unroll
+      for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          top[m][c] = o[m][c] + o[m + 4][c];
+          bot[m][c] = o[m][c] - o[m + 4][c];
+        }
+    } else {
+#pragma unroll
+      for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) top[m][c] = bot[m][c] = T(0);
+    }
+
+    // ---- face of plane p-1 is complete: transpose the y stage
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const T G0 = ctop[0][c] + bot[0][c], G1 = ctop[1][c] + bot[1][c];
+      const T G2 = ctop[2][c] + bot[2][c], G3 = ctop[3][c] + bot[3][c];
+      les[c] = G0 - G2;
+      led[c] = G1 - G3;
+      sc[buf][c][ty][tx] = G0 + G2;
+      sc[buf][3 + c][ty][tx] = G1 + G3;
+    }
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        ctop[m][c] = top[m][c];
+        Fprev[m][c] = Fp[m][c];
+      }
+  }
+}
+
+}  // namespace
+
+template <typename T>
+void launch_apply_fine(const Ctx &c, const T *E, const T *u, const T *b, T *y,
+                         cudaStream_t s) {
+  constexpr int TY = 8;
+  const int Nx = c.nel[0] + 1, Ny = c.nel[1] + 1, Nz = c.nel[2] + 1;
+  const int gx = (Nx + 30) / 31, gy = (Ny + TY - 2) / (TY - 1);
+  int chunks = (3 * 148 + gx * gy - 1) / (gx * gy);
+  const int maxc = (Nz + 7) / 8;   // keep >= 8 planes per chunk
+  if (chunks > maxc) chunks = maxc;
+  if (chunks < 1) chunks = 1;
+  const int zchunk = (Nz + chunks - 1) / chunks;
+  dim3 grid(gx, gy, (Nz + zchunk - 1) / zchunk), block(32, TY);
+  const Kh<T> &kh = *reinterpret_cast<const Kh<T> *>(
+      sizeof(T) == 8 ? (const void *)&c.kh64 : (const void *)&c.kh32);
+  const size_t smem = sizeof(T) * 2 * 6 * (2 * TY + 1) * 32;
+  // opt in to > 48 KB of dynamic shared memory once per device
+  static unsigned long long attr_set = 0;   // bit per device, per instantiation
+  const int dev = c.device & 63;
+  if (!((attr_set >> dev) & 1ull)) {
+    cudaFuncSetAttribute(k_apply_staged<T, TY, 0>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_apply_staged<T, TY, 1>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_set |= 1ull << dev;
+  }
+  if (b)
+    k_apply_staged<T, TY, 1><<<grid, block, smem, s>>>(
+        c.nel[0], c.nel[1], c.nel[2], zchunk, E, c.fix, u, b, y, kh);
+  else
+    k_apply_staged<T, TY, 0><<<grid, block, smem, s>>>(
+        c.nel[0], c.nel[1], c.nel[2], zchunk, E, c.fix, u, b, y, kh);
+}
+
+template void launch_apply_fine<double>(const Ctx &, const double *,
+                                          const double *, const double *,
+                                          double *, cudaStream_t);
+template void launch_apply_fine<float>(const Ctx &, const float *,
+                                         const float *, const float *, float *,
+                                         cudaStream_t);
+
+}  // namespace tpo

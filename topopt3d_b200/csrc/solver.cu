@@ -7,9 +7,11 @@
 // Chebyshev/Jacobi smoothing and a direct (here Cholesky) coarse solve.
 #include <cusolverDn.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 
+#include "coarse.h"
 #include "solver.h"
 
 namespace tpo {
@@ -57,11 +59,63 @@ void level_apply(Ctx &c, int l, const T *u, const T *b, T *y, cudaStream_t s) {
     launch_apply_stencil<T>(c.lev[l], lv(c.lev[l], (T *)nullptr).S, u, b, y, s);
 }
 
+// parameters of the persistent kernel for levels ps .. L-1 (kernels_coarse.cu)
+template <typename T>
+CoarseCycle<T> coarse_cycle_params(Ctx &c, const tpo_solve_opts &o) {
+  CoarseCycle<T> P{};
+  P.nlev = c.L - 1 - c.ps;
+  for (int i = 0; i < P.nlev; ++i) {
+    Level &v = c.lev[c.ps + i];
+    LV<T> w = lv(v, (T *)nullptr);
+    CoarseLevel<T> &L = P.lev[i];
+    for (int d = 0; d < 3; ++d) L.dims[d] = v.dims[d];
+    L.nn = v.nn;
+    L.S = w.S;
+    L.dinv = w.dinv;
+    L.b = w.b;
+    L.xout = w.x;
+    L.r = w.r;
+    L.d0 = w.d;
+    L.res = w.a;
+    if (sizeof(T) == 8) {
+      L.xpre = reinterpret_cast<T *>(v.w64);
+      L.d1 = reinterpret_cast<T *>(v.e64);
+    } else {
+      L.xpre = reinterpret_cast<T *>(v.w32);
+      L.d1 = reinterpret_cast<T *>(v.e32);
+    }
+    const Cheb ch = cheb_of(v.lam, o);
+    L.inv_theta = static_cast<T>(ch.inv_theta);
+    L.deg = std::min(o.cheb_degree, kMaxChebDegree);
+    double rho = ch.rho0;
+    for (int k = 1; k < L.deg; ++k) {
+      const double rn = 1.0 / (2.0 * ch.sigma - rho);
+      L.c1[k] = static_cast<T>(rn * rho);
+      L.c2[k] = static_cast<T>(2.0 * rn / ch.delta);
+      rho = rn;
+    }
+  }
+  Level &cl = c.lev[c.L - 1];
+  LV<T> cw = lv(cl, (T *)nullptr);
+  P.Ainv = c.Ainv;
+  P.nc = c.nc;
+  for (int d = 0; d < 3; ++d) P.cdims[d] = cl.dims[d];
+  P.bc = cw.b;
+  P.xc = cw.x;
+  return P;
+}
+
 template <typename T>
 void vcycle_rec(Ctx &c, int l, const T *b, T *x, const tpo_solve_opts &o,
                 cudaStream_t s) {
   if (l == c.L - 1) {
     launch_coarse_gemv<T>(c.nc, c.Ainv, b, x, s);
+    return;
+  }
+  if (l >= 1 && l == c.ps) {
+    // levels ps..L-1 in one cooperative launch; b and x are this level's
+    // own b and x buffers (the restriction above wrote b)
+    c.coarse_err = launch_coarse_cycle<T>(coarse_cycle_params<T>(c, o), s);
     return;
   }
   Level &v = c.lev[l];
@@ -169,6 +223,7 @@ int pcg_loop(Ctx &c, const tpo_solve_opts &o, T *x, T *r, T *z, T *p, T *q,
       cg_body<T>(c, n, x, r, z, p, q, o, first, s);
     }
     CK(cudaGetLastError());
+    CK(c.coarse_err);
     ++k;
     if (int rc = readback(c, 4)) return rc;
     const double rho = c.scal_h[0], pq = c.scal_h[2], rr = c.scal_h[3];
@@ -302,6 +357,7 @@ int vcycle_apply(Ctx &c, const tpo_solve_opts &o, int precision,
     launch_f2d(n, c.z32, z, s);
   }
   CK(cudaGetLastError());
+  CK(c.coarse_err);
   return TPO_OK;
 }
 
@@ -355,7 +411,10 @@ int solve(Ctx &c, const tpo_solve_opts &o, const double *b, double *x,
       CK(cudaMemsetAsync(c.x32, 0, sizeof(float) * n, s));
       launch_dot<float>(c, n, c.r32, c.r32, sc + 3, nullptr, s);
       if (int rc = readback(c, 4)) return rc;
-      const double tgt = o.inner_rtol * o.inner_rtol * c.scal_h[3];
+      // ask the FP32 solve for the reduction that reaches the target with a
+      // 3x margin, but never below the FP32-attainable floor inner_rtol
+      const double eta = std::max(o.inner_rtol, 0.3 * target / rn);
+      const double tgt = eta * eta * c.scal_h[3];
       int its = 0;
       const int st = pcg_loop<float>(c, o, c.x32, c.r32, c.z32, c.p32, c.q32,
                                      tgt, o.maxit - its_total, &its);

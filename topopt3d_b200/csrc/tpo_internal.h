@@ -67,11 +67,12 @@ struct Level {
   double *dinv64 = nullptr;
   float *dinv32 = nullptr;
   double lam = 0.0;
-  // V-cycle work vectors (3*nn each)
+  // V-cycle work vectors (3*nn each); e = second Chebyshev direction and
+  // w = pre-smoothed iterate of the levels run by the persistent kernel
   double *b64 = nullptr, *x64 = nullptr, *r64 = nullptr, *d64 = nullptr,
-         *a64 = nullptr;
+         *a64 = nullptr, *e64 = nullptr, *w64 = nullptr;
   float *b32 = nullptr, *x32 = nullptr, *r32 = nullptr, *d32 = nullptr,
-        *a32 = nullptr;
+        *a32 = nullptr, *e32 = nullptr, *w32 = nullptr;
 };
 
 struct Ctx {
@@ -79,6 +80,8 @@ struct Ctx {
   int nel[3] = {0, 0, 0};
   int64_t ne = 0, nn = 0;
   int L = 0;
+  int ps = 0;   // first level run by the persistent coarse-cycle kernel
+  cudaError_t coarse_err = cudaSuccess;   // last cooperative launch status
   std::vector<Level> lev;
   int device = 0;
   cudaStream_t stream = nullptr;      // stream all work is issued on
