@@ -194,6 +194,32 @@ TPO_API int tpo_set_stream(tpo_ctx *ctx, void *stream);
  * launches count their kernel nodes).  No reference counterpart. */
 TPO_API int64_t tpo_kernel_launches(void);
 
+/* Filtered compliance sensitivity that allocates nothing.  It has no
+ * counterpart in the reference.  It serves callers that may not call
+ * cudaMalloc: a plugin whose host framework owns all device memory through
+ * its own pool, code running while a CUDA graph is being captured, or a
+ * process that fixes its device memory budget up front.  They cannot create
+ * a context (tpo_create allocates), so this call needs none:
+ *   dCdx = P^T(-dEdz .* u_e^T K0 u_e)   (Compliance.cpp:37-51)
+ * for the mesh nel/dx, material E0/nu and filter radius rmin, on caller
+ * device buffers U (3*nNode), dEdz (nElem) and dCdx (nElem), issued on
+ * `stream` (a cudaStream_t; NULL is the legacy default stream).
+ * Its per-element intermediate lives in a fixed device array of
+ * TPO_NOALLOC_MAX_ELEMS doubles (8 MiB) inside the library; every GPU that
+ * loads the library holds that array until the process exits.  Meshes with
+ * more elements are rejected with TPO_E_ARG and a message.  The first call
+ * on a device looks the array's address up with that device current, so
+ * make that first call before any stream capture.  Every call shares the
+ * one array: calls whose kernels overlap on the same GPU race on it, so
+ * order them (one stream, or events).  `msg` (optional, msg_len bytes)
+ * receives an error description. */
+#define TPO_NOALLOC_MAX_ELEMS (1 << 20)
+TPO_API int tpo_sensitivity_noalloc(const int32_t nel[3], const double dx[3],
+                                    double E0, double nu, double rmin,
+                                    const double *U, const double *dEdz,
+                                    double *dCdx, void *stream, char *msg,
+                                    int32_t msg_len);
+
 #ifdef __cplusplus
 }
 #endif

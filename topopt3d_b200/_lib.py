@@ -33,7 +33,9 @@ EXPORTS = (
     "tpo_apply_level", "tpo_vcycle", "tpo_level_lambda", "tpo_get_vector",
     "tpo_set_vector", "tpo_compliance", "tpo_volume", "tpo_filter",
     "tpo_oc_update", "tpo_sync", "tpo_set_stream", "tpo_kernel_launches",
+    "tpo_sensitivity_noalloc",
 )
+NOALLOC_MAX_ELEMS = 1 << 20
 
 
 class MeshParams(C.Structure):
@@ -105,6 +107,8 @@ def load(path: str | None = None):
         "tpo_sync": (C.c_int, [vp]),
         "tpo_set_stream": (C.c_int, [vp, vp]),
         "tpo_kernel_launches": (C.c_int64, []),
+        "tpo_sensitivity_noalloc": (C.c_int, [C.POINTER(i32), dp, d, d, d, vp, vp,
+                                              vp, vp, C.c_char_p, i32]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
