@@ -131,7 +131,14 @@ int alloc_solver(Ctx &c) {
       A(v.b64, n); A(v.x64, n); A(v.b32, n); A(v.x32, n);
       A(v.e64, n); A(v.w64, n); A(v.e32, n); A(v.w32, n);
       A(v.S64, 243 * v.nn);
-      if (l + 1 < c.L) A(v.S32, 243 * v.nn);
+      if (l < c.ps) {
+        A(v.H64, 126 * v.nn);
+        A(v.H32, 126 * v.nn);
+      }
+      if (l >= c.ps && l + 1 < c.L) {
+        A(v.A64, 243 * v.nn);
+        A(v.A32, 243 * v.nn);
+      }
     }
   }
   const int64_t nc = 3 * c.lev[c.L - 1].nn;
@@ -147,6 +154,7 @@ void free_all(Ctx &c) {
   tpo::invalidate_graphs(c);
   for (tpo::Level &v : c.lev) {
     dfree(v.S64); dfree(v.S32); dfree(v.dinv64); dfree(v.dinv32);
+    dfree(v.A64); dfree(v.A32); dfree(v.H64); dfree(v.H32);
     dfree(v.b64); dfree(v.x64); dfree(v.r64); dfree(v.d64); dfree(v.a64);
     dfree(v.b32); dfree(v.x32); dfree(v.r32); dfree(v.d32); dfree(v.a32);
     dfree(v.e64); dfree(v.w64); dfree(v.e32); dfree(v.w32);

@@ -15,7 +15,7 @@ template <typename T>
 struct CoarseLevel {
   int dims[3];
   int64_t nn;
-  const T *S;      // 27-point 3x3-block Galerkin stencil (SoA)
+  const T *A;      // the Galerkin stencil, node-major: A[n*243 + nb*9 + 3r+s]
   const T *dinv;   // 1 / diag
   T *b;            // right-hand side (restricted residual of the parent)
   T *xpre;         // pre-smoothed iterate, then + P x_child

@@ -47,20 +47,58 @@ struct NodeReg {
   unsigned f;
 };
 
-template <typename T>
-__device__ __forceinline__ void fetch_node(const T *__restrict__ u,
+// the input vector of dof i: u_i (IN_U) or the Chebyshev start from a zero
+// guess, invtheta * dinv_i * b_i (IN_CHEB)
+template <typename T, int IN>
+__device__ __forceinline__ T input_value(const ApplyArgs<T> &a, int64_t i) {
+  if (IN == IN_CHEB) return a.invtheta * (__ldg(a.dinv + i) * __ldg(a.b + i));
+  return __ldg(a.u + i);
+}
+
+template <typename T, int IN>
+__device__ __forceinline__ void fetch_node(const ApplyArgs<T> &a,
                                            const uint8_t *__restrict__ fix,
                                            int gx, int gy, int z, int Nx, int Ny,
                                            int Nz, NodeReg<T> &r) {
   if (gx >= 0 && gx < Nx && gy >= 0 && gy < Ny && z >= 0 && z < Nz) {
     const int64_t n = ((int64_t)z * Ny + gy) * Nx + gx;
     r.f = __ldg(fix + n);
-    r.v[0] = __ldg(u + 3 * n);
-    r.v[1] = __ldg(u + 3 * n + 1);
-    r.v[2] = __ldg(u + 3 * n + 2);
+    r.v[0] = input_value<T, IN>(a, 3 * n);
+    r.v[1] = input_value<T, IN>(a, 3 * n + 1);
+    r.v[2] = input_value<T, IN>(a, 3 * n + 2);
   } else {
     r.f = 7u;   // outside the mesh: contributes zero
     r.v[0] = r.v[1] = r.v[2] = T(0);
+  }
+}
+
+// epilogue of dof i with Au_i = (M K M u + (1-M) u)_i and u_i the input:
+//   OUT_Y     y = Au
+//   OUT_RESID y = b - Au
+//   OUT_CHEB2 Chebyshev(2) from a zero guess, input d0 = invtheta dinv b:
+//             r1 = dinv (b - Au); d1 = c1 d0 + c2 r1; y = d0 + d1
+//   OUT_POST0 first Chebyshev step from x = u:  d0 = invtheta dinv (b - Au);
+//             y = d0, y2 = u + d0
+//   OUT_POST1 second step, input d0 = u (so r0 = theta d0):
+//             d1 = c1 d0 + c2 (theta d0 - dinv Au); y = x1 + d1 (x1 = y2)
+template <typename T, int OUT>
+__device__ __forceinline__ void finish_dof(const ApplyArgs<T> &a, int64_t i,
+                                           T Au, T u) {
+  if (OUT == OUT_Y) {
+    a.y[i] = Au;
+  } else if (OUT == OUT_RESID) {
+    a.y[i] = __ldg(a.b + i) - Au;
+  } else if (OUT == OUT_CHEB2) {
+    const T di = __ldg(a.dinv + i), bi = __ldg(a.b + i);
+    const T r1 = di * bi - di * Au;
+    a.y[i] = u + (a.c1 * u + a.c2 * r1);
+  } else if (OUT == OUT_POST0) {
+    const T d0 = a.invtheta * (__ldg(a.dinv + i) * (__ldg(a.b + i) - Au));
+    a.y[i] = d0;
+    a.y2[i] = u + d0;
+  } else {   // OUT_POST1
+    const T r1 = a.theta * u - __ldg(a.dinv + i) * Au;
+    a.y[i] = a.y2[i] + (a.c1 * u + a.c2 * r1);
   }
 }
 
@@ -69,12 +107,11 @@ __device__ __forceinline__ T masked(const NodeReg<T> &r, int c) {
   return ((r.f >> c) & 1u) ? T(0) : r.v[c];
 }
 
-template <typename T, int TY, int MODE>
+template <typename T, int TY, int IN, int OUT>
 __global__ void __launch_bounds__(32 * TY)
     k_apply_staged(int nelx, int nely, int nelz, int zchunk,
                    const T *__restrict__ E, const uint8_t *__restrict__ fix,
-                   const T *__restrict__ u, const T *__restrict__ b,
-                   T *__restrict__ y, const Kh<T> kh) {
+                   const ApplyArgs<T> args, const Kh<T> kh) {
   const int Nx = nelx + 1, Ny = nely + 1, Nz = nelz + 1;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int gx = (int)blockIdx.x * 31 - 1 + tx;
@@ -99,11 +136,11 @@ __global__ void __launch_bounds__(32 * TY)
   for (int c = 0; c < 3; ++c) n1.v[c] = n2.v[c] = n3.v[c] = T(0);
   T nE = T(0);
   auto fetch = [&](int z) {
-    fetch_node(u, fix, gx, gy, z, Nx, Ny, Nz, n0);
-    if (lane31) fetch_node(u, fix, gx + 1, gy, z, Nx, Ny, Nz, n1);
+    fetch_node<T, IN>(args, fix, gx, gy, z, Nx, Ny, Nz, n0);
+    if (lane31) fetch_node<T, IN>(args, fix, gx + 1, gy, z, Nx, Ny, Nz, n1);
     if (lastrow) {
-      fetch_node(u, fix, gx, gy + 1, z, Nx, Ny, Nz, n2);
-      if (lane31) fetch_node(u, fix, gx + 1, gy + 1, z, Nx, Ny, Nz, n3);
+      fetch_node<T, IN>(args, fix, gx, gy + 1, z, Nx, Ny, Nz, n2);
+      if (lane31) fetch_node<T, IN>(args, fix, gx + 1, gy + 1, z, Nx, Ny, Nz, n3);
     }
     // element layer z-1 is applied when plane z is the top plane
     const int ez = z - 1;
@@ -187,10 +224,13 @@ __global__ void __launch_bounds__(32 * TY)
         const unsigned f = __ldg(fix + n);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          T r = val[c];
-          if ((f >> c) & 1u) r = __ldg(u + 3 * n + c);
-          if (MODE == 1) r = __ldg(b + 3 * n + c) - r;
-          y[3 * n + c] = r;
+          // the input is needed for fixed dofs (identity rows) and by the
+          // Chebyshev epilogues
+          const bool need_u = ((f >> c) & 1u) || OUT == OUT_CHEB2 ||
+                              OUT == OUT_POST0 || OUT == OUT_POST1;
+          const T uv = need_u ? input_value<T, IN>(args, 3 * n + c) : T(0);
+          const T Au = ((f >> c) & 1u) ? uv : val[c];
+          finish_dof<T, OUT>(args, 3 * n + c, Au, uv);
         }
       }
     }
@@ -241,46 +281,114 @@ __global__ void __launch_bounds__(32 * TY)
   }
 }
 
+constexpr int kTY = 8;
+
+template <typename T>
+size_t staged_smem() {
+  return sizeof(T) * 2 * 6 * (2 * kTY + 1) * 32;
+}
+
+template <typename T, int IN, int OUT>
+void set_smem_attr() {
+  cudaFuncSetAttribute(k_apply_staged<T, kTY, IN, OUT>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)staged_smem<T>());
+}
+
+// grid of the staged kernel: 31 x (kTY-1) owned node columns per CTA, and z
+// chunks that fill whole waves of co-resident CTAs (a partial last wave
+// idles SMs for the length of a chunk; each chunk costs 3 extra planes)
+template <typename T>
+void staged_grid(const Ctx &c, dim3 &grid, int &zchunk) {
+  const int Nx = c.nel[0] + 1, Ny = c.nel[1] + 1, Nz = c.nel[2] + 1;
+  const int gx = (Nx + 30) / 31, gy = (Ny + kTY - 2) / (kTY - 1);
+  const int dev = c.device & 63;
+  static unsigned long long attr_set = 0;   // bit per device
+  static int slots_cache[64] = {0};
+  if (!((attr_set >> dev) & 1ull)) {
+    // opt in to > 48 KB of dynamic shared memory (the FP64 tiles)
+    set_smem_attr<T, IN_U, OUT_Y>();
+    set_smem_attr<T, IN_U, OUT_RESID>();
+    set_smem_attr<T, IN_CHEB, OUT_CHEB2>();
+    set_smem_attr<T, IN_U, OUT_POST0>();
+    set_smem_attr<T, IN_U, OUT_POST1>();
+    int per_sm = 0, sms = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, k_apply_staged<T, kTY, IN_CHEB, OUT_CHEB2>, 32 * kTY,
+        staged_smem<T>());
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+    slots_cache[dev] = std::max(1, per_sm) * std::max(1, sms);
+    attr_set |= 1ull << dev;
+  }
+  const int slots = slots_cache[dev], tiles = gx * gy;
+  int chunks = 1;
+  for (int w = 1; w <= 8; ++w) {
+    const int ch = (w * slots) / tiles;
+    if (ch >= 1 && (double)(ch * tiles) >= 0.9 * w * slots) {
+      chunks = ch;
+      break;
+    }
+    chunks = std::max(1, ch);
+  }
+  const int maxc = std::max(1, Nz / 8);   // keep >= 8 planes per chunk
+  if (chunks > maxc) chunks = maxc;
+  zchunk = (Nz + chunks - 1) / chunks;
+  grid = dim3(gx, gy, (Nz + zchunk - 1) / zchunk);
+}
+
+template <typename T, int IN, int OUT>
+void launch_mode(const Ctx &c, const T *E, const ApplyArgs<T> &args,
+                 cudaStream_t s) {
+  dim3 grid;
+  int zchunk = 0;
+  staged_grid<T>(c, grid, zchunk);
+  const Kh<T> &kh = *reinterpret_cast<const Kh<T> *>(
+      sizeof(T) == 8 ? (const void *)&c.kh64 : (const void *)&c.kh32);
+  count_launch();
+  k_apply_staged<T, kTY, IN, OUT><<<grid, dim3(32, kTY), staged_smem<T>(), s>>>(
+      c.nel[0], c.nel[1], c.nel[2], zchunk, E, c.fix, args, kh);
+}
+
 }  // namespace
 
 template <typename T>
 void launch_apply_fine(const Ctx &c, const T *E, const T *u, const T *b, T *y,
-                         cudaStream_t s) {
-  constexpr int TY = 8;
-  const int Nx = c.nel[0] + 1, Ny = c.nel[1] + 1, Nz = c.nel[2] + 1;
-  const int gx = (Nx + 30) / 31, gy = (Ny + TY - 2) / (TY - 1);
-  int chunks = (3 * 148 + gx * gy - 1) / (gx * gy);
-  const int maxc = (Nz + 7) / 8;   // keep >= 8 planes per chunk
-  if (chunks > maxc) chunks = maxc;
-  if (chunks < 1) chunks = 1;
-  const int zchunk = (Nz + chunks - 1) / chunks;
-  dim3 grid(gx, gy, (Nz + zchunk - 1) / zchunk), block(32, TY);
-  const Kh<T> &kh = *reinterpret_cast<const Kh<T> *>(
-      sizeof(T) == 8 ? (const void *)&c.kh64 : (const void *)&c.kh32);
-  const size_t smem = sizeof(T) * 2 * 6 * (2 * TY + 1) * 32;
-  // opt in to > 48 KB of dynamic shared memory once per device
-  static unsigned long long attr_set = 0;   // bit per device, per instantiation
-  const int dev = c.device & 63;
-  if (!((attr_set >> dev) & 1ull)) {
-    cudaFuncSetAttribute(k_apply_staged<T, TY, 0>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_apply_staged<T, TY, 1>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_set |= 1ull << dev;
-  }
+                       cudaStream_t s) {
+  ApplyArgs<T> a{};
+  a.u = u;
+  a.b = b;
+  a.y = y;
   if (b)
-    k_apply_staged<T, TY, 1><<<grid, block, smem, s>>>(
-        c.nel[0], c.nel[1], c.nel[2], zchunk, E, c.fix, u, b, y, kh);
+    launch_mode<T, IN_U, OUT_RESID>(c, E, a, s);
   else
-    k_apply_staged<T, TY, 0><<<grid, block, smem, s>>>(
-        c.nel[0], c.nel[1], c.nel[2], zchunk, E, c.fix, u, b, y, kh);
+    launch_mode<T, IN_U, OUT_Y>(c, E, a, s);
+}
+
+template <typename T>
+void launch_apply_fused(const Ctx &c, const T *E, int in, int out,
+                        const ApplyArgs<T> &args, cudaStream_t s) {
+  if (in == IN_CHEB && out == OUT_CHEB2)
+    launch_mode<T, IN_CHEB, OUT_CHEB2>(c, E, args, s);
+  else if (in == IN_U && out == OUT_POST0)
+    launch_mode<T, IN_U, OUT_POST0>(c, E, args, s);
+  else if (in == IN_U && out == OUT_POST1)
+    launch_mode<T, IN_U, OUT_POST1>(c, E, args, s);
+  else if (in == IN_U && out == OUT_RESID)
+    launch_mode<T, IN_U, OUT_RESID>(c, E, args, s);
+  else
+    launch_mode<T, IN_U, OUT_Y>(c, E, args, s);
 }
 
 template void launch_apply_fine<double>(const Ctx &, const double *,
-                                          const double *, const double *,
-                                          double *, cudaStream_t);
+                                        const double *, const double *,
+                                        double *, cudaStream_t);
 template void launch_apply_fine<float>(const Ctx &, const float *,
-                                         const float *, const float *, float *,
+                                       const float *, const float *, float *,
+                                       cudaStream_t);
+template void launch_apply_fused<double>(const Ctx &, const double *, int, int,
+                                         const ApplyArgs<double> &,
                                          cudaStream_t);
+template void launch_apply_fused<float>(const Ctx &, const float *, int, int,
+                                        const ApplyArgs<float> &, cudaStream_t);
 
 }  // namespace tpo

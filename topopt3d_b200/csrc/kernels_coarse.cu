@@ -21,6 +21,7 @@
 #include <cooperative_groups.h>
 
 #include "coarse.h"
+#include "transfer.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -28,35 +29,50 @@ namespace tpo {
 
 namespace {
 
-__device__ __forceinline__ double pw1c(int f, int c, int Nf) {
-  const int d = f - 2 * c;
-  if (d < -1 || d > 1) return 0.0;
-  if (d == 0) return 1.0;
-  return (f + 1 <= Nf - 1) ? 0.5 : 1.0;
-}
-
-// y_I = sum_delta A(I, I+delta) u_{I+delta} for one node, branch-free over
-// the 27 neighbours (out-of-range neighbours have zero blocks; their index is
-// clamped so the load stays in bounds)
-template <typename T>
-__device__ __forceinline__ void stencil_row(const CoarseLevel<T> &L, int64_t n,
-                                            const T *__restrict__ u, T acc[3]) {
+// y_n = sum_delta A(n, n+delta) u_{n+delta} for one node by one warp: lane
+// `nb` < 27 loads block nb (9 contiguous values of the node-major copy,
+// so the warp reads 243 consecutive values) and the neighbour's u, then the
+// three partial sums are reduced across the warp.  Out-of-range neighbours
+// have zero blocks; their index is clamped so every load stays in bounds.
+// Every lane returns the full sums.
+// FROM_B: the input is the Chebyshev start d0 = inv_theta D^-1 b, formed
+// on the fly from b and D^-1 instead of being read from u
+template <typename T, bool FROM_B = false>
+__device__ __forceinline__ void warp_stencil(const CoarseLevel<T> &L, int n,
+                                             const T *__restrict__ u, int lane,
+                                             T acc[3]) {
   const int nx = L.dims[0], ny = L.dims[1], nz = L.dims[2];
-  const int64_t nn = L.nn;
-  const int i = (int)(n % nx), j = (int)((n / nx) % ny), k = (int)(n / ((int64_t)nx * ny));
-  acc[0] = acc[1] = acc[2] = T(0);
-#pragma unroll
-  for (int nb = 0; nb < 27; ++nb) {
-    const int mi = min(max(i + nb % 3 - 1, 0), nx - 1);
-    const int mj = min(max(j + (nb / 3) % 3 - 1, 0), ny - 1);
-    const int mk = min(max(k + nb / 9 - 1, 0), nz - 1);
-    const int64_t m = ((int64_t)mk * ny + mj) * nx + mi;
-    const T u0 = u[3 * m], u1 = u[3 * m + 1], u2 = u[3 * m + 2];
-    const T *s = L.S + (int64_t)nb * 9 * nn + n;
-    acc[0] += s[0] * u0 + s[nn] * u1 + s[2 * nn] * u2;
-    acc[1] += s[3 * nn] * u0 + s[4 * nn] * u1 + s[5 * nn] * u2;
-    acc[2] += s[6 * nn] * u0 + s[7 * nn] * u1 + s[8 * nn] * u2;
+  T p0 = T(0), p1 = T(0), p2 = T(0);
+  if (lane < 27) {
+    const int i = n % nx, j = (n / nx) % ny, k = n / (nx * ny);
+    const int mi = min(max(i + lane % 3 - 1, 0), nx - 1);
+    const int mj = min(max(j + (lane / 3) % 3 - 1, 0), ny - 1);
+    const int mk = min(max(k + lane / 9 - 1, 0), nz - 1);
+    const int m = (mk * ny + mj) * nx + mi;
+    const T *s = L.A + (int64_t)n * 243 + lane * 9;
+    T u0, u1, u2;
+    if (FROM_B) {
+      u0 = L.inv_theta * (L.dinv[3 * m] * L.b[3 * m]);
+      u1 = L.inv_theta * (L.dinv[3 * m + 1] * L.b[3 * m + 1]);
+      u2 = L.inv_theta * (L.dinv[3 * m + 2] * L.b[3 * m + 2]);
+    } else {
+      u0 = u[3 * m];
+      u1 = u[3 * m + 1];
+      u2 = u[3 * m + 2];
+    }
+    p0 = s[0] * u0 + s[1] * u1 + s[2] * u2;
+    p1 = s[3] * u0 + s[4] * u1 + s[5] * u2;
+    p2 = s[6] * u0 + s[7] * u1 + s[8] * u2;
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    p0 += __shfl_xor_sync(0xffffffffu, p0, o);
+    p1 += __shfl_xor_sync(0xffffffffu, p1, o);
+    p2 += __shfl_xor_sync(0xffffffffu, p2, o);
+  }
+  acc[0] = p0;
+  acc[1] = p1;
+  acc[2] = p2;
 }
 
 template <typename T>
@@ -65,28 +81,45 @@ __global__ void __launch_bounds__(kCoarseThreads)
   cg::grid_group grid = cg::this_grid();
   const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
+  const int lane = threadIdx.x & 31;
+  const int gwarp = (int)(tid >> 5), nwarps = (int)(nthr >> 5);
 
   // ---------------- down-sweep: pre-smooth, residual, restrict
   for (int l = 0; l < P.nlev; ++l) {
     CoarseLevel<T> &L = P.lev[l];
-    const int64_t n3 = 3 * L.nn;
-    for (int64_t i = tid; i < n3; i += nthr) {
-      const T r = L.dinv[i] * L.b[i];
-      const T d = r * L.inv_theta;
-      L.r[i] = r;
-      L.d0[i] = d;
-      L.xpre[i] = d;
-    }
-    grid.sync();
+    const int nn = (int)L.nn;
     T *dc = L.d0, *dn = L.d1;
-    for (int k = 1; k < L.deg; ++k) {
-      for (int64_t n = tid; n < L.nn; n += nthr) {
+    if (L.deg >= 2) {
+      // start (d0 = inv_theta D^-1 b, x = d0) fused with the first step
+      for (int n = gwarp; n < nn; n += nwarps) {
         T a[3];
-        stencil_row(L, n, dc, a);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const int64_t i = 3 * n + c;
-          const T r = L.r[i] - L.dinv[i] * a[c];
+        warp_stencil<T, true>(L, n, nullptr, lane, a);
+        if (lane < 3) {
+          const int64_t i = 3 * (int64_t)n + lane;
+          const T di = L.dinv[i];
+          const T r0 = di * L.b[i];
+          const T d0 = r0 * L.inv_theta;
+          const T r = r0 - di * a[lane];
+          const T d = L.c1[1] * d0 + L.c2[1] * r;
+          L.r[i] = r;
+          dn[i] = d;
+          L.xpre[i] = d0 + d;
+        }
+      }
+      grid.sync();
+      T *t = dc; dc = dn; dn = t;
+    } else {
+      for (int64_t i = tid; i < 3 * (int64_t)nn; i += nthr)
+        L.xpre[i] = L.inv_theta * (L.dinv[i] * L.b[i]);
+      grid.sync();
+    }
+    for (int k = 2; k < L.deg; ++k) {
+      for (int n = gwarp; n < nn; n += nwarps) {
+        T a[3];
+        warp_stencil(L, n, dc, lane, a);
+        if (lane < 3) {
+          const int64_t i = 3 * (int64_t)n + lane;
+          const T r = L.r[i] - L.dinv[i] * a[lane];
           const T d = L.c1[k] * dc[i] + L.c2[k] * r;
           L.r[i] = r;
           dn[i] = d;
@@ -96,11 +129,10 @@ __global__ void __launch_bounds__(kCoarseThreads)
       grid.sync();
       T *t = dc; dc = dn; dn = t;
     }
-    for (int64_t n = tid; n < L.nn; n += nthr) {
+    for (int n = gwarp; n < nn; n += nwarps) {
       T a[3];
-      stencil_row(L, n, L.xpre, a);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) L.res[3 * n + c] = L.b[3 * n + c] - a[c];
+      warp_stencil(L, n, L.xpre, lane, a);
+      if (lane < 3) L.res[3 * (int64_t)n + lane] = L.b[3 * (int64_t)n + lane] - a[lane];
     }
     grid.sync();
     // b_child = P^T res
@@ -111,87 +143,49 @@ __global__ void __launch_bounds__(kCoarseThreads)
     const int cz = dense_next ? P.cdims[2] : P.lev[l + 1].dims[2];
     const int fx = L.dims[0], fy = L.dims[1], fz = L.dims[2];
     const int64_t nnc = (int64_t)cx * cy * cz;
-    for (int64_t I = tid; I < nnc; I += nthr) {
-      const int ix = I % cx, iy = (I / cx) % cy, iz = I / ((int64_t)cx * cy);
-      T s0 = 0, s1 = 0, s2 = 0;
-      for (int az = -1; az <= 1; ++az) {
-        const int gz = 2 * iz + az;
-        if (gz < 0 || gz >= fz) continue;
-        const double wz = pw1c(gz, iz, fz);
-        for (int ay = -1; ay <= 1; ++ay) {
-          const int gy = 2 * iy + ay;
-          if (gy < 0 || gy >= fy) continue;
-          const double wy = pw1c(gy, iy, fy);
-          for (int ax = -1; ax <= 1; ++ax) {
-            const int gx = 2 * ix + ax;
-            if (gx < 0 || gx >= fx) continue;
-            const T w = static_cast<T>(pw1c(gx, ix, fx) * wy * wz);
-            const int64_t f = ((int64_t)gz * fy + gy) * fx + gx;
-            s0 += w * L.res[3 * f];
-            s1 += w * L.res[3 * f + 1];
-            s2 += w * L.res[3 * f + 2];
-          }
-        }
-      }
-      bc[3 * I] = s0;
-      bc[3 * I + 1] = s1;
-      bc[3 * I + 2] = s2;
+    for (int I = (int)tid; I < (int)nnc; I += (int)nthr) {
+      const int ix = I % cx, iy = (I / cx) % cy, iz = I / (cx * cy);
+      T s[3];
+      restrict_node(fx, fy, fz, ix, iy, iz, L.res, s);
+      bc[3 * I] = s[0];
+      bc[3 * I + 1] = s[1];
+      bc[3 * I + 2] = s[2];
     }
     grid.sync();
   }
 
   // ---------------- coarsest: x = Ainv b, a warp per row, FP64 accumulation
-  {
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = tid >> 5, nwarps = nthr >> 5;
-    for (int64_t row = warp; row < P.nc; row += nwarps) {
-      const double *a = P.Ainv + row * P.nc;
-      double s = 0;
-      for (int64_t k = lane; k < P.nc; k += 32) s += a[k] * static_cast<double>(P.bc[k]);
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane == 0) P.xc[row] = static_cast<T>(s);
-    }
+  for (int row = gwarp; row < (int)P.nc; row += nwarps) {
+    const double s = gemv_row(P.Ainv + (int64_t)row * P.nc, P.bc, P.nc, lane);
+    if (lane == 0) P.xc[row] = static_cast<T>(s);
   }
   grid.sync();
 
   // ---------------- up-sweep: prolong-add, post-smooth
   for (int l = P.nlev - 1; l >= 0; --l) {
     CoarseLevel<T> &L = P.lev[l];
+    const int nn = (int)L.nn;
     const bool dense_child = (l + 1 == P.nlev);
     const T *xc = dense_child ? P.xc : P.lev[l + 1].xout;
     const int cx = dense_child ? P.cdims[0] : P.lev[l + 1].dims[0];
     const int cy = dense_child ? P.cdims[1] : P.lev[l + 1].dims[1];
     const int cz = dense_child ? P.cdims[2] : P.lev[l + 1].dims[2];
     const int fx = L.dims[0], fy = L.dims[1], fz = L.dims[2];
-    for (int64_t f = tid; f < L.nn; f += nthr) {
-      const int gx = f % fx, gy = (f / fx) % fy, gz = f / ((int64_t)fx * fy);
-      T s0 = 0, s1 = 0, s2 = 0;
-      for (int c2 = gz / 2; 2 * c2 <= gz + 1 && c2 < cz; ++c2) {
-        const double wz = pw1c(gz, c2, fz);
-        for (int c1 = gy / 2; 2 * c1 <= gy + 1 && c1 < cy; ++c1) {
-          const double wy = pw1c(gy, c1, fy);
-          for (int c0 = gx / 2; 2 * c0 <= gx + 1 && c0 < cx; ++c0) {
-            const T w = static_cast<T>(pw1c(gx, c0, fx) * wy * wz);
-            const int64_t I = ((int64_t)c2 * cy + c1) * cx + c0;
-            s0 += w * xc[3 * I];
-            s1 += w * xc[3 * I + 1];
-            s2 += w * xc[3 * I + 2];
-          }
-        }
-      }
-      L.xpre[3 * f] += s0;
-      L.xpre[3 * f + 1] += s1;
-      L.xpre[3 * f + 2] += s2;
+    for (int f = (int)tid; f < nn; f += (int)nthr) {
+      const int gx = f % fx, gy = (f / fx) % fy, gz = f / (fx * fy);
+      T s[3];
+      prolong_node(fx, fy, fz, cx, cy, cz, gx, gy, gz, xc, s);
+      L.xpre[3 * f] += s[0];
+      L.xpre[3 * f + 1] += s[1];
+      L.xpre[3 * f + 2] += s[2];
     }
     grid.sync();
-    for (int64_t n = tid; n < L.nn; n += nthr) {
+    for (int n = gwarp; n < nn; n += nwarps) {
       T a[3];
-      stencil_row(L, n, L.xpre, a);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const int64_t i = 3 * n + c;
-        const T r = L.dinv[i] * (L.b[i] - a[c]);
+      warp_stencil(L, n, L.xpre, lane, a);
+      if (lane < 3) {
+        const int64_t i = 3 * (int64_t)n + lane;
+        const T r = L.dinv[i] * (L.b[i] - a[lane]);
         const T d = r * L.inv_theta;
         L.r[i] = r;
         L.d0[i] = d;
@@ -201,13 +195,12 @@ __global__ void __launch_bounds__(kCoarseThreads)
     grid.sync();
     T *dc = L.d0, *dn = L.d1;
     for (int k = 1; k < L.deg; ++k) {
-      for (int64_t n = tid; n < L.nn; n += nthr) {
+      for (int n = gwarp; n < nn; n += nwarps) {
         T a[3];
-        stencil_row(L, n, dc, a);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const int64_t i = 3 * n + c;
-          const T r = L.r[i] - L.dinv[i] * a[c];
+        warp_stencil(L, n, dc, lane, a);
+        if (lane < 3) {
+          const int64_t i = 3 * (int64_t)n + lane;
+          const T r = L.r[i] - L.dinv[i] * a[lane];
           const T d = L.c1[k] * dc[i] + L.c2[k] * r;
           L.r[i] = r;
           dn[i] = d;

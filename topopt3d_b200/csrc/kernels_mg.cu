@@ -14,6 +14,7 @@
 // FEAnalysis.cpp:412), stored as 27-point 3x3-block stencils in SoA form
 // S[(nb*9 + 3r + s) * nn + node].
 #include "tpo_internal.h"
+#include "transfer.cuh"
 
 namespace tpo {
 
@@ -133,6 +134,73 @@ __global__ void k_apply_stencil(int nx, int ny, int nz, const T *__restrict__ S,
   }
 }
 
+// Symmetric half of a Galerkin stencil: A(n, n+d) = A(n+d, n)^T, so only
+// the centre block and the 13 forward offsets (nb = 13..26) are stored,
+// H[(h*9 + 3r + s) * nn + n] with h = nb - 13.  The apply reads the forward
+// blocks of node n and, transposed, the forward blocks that its 13 backward
+// neighbours store for it; those were read moments earlier by the
+// neighbouring threads, so the second read hits L2 and DRAM traffic is the
+// half-size array.
+__global__ void k_stencil_to_half(int64_t nn, const double *__restrict__ S,
+                                  double *__restrict__ H64,
+                                  float *__restrict__ H32) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 126 * nn;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const double v = S[117 * nn + t];   // (13*9 + q) * nn + n
+    H64[t] = v;
+    H32[t] = static_cast<float>(v);
+  }
+}
+
+template <typename T, bool RESID>
+__global__ void k_apply_stencil_sym(int nx, int ny, int nz,
+                                    const T *__restrict__ H,
+                                    const T *__restrict__ u,
+                                    const T *__restrict__ b, T *__restrict__ y) {
+  const int nn = nx * ny * nz;
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nn;
+       n += gridDim.x * blockDim.x) {
+    const int i = n % nx, j = (n / nx) % ny, k = n / (nx * ny);
+    T a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll
+    for (int h = 0; h < 14; ++h) {
+      const int nb = 13 + h;
+      const int di = nb % 3 - 1, dj = (nb / 3) % 3 - 1, dk = nb / 9 - 1;
+      // forward block A(n, n+d): zero when n+d is outside, index clamped
+      {
+        const int mi = min(i + di, nx - 1), mj = min(max(j + dj, 0), ny - 1),
+                  mk = min(k + dk, nz - 1);
+        const int m = (mk * ny + mj) * nx + max(mi, 0);
+        const T u0 = u[3 * m], u1 = u[3 * m + 1], u2 = u[3 * m + 2];
+        const T *s = H + (int64_t)h * 9 * nn + n;
+        a0 += s[0] * u0 + s[nn] * u1 + s[2 * (int64_t)nn] * u2;
+        a1 += s[3 * (int64_t)nn] * u0 + s[4 * (int64_t)nn] * u1 + s[5 * (int64_t)nn] * u2;
+        a2 += s[6 * (int64_t)nn] * u0 + s[7 * (int64_t)nn] * u1 + s[8 * (int64_t)nn] * u2;
+      }
+      // backward block A(n, n-d) = A(n-d, n)^T, stored by node n-d
+      if (h > 0) {
+        const int mi = i - di, mj = j - dj, mk = k - dk;
+        const bool in = mi >= 0 && mi < nx && mj >= 0 && mj < ny && mk >= 0 && mk < nz;
+        const int m = in ? (mk * ny + mj) * nx + mi : n;
+        const T w = in ? T(1) : T(0);
+        const T u0 = w * u[3 * m], u1 = w * u[3 * m + 1], u2 = w * u[3 * m + 2];
+        const T *s = H + (int64_t)h * 9 * nn + m;
+        a0 += s[0] * u0 + s[3 * (int64_t)nn] * u1 + s[6 * (int64_t)nn] * u2;
+        a1 += s[nn] * u0 + s[4 * (int64_t)nn] * u1 + s[7 * (int64_t)nn] * u2;
+        a2 += s[2 * (int64_t)nn] * u0 + s[5 * (int64_t)nn] * u1 + s[8 * (int64_t)nn] * u2;
+      }
+    }
+    if (RESID) {
+      a0 = b[3 * n] - a0;
+      a1 = b[3 * n + 1] - a1;
+      a2 = b[3 * n + 2] - a2;
+    }
+    y[3 * n] = a0;
+    y[3 * n + 1] = a1;
+    y[3 * n + 2] = a2;
+  }
+}
+
 __global__ void k_stencil_diag(int64_t nn, const double *__restrict__ S,
                                double *dinv64, float *dinv32) {
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
@@ -153,33 +221,11 @@ __global__ void k_restrict(int fx, int fy, int fz, int cx, int cy, int cz,
   for (int64_t I = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; I < nnc;
        I += (int64_t)gridDim.x * blockDim.x) {
     const int ix = I % cx, iy = (I / cx) % cy, iz = I / ((int64_t)cx * cy);
-    T s0 = 0, s1 = 0, s2 = 0;
-    for (int az = -1; az <= 1; ++az) {
-      const int gz = 2 * iz + az;
-      if (gz < 0 || gz >= fz) continue;
-      const double wz = pw1(gz, iz, fz);
-      if (wz == 0.0) continue;
-      for (int ay = -1; ay <= 1; ++ay) {
-        const int gy = 2 * iy + ay;
-        if (gy < 0 || gy >= fy) continue;
-        const double wy = pw1(gy, iy, fy);
-        if (wy == 0.0) continue;
-        for (int ax = -1; ax <= 1; ++ax) {
-          const int gx = 2 * ix + ax;
-          if (gx < 0 || gx >= fx) continue;
-          const double wx = pw1(gx, ix, fx);
-          if (wx == 0.0) continue;
-          const T w = static_cast<T>(wx * wy * wz);
-          const int64_t f = ((int64_t)gz * fy + gy) * fx + gx;
-          s0 += w * rf[3 * f];
-          s1 += w * rf[3 * f + 1];
-          s2 += w * rf[3 * f + 2];
-        }
-      }
-    }
-    bc[3 * I] = s0;
-    bc[3 * I + 1] = s1;
-    bc[3 * I + 2] = s2;
+    T s[3];
+    restrict_node(fx, fy, fz, ix, iy, iz, rf, s);
+    bc[3 * I] = s[0];
+    bc[3 * I + 1] = s[1];
+    bc[3 * I + 2] = s[2];
   }
 }
 
@@ -191,27 +237,11 @@ __global__ void k_prolong_add(int fx, int fy, int fz, int cx, int cy, int cz,
   for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < nnf;
        f += (int64_t)gridDim.x * blockDim.x) {
     const int gx = f % fx, gy = (f / fx) % fy, gz = f / ((int64_t)fx * fy);
-    T s0 = 0, s1 = 0, s2 = 0;
-    for (int cz2 = (gz - 1 + 1) / 2; 2 * cz2 <= gz + 1 && cz2 < cz; ++cz2) {
-      const double wz = pw1(gz, cz2, fz);
-      if (wz == 0.0) continue;
-      for (int cy2 = (gy - 1 + 1) / 2; 2 * cy2 <= gy + 1 && cy2 < cy; ++cy2) {
-        const double wy = pw1(gy, cy2, fy);
-        if (wy == 0.0) continue;
-        for (int cx2 = (gx - 1 + 1) / 2; 2 * cx2 <= gx + 1 && cx2 < cx; ++cx2) {
-          const double wx = pw1(gx, cx2, fx);
-          if (wx == 0.0) continue;
-          const T w = static_cast<T>(wx * wy * wz);
-          const int64_t I = ((int64_t)cz2 * cy + cy2) * cx + cx2;
-          s0 += w * xc[3 * I];
-          s1 += w * xc[3 * I + 1];
-          s2 += w * xc[3 * I + 2];
-        }
-      }
-    }
-    xf[3 * f] += s0;
-    xf[3 * f + 1] += s1;
-    xf[3 * f + 2] += s2;
+    T s[3];
+    prolong_node(fx, fy, fz, cx, cy, cz, gx, gy, gz, xc, s);
+    xf[3 * f] += s[0];
+    xf[3 * f + 1] += s[1];
+    xf[3 * f + 2] += s[2];
   }
 }
 
@@ -240,11 +270,7 @@ __global__ void k_coarse_gemv(int64_t n, const double *__restrict__ A,
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t row = warp; row < n; row += nwarps) {
-    const double *a = A + row * n;
-    double s = 0;
-    for (int64_t k = lane; k < n; k += 32) s += a[k] * static_cast<double>(b[k]);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const double s = gemv_row(A + row * n, b, n, lane);
     if (lane == 0) x[row] = static_cast<T>(s);
   }
 }
@@ -301,6 +327,31 @@ template void launch_apply_stencil<double>(const Level &, const double *,
 template void launch_apply_stencil<float>(const Level &, const float *,
                                           const float *, const float *, float *,
                                           cudaStream_t);
+
+template <typename T>
+void launch_apply_stencil_sym(const Level &v, const T *H, const T *u,
+                              const T *b, T *y, cudaStream_t s) {
+  count_launch();
+  const int g = grid_for(v.nn, 128);
+  if (b)
+    k_apply_stencil_sym<T, true><<<g, 128, 0, s>>>(v.dims[0], v.dims[1],
+                                                   v.dims[2], H, u, b, y);
+  else
+    k_apply_stencil_sym<T, false><<<g, 128, 0, s>>>(v.dims[0], v.dims[1],
+                                                    v.dims[2], H, u, b, y);
+}
+template void launch_apply_stencil_sym<double>(const Level &, const double *,
+                                               const double *, const double *,
+                                               double *, cudaStream_t);
+template void launch_apply_stencil_sym<float>(const Level &, const float *,
+                                              const float *, const float *,
+                                              float *, cudaStream_t);
+
+void launch_stencil_to_half(int64_t nn, const double *S, double *H64,
+                            float *H32, cudaStream_t s) {
+  count_launch();
+  k_stencil_to_half<<<grid_for(126 * nn, 256), 256, 0, s>>>(nn, S, H64, H32);
+}
 
 void launch_galerkin(const Level &fine, const double *Sf, const Level &coarse,
                      double *Sc, cudaStream_t s) {
@@ -359,6 +410,26 @@ __global__ void k_eye(int64_t n, double *A) {
     A[t] = (t / n == t % n) ? 1.0 : 0.0;
 }
 }  // namespace
+
+namespace {
+__global__ void k_soa_to_aos(int64_t nn, const double *__restrict__ S,
+                             double *__restrict__ A64, float *__restrict__ A32) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nn * 243;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t n = t / 243;
+    const int q = (int)(t - n * 243);
+    const double v = S[(int64_t)q * nn + n];
+    A64[t] = v;
+    A32[t] = static_cast<float>(v);
+  }
+}
+}  // namespace
+
+void launch_soa_to_aos(int64_t nn, const double *S, double *A64, float *A32,
+                       cudaStream_t s) {
+  count_launch();
+  k_soa_to_aos<<<grid_for(nn * 243, 256), 256, 0, s>>>(nn, S, A64, A32);
+}
 
 void launch_eye(int64_t n, double *A, cudaStream_t s) {
   count_launch();

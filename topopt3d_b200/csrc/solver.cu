@@ -25,14 +25,14 @@ double now_ms() {
 }
 
 struct Cheb {
-  double inv_theta, sigma, delta, rho0;
+  double inv_theta, sigma, delta, rho0, theta;
 };
 
 Cheb cheb_of(double lam, const tpo_solve_opts &o) {
   const double a = o.cheb_lo * lam, b = o.cheb_hi * lam;
   const double theta = 0.5 * (b + a), delta = 0.5 * (b - a);
   const double sigma = theta / delta;
-  return {1.0 / theta, sigma, delta, 1.0 / sigma};
+  return {1.0 / theta, sigma, delta, 1.0 / sigma, theta};
 }
 
 template <typename T>
@@ -51,10 +51,19 @@ LV<float> lv(Level &v, float *) {
 const double *fineE(const Ctx &c, double *) { return c.E64; }
 const float *fineE(const Ctx &c, float *) { return c.E32; }
 
+const double *halfS(const Level &v, double *) { return v.H64; }
+const float *halfS(const Level &v, float *) { return v.H32; }
+
+// A_l u (or b - A_l u): matrix-free on the finest level, the symmetric
+// half-stored Galerkin stencil between it and the persistent levels, the
+// full FP64 stencil on the persistent levels (used there only for the set-up
+// eigenvalue estimate)
 template <typename T>
 void level_apply(Ctx &c, int l, const T *u, const T *b, T *y, cudaStream_t s) {
   if (l == 0)
     launch_apply_fine<T>(c, fineE(c, (T *)nullptr), u, b, y, s);
+  else if (l < c.ps)
+    launch_apply_stencil_sym<T>(c.lev[l], halfS(c.lev[l], (T *)nullptr), u, b, y, s);
   else
     launch_apply_stencil<T>(c.lev[l], lv(c.lev[l], (T *)nullptr).S, u, b, y, s);
 }
@@ -70,7 +79,8 @@ CoarseCycle<T> coarse_cycle_params(Ctx &c, const tpo_solve_opts &o) {
     CoarseLevel<T> &L = P.lev[i];
     for (int d = 0; d < 3; ++d) L.dims[d] = v.dims[d];
     L.nn = v.nn;
-    L.S = w.S;
+    L.A = (sizeof(T) == 8) ? reinterpret_cast<const T *>(v.A64)
+                           : reinterpret_cast<const T *>(v.A32);
     L.dinv = w.dinv;
     L.b = w.b;
     L.xout = w.x;
@@ -122,6 +132,36 @@ void vcycle_rec(Ctx &c, int l, const T *b, T *x, const tpo_solve_opts &o,
   LV<T> w = lv(v, (T *)nullptr);
   const int64_t n = 3 * v.nn;
   const Cheb ch = cheb_of(v.lam, o);
+  if (l == 0 && o.cheb_degree == 2) {
+    // fine level, Chebyshev(2): the smoother updates run in the epilogues
+    // of the matrix-free apply (kernels_apply_staged.cu, finish_dof)
+    const T *E = fineE(c, (T *)nullptr);
+    const double rn = 1.0 / (2.0 * ch.sigma - ch.rho0);
+    ApplyArgs<T> a{};
+    a.b = b;
+    a.dinv = w.dinv;
+    a.invtheta = static_cast<T>(ch.inv_theta);
+    a.theta = static_cast<T>(ch.theta);
+    a.c1 = static_cast<T>(rn * ch.rho0);
+    a.c2 = static_cast<T>(2.0 * rn / ch.delta);
+    a.y = x;
+    launch_apply_fused<T>(c, E, IN_CHEB, OUT_CHEB2, a, s);   // pre-smooth
+    launch_apply_fine<T>(c, E, x, b, w.a, s);                 // residual
+    Level &cv = c.lev[l + 1];
+    LV<T> cw = lv(cv, (T *)nullptr);
+    launch_restrict<T>(v, cv, w.a, cw.b, s);
+    vcycle_rec<T>(c, l + 1, cw.b, cw.x, o, s);
+    launch_prolong_add<T>(v, cv, cw.x, x, s);
+    a.u = x;                                                  // post-smooth
+    a.y = w.d;
+    a.y2 = w.r;
+    launch_apply_fused<T>(c, E, IN_U, OUT_POST0, a, s);
+    a.u = w.d;
+    a.y = x;
+    a.y2 = w.r;
+    launch_apply_fused<T>(c, E, IN_U, OUT_POST1, a, s);
+    return;
+  }
   // pre-smoothing from a zero guess
   launch_cheb_init<T>(n, w.dinv, b, w.r, w.d, x, ch.inv_theta, true, s);
   double rho = ch.rho0;
@@ -284,8 +324,12 @@ int setup_hierarchy(Ctx &c, const tpo_solve_opts &o) {
     launch_galerkin(c.lev[l], Sf, c.lev[l + 1], c.lev[l + 1].S64, s);
     launch_stencil_diag(c.lev[l + 1], c.lev[l + 1].S64, c.lev[l + 1].dinv64,
                         c.lev[l + 1].dinv32, s);
-    if (l + 1 < c.L - 1)
-      launch_d2f(243 * c.lev[l + 1].nn, c.lev[l + 1].S64, c.lev[l + 1].S32, s);
+    if (l + 1 < c.ps)
+      launch_stencil_to_half(c.lev[l + 1].nn, c.lev[l + 1].S64, c.lev[l + 1].H64,
+                             c.lev[l + 1].H32, s);
+    if (l + 1 >= c.ps && l + 1 < c.L - 1)
+      launch_soa_to_aos(c.lev[l + 1].nn, c.lev[l + 1].S64, c.lev[l + 1].A64,
+                        c.lev[l + 1].A32, s);
   }
   CK(cudaGetLastError());
   // coarsest level: dense Cholesky, then the explicit inverse for a

@@ -64,6 +64,13 @@ struct Level {
   // S[(nb*9 + 3r + s) * nn + node], nb = (dk+1)*9 + (dj+1)*3 + (di+1)
   double *S64 = nullptr;
   float *S32 = nullptr;
+  // node-major copies A[n*243 + nb*9 + 3r + s] for the persistent kernel
+  double *A64 = nullptr;
+  float *A32 = nullptr;
+  // symmetric half (centre + 13 forward blocks) for the levels between the
+  // finest and the persistent kernel: H[(h*9 + 3r + s) * nn + n]
+  double *H64 = nullptr;
+  float *H32 = nullptr;
   double *dinv64 = nullptr;
   float *dinv32 = nullptr;
   double lam = 0.0;
@@ -159,6 +166,22 @@ constexpr int kRedBlocks = 592;   // 4 x 148 SMs: fixed grid for reductions
 template <typename T>
 void launch_apply_fine(const Ctx &c, const T *E, const T *u, const T *b, T *y,
                        cudaStream_t s);
+
+// fused fine-level variants: how the input is formed and what the epilogue
+// writes (kernels_apply_staged.cu, finish_dof)
+enum { IN_U = 0, IN_CHEB = 1 };
+enum { OUT_Y = 0, OUT_RESID = 1, OUT_CHEB2 = 2, OUT_POST0 = 3, OUT_POST1 = 4 };
+
+template <typename T>
+struct ApplyArgs {
+  const T *u, *b, *dinv;
+  T *y, *y2;
+  T invtheta, theta, c1, c2;
+};
+
+template <typename T>
+void launch_apply_fused(const Ctx &c, const T *E, int in, int out,
+                        const ApplyArgs<T> &args, cudaStream_t s);
 void launch_fine_diag(const Ctx &c, double *dinv64, float *dinv32,
                       cudaStream_t s);
 void launch_fine_stencil(const Ctx &c, double *S, cudaStream_t s);
@@ -167,6 +190,11 @@ void launch_fine_stencil(const Ctx &c, double *S, cudaStream_t s);
 template <typename T>
 void launch_apply_stencil(const Level &v, const T *S, const T *u, const T *b,
                           T *y, cudaStream_t s);
+template <typename T>
+void launch_apply_stencil_sym(const Level &v, const T *H, const T *u,
+                              const T *b, T *y, cudaStream_t s);
+void launch_stencil_to_half(int64_t nn, const double *S, double *H64,
+                            float *H32, cudaStream_t s);
 void launch_galerkin(const Level &fine, const double *Sf, const Level &coarse,
                      double *Sc, cudaStream_t s);
 void launch_stencil_diag(const Level &v, const double *S, double *dinv64,
@@ -180,6 +208,9 @@ void launch_prolong_add(const Level &fine, const Level &coarse, const T *xc,
 void launch_to_dense(const Level &v, const double *S, double *A,
                      cudaStream_t s);
 void launch_eye(int64_t n, double *A, cudaStream_t s);
+// stencil SoA S[q*nn + n] -> node-major A[n*243 + q] (FP64 and an FP32 copy)
+void launch_soa_to_aos(int64_t nn, const double *S, double *A64, float *A32,
+                       cudaStream_t s);
 template <typename T>
 void launch_coarse_gemv(int64_t n, const double *Ainv, const T *b, T *x,
                         cudaStream_t s);
