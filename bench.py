@@ -46,6 +46,13 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    # profiling case: set up `--config` and launch one operation `--reps`
+    # times with nothing else around it (for ncu captures; prints no line)
+    ap.add_argument("--kernel", default=None,
+                    choices=["apply32", "apply64", "vcycle32", "vcycle64",
+                             "solve_mixed", "solve_fp64"])
+    ap.add_argument("--config", default=CONFIG)
+    ap.add_argument("--reps", type=int, default=3)
     return ap.parse_args()
 
 
@@ -303,7 +310,7 @@ def run_ours(args, rank, world, local):
         "roofline": {"bound": "hbm", "achieved": round(achieved32, 1),
                      "peak": peak, "unit": "GB/s",
                      "frac": round(achieved32 / peak, 4), "traffic": traffic,
-                     "kernel": "k_apply_fine<float>", "peak_kind": peak_kind},
+                     "kernel": "k_apply_staged<float, 8, IN_U, OUT_Y>", "peak_kind": peak_kind},
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
@@ -353,9 +360,10 @@ def run_e2e(args, T, P, t, x, world, dev, torch):
 
 def cpu_baseline(sample_its=3, steps=None, warmup=0):
     """The oracle's assembled FP64 PCG + GMG (OpenMP, all host threads) on
-    the same 192x96x96 problem.  Sample: `sample_its` PCG iterations per
-    step from U = 0; solves/s = 1 / (per-iteration time x iterations of the
-    full solve, measured once untimed)."""
+    the same 192x96x96 problem.  Without `steps`: one complete solve from
+    U = 0 is timed (solves/s = 1 / its time).  With `steps` (the reference
+    arm): each step runs `sample_its` PCG iterations and solves/s = 1 /
+    (per-iteration time x iterations of the full solve)."""
     from oracle import oracle as O
     from topopt3d_b200 import problems as P
     c = P.CONFIGS[CONFIG]
@@ -366,10 +374,17 @@ def cpu_baseline(sample_its=3, steps=None, warmup=0):
     t0 = time.perf_counter()
     ref.assemble(O.default_opts())
     setup_s = time.perf_counter() - t0
-    # iterations of the full solve (untimed)
     t0 = time.perf_counter()
     _, st, its_full, rr = ref.solve(opts=O.default_opts())
     full_s = time.perf_counter() - t0
+    if not steps:
+        return {"value": round(1.0 / full_s, 6), "unit": UNIT, "cores": cores,
+                "kind": "port",
+                "sample": f"one complete FP64 PCG+GMG solve from U=0 of the 192x96x96 "
+                          f"problem ({its_full} iterations, relres {rr:.2e}, status {st}; "
+                          f"assembled BSR SpMV, Galerkin PtAP, OpenMP); set-up "
+                          f"{setup_s:.1f} s untimed",
+                "full_solve_s": full_s, "setup_s": setup_s}
 
     def sample():
         o0 = O.default_opts(rtol=1e-300, maxit=0)
@@ -416,8 +431,48 @@ def run_reference(args, rank, world):
                     "d2h_bytes_per_step": 0}}
 
 
+def run_kernel_case(args):
+    """Profiling case: set up `args.config` and launch one operation
+    `args.reps` times (the set-up launches precede them)."""
+    import ctypes as C
+
+    import torch
+
+    import topopt3d_b200 as T
+    from topopt3d_b200 import problems as P
+    dev = torch.device("cuda", 0)
+    t = build_problem(T, P, args.config)
+    t.MatIntFnc(torch.tensor(P.design(args.config), device=dev))
+    t.FEAssemble()
+    torch.cuda.synchronize(dev)
+    n = 3 * t.nNode
+    lib = T.load()
+    u64 = torch.randn(n, dtype=torch.float64, device=dev)
+    y64 = torch.empty_like(u64)
+    u32, y32 = u64.float(), torch.empty(n, dtype=torch.float32, device=dev)
+    for _ in range(args.reps):
+        if args.kernel == "apply32":
+            rc = lib.tpo_apply_f32(t._h, C.c_void_p(u32.data_ptr()),
+                                   C.c_void_p(y32.data_ptr()))
+            assert rc == 0, lib.tpo_last_error(t._h)
+        elif args.kernel == "apply64":
+            t.apply(u64, y64, precision=T.PREC_FP64)
+        elif args.kernel in ("vcycle32", "vcycle64"):
+            prec = T.PREC_MIXED if args.kernel == "vcycle32" else T.PREC_FP64
+            t.vcycle(u64, y64, precision=prec)
+        else:
+            prec = T.PREC_MIXED if args.kernel == "solve_mixed" else T.PREC_FP64
+            t.set("U", torch.zeros(n, dtype=torch.float64, device=dev))
+            t.FESolve(T.default_opts(precision=prec))
+    torch.cuda.synchronize(dev)
+    print(f"{args.kernel} on {args.config}: {args.reps} launches done", flush=True)
+
+
 def main():
     args = parse()
+    if args.kernel:
+        run_kernel_case(args)
+        return
     rank, world, local = dist_setup(args)
     if args.impl == "reference":
         line = run_reference(args, rank, world)
