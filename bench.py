@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-multi-rhs", action="store_true")
     # profiling case: set up `--config` and launch one operation `--reps`
     # times with nothing else around it (for ncu captures; prints no line)
     ap.add_argument("--kernel", default=None,
@@ -315,12 +316,58 @@ def run_ours(args, rank, world, local):
         "clocks": clocks,
     }
     t.set_stream(None)
+    if not args.no_multi_rhs:
+        line["multi_rhs"] = run_multi_rhs(args, T, P, torch, dev, stream)
 
     if not args.no_e2e:
         line["e2e"] = run_e2e(args, T, P, t, x, world, dev, torch)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(sample_its=3)
     return line
+
+
+def run_multi_rhs(args, T, P, torch, dev, stream, nrhs=8, reps=3):
+    """Multi-load solves (128x64x64, `nrhs` seeded unit point loads on the
+    x = 128 face): right-hand sides per second with blocks of 1, 4, 8 and
+    the autotuned choice, mixed and FP64, device-resident loads."""
+    cfg = "cfg2"
+    c = P.CONFIGS[cfg]
+    t = build_problem(T, P, cfg)
+    t.set_stream(stream.cuda_stream)
+    t.MatIntFnc(torch.tensor(P.design(cfg), device=dev))
+    t.FEAssemble()
+    F = torch.tensor(P.point_loads(c["nel"], nrhs, seed=2), device=dev)
+    U = torch.zeros_like(F)
+    out = {"workload": f"{c['nel'][0]}x{c['nel'][1]}x{c['nel'][2]} hex8, "
+                       f"{3 * t.nNode} dof, {nrhs} point loads, 1e-8",
+           "unit": "solves/s", "nrhs": nrhs, "reps": reps}
+    for prec, pname in ((T.PREC_MIXED, "mixed"), (T.PREC_FP64, "fp64")):
+        res = {}
+        for block in (1, 4, 8, 0):
+            opts = T.default_opts(precision=prec, rhs_block=block)
+            times, its = [], 0
+            for r in range(reps + 1):
+                U.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                info = t.solve(F, U, nrhs=nrhs, opts=opts)
+                e1.record(stream)
+                torch.cuda.synchronize(dev)
+                assert info["status"] == 0, info
+                if r:                       # the first run is warm-up
+                    times.append(e0.elapsed_time(e1))
+                its = info["iterations"]
+            ms = statistics.median(times)
+            res["auto" if block == 0 else f"block{block}"] = {
+                "value": round(nrhs / (ms / 1e3), 3), "ms": round(ms, 3),
+                "iterations_sum": its}
+        res["best_over_block1"] = round(
+            max(v["value"] for k, v in res.items() if k != "block1")
+            / res["block1"]["value"], 3)
+        out[pname] = res
+    t.set_stream(None)
+    return out
 
 
 def run_e2e(args, T, P, t, x, world, dev, torch):

@@ -73,6 +73,9 @@ typedef struct {
                          that reaches rtol with a 3x margin, if larger */
   int32_t max_outer;  /* mixed form: defect-correction passes (10) */
   int32_t use_graph;  /* capture the V-cycle/CG iteration in a CUDA graph */
+  int32_t rhs_block;  /* tpo_solve: right-hand sides solved together as one
+                         block (1, 2, 4 or 8); 0 = autotuned between 4 and 8
+                         once per context (default) */
 } tpo_solve_opts;
 
 typedef struct {
@@ -86,7 +89,7 @@ typedef struct {
 
 /* fills the defaults used throughout (rtol 1e-8, maxit 500, FP64, Chebyshev
  * degree 2 on [0.1, 1.1] * lambda, 15 power iterations, inner_rtol 1e-5,
- * max_outer 10, graphs on) */
+ * max_outer 10, graphs on, autotuned right-hand-side blocks) */
 TPO_API void tpo_default_solve_opts(tpo_solve_opts *opts);
 
 /* TopOpt::CreateMesh (RecMesh.cpp:426-728) on one device: structured box
@@ -140,7 +143,13 @@ TPO_API int tpo_fe_solve(tpo_ctx *ctx, const tpo_solve_opts *opts,
                  tpo_solve_info *info);
 
 /* solve K U = b for nrhs right-hand sides (column-major, 3*nNode each);
- * U holds the initial guesses and receives the solutions. */
+ * U holds the initial guesses and receives the solutions.  The right-hand
+ * sides run in blocks of opts->rhs_block columns (power-of-two remainders):
+ * one block shares every operator read, V-cycle launch and grid barrier,
+ * with per-column CG scalars and convergence.  info: iterations and outer
+ * passes summed over the right-hand sides, the largest relative residual,
+ * the worst status.  (The reference solves its load cases one KSPSolve at
+ * a time, FEAnalysis.cpp:673.) */
 TPO_API int tpo_solve(tpo_ctx *ctx, const double *b, double *U, int32_t nrhs,
               int mem, const tpo_solve_opts *opts, tpo_solve_info *info);
 

@@ -295,3 +295,40 @@ def oc_update(x, dfdx, g, dgdx, move, xmin=None, xmax=None):
     ch = lib().tor_oc_update(n, xx, xmin, xmax, df, float(g),
                              np.ascontiguousarray(dgdx, np.float64), float(move))
     return xx, ch
+
+
+def optimize_oc(pb, x0, volfrac, iters, move=0.5, penal=3.0, opts=None):
+    """The optimisation loop of Main.cpp:130-170 restated over the oracle:
+    Compliance objective (weight 1, range [0, 1]) and one Volume constraint
+    V <= volfrac (Functions.cpp:39-62 with Inputs.cpp:554-557 pre-scaling),
+    updated by OCsub (MMA.cpp:103-180) for `iters` updates, i.e. iters + 1
+    evaluations.  Each FE solve warm-starts from the previous U
+    (FEAnalysis.cpp:389).  Returns per-evaluation C, V, Change and PCG
+    iterations, and the final design."""
+    opts = opts or default_opts()
+    x = np.array(x0, np.float64)
+    U = None
+    Cs, Vs, chs, its_l = [], [], [], []
+    change = 1.0
+
+    def evaluate():
+        nonlocal U
+        pb.set_design(x, penal, 1e-10)
+        pb.assemble(opts)
+        U, st, its, _ = pb.solve(U0=U, opts=opts)
+        if st != 0:
+            raise RuntimeError(f"oracle solve did not converge (status {st})")
+        C, dCdx, _ = pb.compliance(U)
+        V, dVdx = pb.volume()
+        Cs.append(C)
+        Vs.append(V)
+        chs.append(change)
+        its_l.append(its)
+        return dCdx, V - volfrac, dVdx
+
+    dfdx, g, dgdx = evaluate()
+    for _ in range(iters):
+        x, change = oc_update(x, dfdx, g, dgdx, move)
+        dfdx, g, dgdx = evaluate()
+    return dict(C=np.array(Cs), V=np.array(Vs), change=np.array(chs),
+                its=np.array(its_l), x=x)

@@ -106,6 +106,25 @@ def case(name, nel, levels, rmin, x, spec, store_full):
     print(f"{name}: C = {C:.15g}, its = {its}, direct rel err = {err:.2e}")
 
 
+def oc_trajectory(name, cfg, iters, volfrac=0.3, rtol=1e-10):
+    """The oracle's optimisation loop on a configuration: per-evaluation
+    compliance, volume and change, and a summary of the final design.  The
+    solves run to `rtol` (tighter than the 1e-8 default) so that the
+    trajectory is pinned well below the solver's own error."""
+    c = P.CONFIGS[cfg]
+    pb = O.Problem(c["nel"], rmin=c["rmin"], mg_levels=c["levels"])
+    P.apply_bcs(pb, P.bcs(cfg))
+    h = O.optimize_oc(pb, P.design(cfg), volfrac, iters,
+                      opts=O.default_opts(rtol=rtol, maxit=1000))
+    x = h["x"]
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), cfg=cfg, iters=iters,
+                        volfrac=volfrac, rtol=rtol, C=h["C"], V=h["V"], change=h["change"],
+                        its=h["its"], x_sum=x.sum(), x_sel=x[::61],
+                        x_zero=int((x == 0).sum()))
+    print(f"{name}: C[0] = {h['C'][0]:.12g}, C[-1] = {h['C'][-1]:.12g}, "
+          f"V[-1] = {h['V'][-1]:.12g}")
+
+
 def main():
     nel = (12, 6, 6)
     x = np.random.default_rng(7).uniform(0.1, 1.0, int(np.prod(nel)))
@@ -115,6 +134,7 @@ def main():
     case("column_9x5x4_r2", nel, 2, 2.0, x, P.column_bcs(nel), True)
     nel = P.CONFIGS["cfg0"]["nel"]
     case("cfg0_48x24x24", nel, 3, 1.5, P.design("cfg0"), P.bcs("cfg0"), False)
+    oc_trajectory("oc_cfg3_64x32x32", "cfg3", 50)
 
 
 if __name__ == "__main__":

@@ -7,9 +7,10 @@ filter.  ``TopOpt`` mirrors the reference's call surface.
 """
 from ._lib import (BC_LOAD, BC_SUPPORT, MEM_DEVICE, MEM_HOST, PREC_FP64,
                    PREC_MIXED, SolveInfo, SolveOpts, default_opts, load)
-from .topopt import OC, Compliance, Function_Base, TopOpt, TopOptError, Volume
+from .topopt import (OC, Compliance, Function_Base, TopOpt, TopOptError, Volume,
+                     optimize)
 
 __all__ = ["TopOpt", "TopOptError", "Compliance", "Volume", "Function_Base",
-           "OC", "SolveOpts", "SolveInfo", "default_opts", "load",
+           "OC", "optimize", "SolveOpts", "SolveInfo", "default_opts", "load",
            "PREC_FP64", "PREC_MIXED", "MEM_HOST", "MEM_DEVICE", "BC_SUPPORT",
            "BC_LOAD"]

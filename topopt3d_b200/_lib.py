@@ -49,7 +49,8 @@ class SolveOpts(C.Structure):
                 ("precision", C.c_int32), ("cheb_degree", C.c_int32),
                 ("cheb_lo", C.c_double), ("cheb_hi", C.c_double),
                 ("power_its", C.c_int32), ("inner_rtol", C.c_double),
-                ("max_outer", C.c_int32), ("use_graph", C.c_int32)]
+                ("max_outer", C.c_int32), ("use_graph", C.c_int32),
+                ("rhs_block", C.c_int32)]
 
 
 class SolveInfo(C.Structure):

@@ -114,8 +114,57 @@ int check_mem(Ctx &c, int mem) {
   return TPO_OK;
 }
 
+// per-level V-cycle vectors and the fine-level Krylov vectors: nb_cap
+// columns each
+int alloc_columns(Ctx &c) {
+  const size_t n0 = 3 * c.nn, cap = c.nb_cap;
+  int rc = 0;
+#define A(p, n) \
+  if ((rc = dalloc(c, &(p), (n))) != TPO_OK) return rc
+  for (int l = 0; l < c.L; ++l) {
+    tpo::Level &v = c.lev[l];
+    const size_t n = 3 * v.nn * cap;
+    A(v.r64, n); A(v.d64, n); A(v.a64, n);
+    A(v.r32, n); A(v.d32, n); A(v.a32, n);
+    if (l > 0) {
+      A(v.b64, n); A(v.x64, n); A(v.b32, n); A(v.x32, n);
+      A(v.e64, n); A(v.w64, n); A(v.e32, n); A(v.w32, n);
+    }
+  }
+  A(c.r64, n0 * cap); A(c.z64, n0 * cap); A(c.p64, n0 * cap); A(c.q64, n0 * cap);
+  A(c.r32, n0 * cap); A(c.z32, n0 * cap); A(c.p32, n0 * cap); A(c.q32, n0 * cap);
+  A(c.x32, n0 * cap);
+  if (cap > 1) {
+    A(c.io_ba, n0 * cap);
+    A(c.io_bb, n0 * cap);
+  }
+#undef A
+  return TPO_OK;
+}
+
+void free_columns(Ctx &c) {
+  for (tpo::Level &v : c.lev) {
+    dfree(v.b64); dfree(v.x64); dfree(v.r64); dfree(v.d64); dfree(v.a64);
+    dfree(v.b32); dfree(v.x32); dfree(v.r32); dfree(v.d32); dfree(v.a32);
+    dfree(v.e64); dfree(v.w64); dfree(v.e32); dfree(v.w32);
+  }
+  dfree(c.r64); dfree(c.z64); dfree(c.p64); dfree(c.q64);
+  dfree(c.r32); dfree(c.z32); dfree(c.p32); dfree(c.q32); dfree(c.x32);
+  dfree(c.io_ba); dfree(c.io_bb);
+}
+
+// room for nb columns: the column vectors are re-allocated for kMaxBatch
+// columns the first time a block of more than one is asked for
+int ensure_columns(Ctx &c, int nb) {
+  if (nb <= c.nb_cap) return TPO_OK;
+  CK(cudaStreamSynchronize(c.stream));
+  tpo::invalidate_graphs(c);
+  free_columns(c);
+  c.nb_cap = tpo::kMaxBatch;
+  return alloc_columns(c);
+}
+
 int alloc_solver(Ctx &c) {
-  const size_t n0 = 3 * c.nn;
   int rc = 0;
 #define A(p, n) \
   if ((rc = dalloc(c, &(p), (n))) != TPO_OK) return rc
@@ -125,11 +174,7 @@ int alloc_solver(Ctx &c) {
     const size_t n = 3 * v.nn;
     A(v.dinv64, n);
     A(v.dinv32, n);
-    A(v.r64, n); A(v.d64, n); A(v.a64, n);
-    A(v.r32, n); A(v.d32, n); A(v.a32, n);
     if (l > 0) {
-      A(v.b64, n); A(v.x64, n); A(v.b32, n); A(v.x32, n);
-      A(v.e64, n); A(v.w64, n); A(v.e32, n); A(v.w32, n);
       A(v.S64, 243 * v.nn);
       if (l < c.ps) {
         A(v.H64, 126 * v.nn);
@@ -144,27 +189,23 @@ int alloc_solver(Ctx &c) {
   const int64_t nc = 3 * c.lev[c.L - 1].nn;
   A(c.Adense, (size_t)(nc * nc));
   A(c.Ainv, (size_t)(nc * nc));
-  A(c.r64, n0); A(c.z64, n0); A(c.p64, n0); A(c.q64, n0); A(c.w64, n0);
-  A(c.r32, n0); A(c.z32, n0); A(c.p32, n0); A(c.q32, n0); A(c.x32, n0);
+  A(c.w64, 3 * c.nn);
 #undef A
-  return TPO_OK;
+  return alloc_columns(c);
 }
 
 void free_all(Ctx &c) {
   tpo::invalidate_graphs(c);
+  free_columns(c);
   for (tpo::Level &v : c.lev) {
     dfree(v.S64); dfree(v.S32); dfree(v.dinv64); dfree(v.dinv32);
     dfree(v.A64); dfree(v.A32); dfree(v.H64); dfree(v.H32);
-    dfree(v.b64); dfree(v.x64); dfree(v.r64); dfree(v.d64); dfree(v.a64);
-    dfree(v.b32); dfree(v.x32); dfree(v.r32); dfree(v.d32); dfree(v.a32);
-    dfree(v.e64); dfree(v.w64); dfree(v.e32); dfree(v.w32);
   }
   dfree(c.fix); dfree(c.F); dfree(c.U); dfree(c.x); dfree(c.rho);
   dfree(c.E64); dfree(c.dEdz); dfree(c.E32); dfree(c.S0); dfree(c.K0lex);
   dfree(c.Ainv); dfree(c.Adense); dfree(c.solver_work); dfree(c.dev_info);
   dfree(c.finv); dfree(c.taps_d);
-  dfree(c.r64); dfree(c.z64); dfree(c.p64); dfree(c.q64); dfree(c.w64);
-  dfree(c.r32); dfree(c.z32); dfree(c.p32); dfree(c.q32); dfree(c.x32);
+  dfree(c.w64);
   dfree(c.scal); dfree(c.part); dfree(c.ticket); dfree(c.tmpe); dfree(c.tmpe2);
   dfree(c.io_a); dfree(c.io_b);
   dfree(c.oc_ws);
@@ -203,6 +244,7 @@ void tpo_default_solve_opts(tpo_solve_opts *o) {
   o->inner_rtol = 1e-5;
   o->max_outer = 10;
   o->use_graph = 1;
+  o->rhs_block = 0;
 }
 
 const char *tpo_last_error(const tpo_ctx *ctx) {
@@ -291,11 +333,13 @@ int tpo_create(const tpo_mesh_params *p, tpo_ctx **out) {
   A(c.finv, c.ne); A(c.K0lex, 576);
   A(c.x, c.ne); A(c.rho, c.ne); A(c.E64, c.ne); A(c.dEdz, c.ne); A(c.E32, c.ne);
   A(c.fix, c.nn); A(c.F, 3 * c.nn); A(c.U, 3 * c.nn);
-  A(c.scal, 16); A(c.part, tpo::kRedBlocks); A(c.ticket, 1);
+  A(c.scal, tpo::kScalCount); A(c.part, tpo::kPartCount); A(c.ticket, tpo::kMaxBatch);
   A(c.tmpe, c.ne); A(c.tmpe2, c.ne); A(c.dev_info, 1);
   A(c.io_a, nio); A(c.io_b, nio);
 #undef A
-  if (cudaMallocHost(&c.scal_h, 16 * sizeof(double)) != cudaSuccess)
+  // scalar mirror plus a staging row for per-column uploads
+  if (cudaMallocHost(&c.scal_h, (tpo::kScalCount + tpo::kMaxBatch) * sizeof(double)) !=
+      cudaSuccess)
     return fail(TPO_E_CUDA);
   static constexpr int kLexToLocal[8] = {0, 1, 3, 2, 4, 5, 7, 6};
   double Kl[576];
@@ -487,6 +531,52 @@ int tpo_fe_solve(tpo_ctx *ctx, const tpo_solve_opts *opts, tpo_solve_info *info)
   return finish(c, tpo::solve(c, o, c.F, c.U, info));
 }
 
+// largest power of two <= min(n, cap)
+static int pow2_block(int n, int cap) {
+  int w = 1;
+  while (2 * w <= n && 2 * w <= cap) w *= 2;
+  return w;
+}
+
+// right-hand-side block for a solve: the caller's choice, else the faster
+// per column of 4 and 8 on this context, measured once: one V-cycle and one
+// fine apply of each block size on scratch columns (CUDA events on the
+// context's stream)
+static int rhs_block_for(Ctx &c, const tpo_solve_opts &o, int nrhs, int *block) {
+  if (o.rhs_block > 0) {
+    *block = o.rhs_block;
+    return TPO_OK;
+  }
+  if (nrhs < 8) {
+    *block = pow2_block(nrhs, 4);
+    return TPO_OK;
+  }
+  if (!c.rhs_block_tuned) {
+    if (int rc = ensure_columns(c, tpo::kMaxBatch)) return rc;
+    float ms[2] = {0, 0};
+    const int cand[2] = {4, 8};
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    for (int t = 0; t < 2; ++t) {
+      for (int rep = 0; rep < 3; ++rep) {
+        CK(cudaEventRecord(e0, c.stream));
+        if (int rc = tpo::vcycle_block(c, c.setup_opts, o.precision, cand[t])) return rc;
+        CK(cudaEventRecord(e1, c.stream));
+        CK(cudaEventSynchronize(e1));
+        float v = 0;
+        CK(cudaEventElapsedTime(&v, e0, e1));
+        if (rep > 0) ms[t] += v / cand[t];   // first run warms up
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c.rhs_block_tuned = ms[1] < ms[0] ? 8 : 4;
+  }
+  *block = c.rhs_block_tuned;
+  return TPO_OK;
+}
+
 int tpo_solve(tpo_ctx *ctx, const double *b, double *U, int32_t nrhs, int mem,
               const tpo_solve_opts *opts, tpo_solve_info *info) {
   if (int rc = begin(ctx)) return rc;
@@ -496,28 +586,39 @@ int tpo_solve(tpo_ctx *ctx, const double *b, double *U, int32_t nrhs, int mem,
   tpo_solve_opts o;
   if (opts) o = *opts; else tpo_default_solve_opts(&o);
   if (int rc = validate_solve(c, o)) return rc;
+  REQUIRE(o.rhs_block == 0 || o.rhs_block == 1 || o.rhs_block == 2 || o.rhs_block == 4 ||
+              o.rhs_block == 8,
+          "rhs_block must be 0, 1, 2, 4 or 8");
+  int block = 1;
+  if (int rc = rhs_block_for(c, o, nrhs, &block)) return finish(c, rc);
   const size_t n = 3 * c.nn;
   int worst = TPO_OK;
   tpo_solve_info acc{};
-  for (int j = 0; j < nrhs; ++j) {
-    const double *bj = b + j * n;
-    double *uj = U + j * n;
-    const double *db = nullptr;
+  for (int j0 = 0; j0 < nrhs;) {
+    const int nb = pow2_block(nrhs - j0, block);
+    if (int rc = ensure_columns(c, nb)) return rc;
+    const double *bj = b + j0 * n;
+    double *uj = U + j0 * n;
+    const double *db = bj;
     double *du = uj;
-    if (int rc = stage_in(c, bj, n, mem, c.io_a, &db)) return rc;
     if (mem != TPO_MEM_DEVICE) {
-      CK(cudaMemcpyAsync(c.io_b, uj, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream));
-      du = c.io_b;
+      double *sb = nb > 1 ? c.io_ba : c.io_a;
+      double *su = nb > 1 ? c.io_bb : c.io_b;
+      CK(cudaMemcpyAsync(sb, bj, sizeof(double) * n * nb, cudaMemcpyHostToDevice, c.stream));
+      CK(cudaMemcpyAsync(su, uj, sizeof(double) * n * nb, cudaMemcpyHostToDevice, c.stream));
+      db = sb;
+      du = su;
     }
     tpo_solve_info one{};
-    const int rc = tpo::solve(c, o, db, du, &one);
-    if (rc < 0) return finish(c, rc);
-    if (int rc2 = copy_out(c, uj, du, n, mem)) return rc2;
-    if (rc != TPO_OK && worst == TPO_OK) worst = rc;
+    const int rc = tpo::solve(c, o, db, du, &one, nb);
+    if (rc < 0 && rc != TPO_E_BREAKDOWN) return finish(c, rc);
+    if (int rc2 = copy_out(c, uj, du, n * nb, mem)) return rc2;
+    if (rc < 0 ? rc < worst : (worst == TPO_OK && rc != TPO_OK)) worst = rc;
     acc.iterations += one.iterations;
     acc.outer += one.outer;
     acc.relres = std::max(acc.relres, one.relres);
     acc.solve_ms += one.solve_ms;
+    j0 += nb;
   }
   acc.status = worst;
   acc.setup_ms = c.setup_ms;
@@ -534,18 +635,26 @@ int tpo_apply(tpo_ctx *ctx, const double *u, double *y, int32_t nrhs,
   REQUIRE(c.initialized && c.have_material, "mesh not initialised or no material");
   REQUIRE(precision == TPO_PREC_FP64 || precision == TPO_PREC_MIXED, "invalid precision");
   const size_t n = 3 * c.nn;
-  for (int j = 0; j < nrhs; ++j) {
-    const double *du = nullptr;
-    if (int rc = stage_in(c, u + j * n, n, mem, c.io_a, &du)) return rc;
-    double *dy = (mem == TPO_MEM_DEVICE) ? y + j * n : c.io_b;
-    if (precision == TPO_PREC_FP64) {
-      tpo::launch_apply_fine<double>(c, c.E64, du, nullptr, dy, c.stream);
-    } else {
-      tpo::launch_d2f(n, du, c.r32, c.stream);
-      tpo::launch_apply_fine<float>(c, c.E32, c.r32, nullptr, c.q32, c.stream);
-      tpo::launch_f2d(n, c.q32, dy, c.stream);
+  for (int j0 = 0; j0 < nrhs;) {
+    const int nb = std::min<int>(nrhs - j0, tpo::kMaxBatch);
+    if (int rc = ensure_columns(c, nb)) return rc;
+    const double *du = u + j0 * n;
+    double *dy = y + j0 * n;
+    if (mem != TPO_MEM_DEVICE) {
+      double *sa = nb > 1 ? c.io_ba : c.io_a;
+      CK(cudaMemcpyAsync(sa, du, sizeof(double) * n * nb, cudaMemcpyHostToDevice, c.stream));
+      du = sa;
+      dy = nb > 1 ? c.io_bb : c.io_b;
     }
-    if (int rc = copy_out(c, y + j * n, dy, n, mem)) return rc;
+    if (precision == TPO_PREC_FP64) {
+      tpo::launch_apply_fine<double>(c, c.E64, du, nullptr, dy, c.stream, nb);
+    } else {
+      tpo::launch_d2f(n * nb, du, c.r32, c.stream);
+      tpo::launch_apply_fine<float>(c, c.E32, c.r32, nullptr, c.q32, c.stream, nb);
+      tpo::launch_f2d(n * nb, c.q32, dy, c.stream);
+    }
+    if (int rc = copy_out(c, y + j0 * n, dy, n * nb, mem)) return rc;
+    j0 += nb;
   }
   return finish(c, TPO_OK);
 }
@@ -641,8 +750,8 @@ int tpo_compliance(tpo_ctx *ctx, double *C, double *dCdx, double *dCdrho, int me
   REQUIRE(c.initialized && c.have_material, "mesh not initialised or no material");
   const int64_t n = 3 * c.nn;
   if (C) {
-    tpo::launch_dot<double>(c, n, c.U, c.F, c.scal + 8, nullptr, c.stream);  // :19
-    CK(cudaMemcpyAsync(c.scal_h + 8, c.scal + 8, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    tpo::launch_dot<double>(c, n, c.U, c.F, c.scal + tpo::SC_COMPLIANCE, nullptr, c.stream);  // :19
+    CK(cudaMemcpyAsync(c.scal_h + tpo::SC_COMPLIANCE, c.scal + tpo::SC_COMPLIANCE, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
   }
   if (dCdx || dCdrho) {
     tpo::launch_sensitivity(c, c.U, c.tmpe, c.stream);                      // :37-46
@@ -654,7 +763,7 @@ int tpo_compliance(tpo_ctx *ctx, double *C, double *dCdx, double *dCdrho, int me
     }
   }
   CK(cudaStreamSynchronize(c.stream));
-  if (C) *C = c.scal_h[8];
+  if (C) *C = c.scal_h[tpo::SC_COMPLIANCE];
   return finish(c, TPO_OK);
 }
 
@@ -665,15 +774,15 @@ int tpo_volume(tpo_ctx *ctx, double *V, double *dVdx, int mem) {
   REQUIRE(c.have_material, "no material");
   if (V) {
     tpo::launch_fill(c.ne, c.tmpe2, 1.0, c.stream);
-    tpo::launch_dot<double>(c, c.ne, c.rho, c.tmpe2, c.scal + 9, nullptr, c.stream);
-    CK(cudaMemcpyAsync(c.scal_h + 9, c.scal + 9, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    tpo::launch_dot<double>(c, c.ne, c.rho, c.tmpe2, c.scal + tpo::SC_VOLUME, nullptr, c.stream);
+    CK(cudaMemcpyAsync(c.scal_h + tpo::SC_VOLUME, c.scal + tpo::SC_VOLUME, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
   }
   if (dVdx) {
     tpo::launch_filter_adj_uniform(c, 1.0 / (double)c.ne, c.tmpe, c.stream);
     if (int rc = copy_out(c, dVdx, c.tmpe, c.ne, mem)) return rc;
   }
   CK(cudaStreamSynchronize(c.stream));
-  if (V) *V = c.scal_h[9] / (double)c.ne;
+  if (V) *V = c.scal_h[tpo::SC_VOLUME] / (double)c.ne;
   return finish(c, TPO_OK);
 }
 
@@ -713,18 +822,18 @@ int tpo_oc_update(tpo_ctx *ctx, double *x, const double *xmin, const double *xma
   double l1 = 0, l2 = 1e6;
   while (l2 - l1 > 1e-4) {
     const double lmid = 0.5 * (l1 + l2);
-    tpo::launch_oc_step(c, n, dx, dxold, dmin, dmax, ddf, ddg, move, lmid, c.scal + 10, c.stream);
-    CK(cudaMemcpyAsync(c.scal_h + 10, c.scal + 10, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    tpo::launch_oc_step(c, n, dx, dxold, dmin, dmax, ddf, ddg, move, lmid, c.scal + tpo::SC_OC_DG, c.stream);
+    CK(cudaMemcpyAsync(c.scal_h + tpo::SC_OC_DG, c.scal + tpo::SC_OC_DG, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
-    if (g + c.scal_h[10] > 0) l1 = lmid; else l2 = lmid;
+    if (g + c.scal_h[tpo::SC_OC_DG] > 0) l1 = lmid; else l2 = lmid;
   }
-  tpo::launch_oc_finish(c, n, dx, dxold, dmin, dmax, c.scal + 11, c.stream);
-  CK(cudaMemcpyAsync(c.scal_h + 11, c.scal + 11, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  tpo::launch_oc_finish(c, n, dx, dxold, dmin, dmax, c.scal + tpo::SC_OC_CHANGE, c.stream);
+  CK(cudaMemcpyAsync(c.scal_h + tpo::SC_OC_CHANGE, c.scal + tpo::SC_OC_CHANGE, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
   const cudaMemcpyKind ko = mem == TPO_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   CK(cudaMemcpyAsync(x, dx, sizeof(double) * n, ko, c.stream));
   CK(cudaMemcpyAsync(dfdx, ddf, sizeof(double) * n, ko, c.stream));
   CK(cudaStreamSynchronize(c.stream));
-  if (change) *change = c.scal_h[11];
+  if (change) *change = c.scal_h[tpo::SC_OC_CHANGE];
   return finish(c, TPO_OK);
 }
 

@@ -11,6 +11,8 @@ constexpr int kMaxCoarseLevels = 8;
 // levels with at most this many nodes run inside the persistent kernel
 constexpr int64_t kPersistentMaxNodes = 65536;
 
+// Every vector below holds `nb` columns (CoarseCycle::nb), column j at
+// offset j * 3 * nn; A and dinv are shared by the columns.
 template <typename T>
 struct CoarseLevel {
   int dims[3];
@@ -30,11 +32,13 @@ struct CoarseLevel {
 template <typename T>
 struct CoarseCycle {
   int nlev;                          // stencil levels handled in the kernel
+  int nb;                            // columns (1, 2, 4 or 8)
   CoarseLevel<T> lev[kMaxCoarseLevels];
   const double *Ainv;                // dense inverse of the coarsest operator
   int64_t nc;                        // coarsest dof count
   int cdims[3];                      // coarsest nodes per dimension
   T *bc, *xc;                        // coarsest right-hand side / solution
+                                     // (column stride nc)
 };
 
 template <typename T>

@@ -107,16 +107,33 @@ __device__ __forceinline__ T masked(const NodeReg<T> &r, int c) {
   return ((r.f >> c) & 1u) ? T(0) : r.v[c];
 }
 
-template <typename T, int TY, int IN, int OUT>
+// COLS: a block of columns, blockIdx.z = column * nchunk + z chunk, the
+// column selecting u, b, y, y2 (stride ld).  The single-column
+// instantiation reads the parameters in place.
+template <typename T, int TY, int IN, int OUT, bool COLS>
 __global__ void __launch_bounds__(32 * TY)
     k_apply_staged(int nelx, int nely, int nelz, int zchunk,
                    const T *__restrict__ E, const uint8_t *__restrict__ fix,
-                   const ApplyArgs<T> args, const Kh<T> kh) {
+                   const ApplyArgs<T> args_in, const Kh<T> kh) {
   const int Nx = nelx + 1, Ny = nely + 1, Nz = nelz + 1;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int gx = (int)blockIdx.x * 31 - 1 + tx;
   const int gy = (int)blockIdx.y * (TY - 1) - 1 + ty;
-  const int zs = (int)blockIdx.z * zchunk;
+  int zs;
+  ApplyArgs<T> args_col;
+  if (COLS) {
+    const int col = (int)blockIdx.z / args_in.nchunk;
+    zs = ((int)blockIdx.z - col * args_in.nchunk) * zchunk;
+    args_col = args_in;
+    const int64_t o = col * args_in.ld;
+    if (args_col.u) args_col.u += o;
+    if (args_col.b) args_col.b += o;
+    args_col.y += o;
+    if (args_col.y2) args_col.y2 += o;
+  } else {
+    zs = (int)blockIdx.z * zchunk;
+  }
+  const ApplyArgs<T> &args = COLS ? args_col : args_in;
   const int ze = min(zs + zchunk, Nz);
   const bool lane31 = (tx == 31);
   const bool lastrow = (ty == TY - 1);
@@ -290,7 +307,10 @@ size_t staged_smem() {
 
 template <typename T, int IN, int OUT>
 void set_smem_attr() {
-  cudaFuncSetAttribute(k_apply_staged<T, kTY, IN, OUT>,
+  cudaFuncSetAttribute(k_apply_staged<T, kTY, IN, OUT, false>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)staged_smem<T>());
+  cudaFuncSetAttribute(k_apply_staged<T, kTY, IN, OUT, true>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)staged_smem<T>());
 }
@@ -299,7 +319,7 @@ void set_smem_attr() {
 // chunks that fill whole waves of co-resident CTAs (a partial last wave
 // idles SMs for the length of a chunk; each chunk costs 3 extra planes)
 template <typename T>
-void staged_grid(const Ctx &c, dim3 &grid, int &zchunk) {
+void staged_grid(const Ctx &c, int nb, dim3 &grid, int &zchunk) {
   const int Nx = c.nel[0] + 1, Ny = c.nel[1] + 1, Nz = c.nel[2] + 1;
   const int gx = (Nx + 30) / 31, gy = (Ny + kTY - 2) / (kTY - 1);
   const int dev = c.device & 63;
@@ -314,13 +334,13 @@ void staged_grid(const Ctx &c, dim3 &grid, int &zchunk) {
     set_smem_attr<T, IN_U, OUT_POST1>();
     int per_sm = 0, sms = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, k_apply_staged<T, kTY, IN_CHEB, OUT_CHEB2>, 32 * kTY,
+        &per_sm, k_apply_staged<T, kTY, IN_CHEB, OUT_CHEB2, true>, 32 * kTY,
         staged_smem<T>());
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
     slots_cache[dev] = std::max(1, per_sm) * std::max(1, sms);
     attr_set |= 1ull << dev;
   }
-  const int slots = slots_cache[dev], tiles = gx * gy;
+  const int slots = slots_cache[dev], tiles = gx * gy * nb;
   int chunks = 1;
   for (int w = 1; w <= 8; ++w) {
     const int ch = (w * slots) / tiles;
@@ -333,62 +353,70 @@ void staged_grid(const Ctx &c, dim3 &grid, int &zchunk) {
   const int maxc = std::max(1, Nz / 8);   // keep >= 8 planes per chunk
   if (chunks > maxc) chunks = maxc;
   zchunk = (Nz + chunks - 1) / chunks;
-  grid = dim3(gx, gy, (Nz + zchunk - 1) / zchunk);
+  grid = dim3(gx, gy, nb * ((Nz + zchunk - 1) / zchunk));
 }
 
 template <typename T, int IN, int OUT>
-void launch_mode(const Ctx &c, const T *E, const ApplyArgs<T> &args,
-                 cudaStream_t s) {
+void launch_mode(const Ctx &c, const T *E, const ApplyArgs<T> &args_in,
+                 cudaStream_t s, int nb) {
   dim3 grid;
   int zchunk = 0;
-  staged_grid<T>(c, grid, zchunk);
+  staged_grid<T>(c, nb, grid, zchunk);
+  ApplyArgs<T> args = args_in;
+  args.ld = 3 * c.nn;
+  args.nchunk = (int)grid.z / nb;
   const Kh<T> &kh = *reinterpret_cast<const Kh<T> *>(
       sizeof(T) == 8 ? (const void *)&c.kh64 : (const void *)&c.kh32);
   count_launch();
-  k_apply_staged<T, kTY, IN, OUT><<<grid, dim3(32, kTY), staged_smem<T>(), s>>>(
-      c.nel[0], c.nel[1], c.nel[2], zchunk, E, c.fix, args, kh);
+  if (nb == 1)
+    k_apply_staged<T, kTY, IN, OUT, false><<<grid, dim3(32, kTY), staged_smem<T>(), s>>>(
+        c.nel[0], c.nel[1], c.nel[2], zchunk, E, c.fix, args, kh);
+  else
+    k_apply_staged<T, kTY, IN, OUT, true><<<grid, dim3(32, kTY), staged_smem<T>(), s>>>(
+        c.nel[0], c.nel[1], c.nel[2], zchunk, E, c.fix, args, kh);
 }
 
 }  // namespace
 
 template <typename T>
 void launch_apply_fine(const Ctx &c, const T *E, const T *u, const T *b, T *y,
-                       cudaStream_t s) {
+                       cudaStream_t s, int nb) {
   ApplyArgs<T> a{};
   a.u = u;
   a.b = b;
   a.y = y;
   if (b)
-    launch_mode<T, IN_U, OUT_RESID>(c, E, a, s);
+    launch_mode<T, IN_U, OUT_RESID>(c, E, a, s, nb);
   else
-    launch_mode<T, IN_U, OUT_Y>(c, E, a, s);
+    launch_mode<T, IN_U, OUT_Y>(c, E, a, s, nb);
 }
 
 template <typename T>
 void launch_apply_fused(const Ctx &c, const T *E, int in, int out,
-                        const ApplyArgs<T> &args, cudaStream_t s) {
+                        const ApplyArgs<T> &args, cudaStream_t s, int nb) {
   if (in == IN_CHEB && out == OUT_CHEB2)
-    launch_mode<T, IN_CHEB, OUT_CHEB2>(c, E, args, s);
+    launch_mode<T, IN_CHEB, OUT_CHEB2>(c, E, args, s, nb);
   else if (in == IN_U && out == OUT_POST0)
-    launch_mode<T, IN_U, OUT_POST0>(c, E, args, s);
+    launch_mode<T, IN_U, OUT_POST0>(c, E, args, s, nb);
   else if (in == IN_U && out == OUT_POST1)
-    launch_mode<T, IN_U, OUT_POST1>(c, E, args, s);
+    launch_mode<T, IN_U, OUT_POST1>(c, E, args, s, nb);
   else if (in == IN_U && out == OUT_RESID)
-    launch_mode<T, IN_U, OUT_RESID>(c, E, args, s);
+    launch_mode<T, IN_U, OUT_RESID>(c, E, args, s, nb);
   else
-    launch_mode<T, IN_U, OUT_Y>(c, E, args, s);
+    launch_mode<T, IN_U, OUT_Y>(c, E, args, s, nb);
 }
 
 template void launch_apply_fine<double>(const Ctx &, const double *,
                                         const double *, const double *,
-                                        double *, cudaStream_t);
+                                        double *, cudaStream_t, int);
 template void launch_apply_fine<float>(const Ctx &, const float *,
                                        const float *, const float *, float *,
-                                       cudaStream_t);
+                                       cudaStream_t, int);
 template void launch_apply_fused<double>(const Ctx &, const double *, int, int,
                                          const ApplyArgs<double> &,
-                                         cudaStream_t);
+                                         cudaStream_t, int);
 template void launch_apply_fused<float>(const Ctx &, const float *, int, int,
-                                        const ApplyArgs<float> &, cudaStream_t);
+                                        const ApplyArgs<float> &, cudaStream_t,
+                                        int);
 
 }  // namespace tpo

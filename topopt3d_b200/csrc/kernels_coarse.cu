@@ -7,7 +7,9 @@
 // stays resident (one cooperative launch sized to the co-resident block
 // count) and the phases are separated by grid-wide barriers
 // (cooperative_groups grid sync, valid because the launch guarantees
-// co-residency).  Each phase is a grid-stride loop over nodes.
+// co-residency).  Each phase is a grid-stride loop over nodes.  A block of
+// NB right-hand sides rides through the same barriers: the stencil of a
+// node is read once for all NB columns.
 //
 // Per level (Chebyshev degree m, Jacobi): the stencil apply and the
 // Chebyshev update of a node are fused into one phase by ping-ponging the
@@ -23,26 +25,33 @@
 #include "coarse.h"
 #include "transfer.cuh"
 
-namespace cg = cooperative_groups;
-
 namespace tpo {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
-// y_n = sum_delta A(n, n+delta) u_{n+delta} for one node by one warp: lane
-// `nb` < 27 loads block nb (9 contiguous values of the node-major copy,
-// so the warp reads 243 consecutive values) and the neighbour's u, then the
-// three partial sums are reduced across the warp.  Out-of-range neighbours
-// have zero blocks; their index is clamped so every load stays in bounds.
-// Every lane returns the full sums.
+// y_n = sum_delta A(n, n+delta) u_{n+delta} for one node by one warp, for
+// NB columns: lane `q` < 27 loads block q (9 contiguous values of the
+// node-major copy, so the warp reads 243 consecutive values) and the
+// neighbour's u of every column.  The 3 NB partial sums are then reduced
+// across the warp by a reduce-scatter: at each of the first log2(NB)
+// butterfly steps a lane keeps half of its columns and sends the other
+// half, so that afterwards the lanes of group col = lane / (32 / NB) hold
+// column col; the remaining steps complete the sums inside each group.
+// Out-of-range neighbours have zero blocks; their index is clamped so every
+// load stays in bounds.
 // FROM_B: the input is the Chebyshev start d0 = inv_theta D^-1 b, formed
 // on the fly from b and D^-1 instead of being read from u
-template <typename T, bool FROM_B = false>
+template <typename T, int NB, bool FROM_B = false>
 __device__ __forceinline__ void warp_stencil(const CoarseLevel<T> &L, int n,
                                              const T *__restrict__ u, int lane,
                                              T acc[3]) {
   const int nx = L.dims[0], ny = L.dims[1], nz = L.dims[2];
-  T p0 = T(0), p1 = T(0), p2 = T(0);
+  const int64_t ld = 3 * L.nn;
+  T p[NB][3];
+#pragma unroll
+  for (int c = 0; c < NB; ++c) p[c][0] = p[c][1] = p[c][2] = T(0);
   if (lane < 27) {
     const int i = n % nx, j = (n / nx) % ny, k = n / (nx * ny);
     const int mi = min(max(i + lane % 3 - 1, 0), nx - 1);
@@ -50,56 +59,101 @@ __device__ __forceinline__ void warp_stencil(const CoarseLevel<T> &L, int n,
     const int mk = min(max(k + lane / 9 - 1, 0), nz - 1);
     const int m = (mk * ny + mj) * nx + mi;
     const T *s = L.A + (int64_t)n * 243 + lane * 9;
-    T u0, u1, u2;
-    if (FROM_B) {
-      u0 = L.inv_theta * (L.dinv[3 * m] * L.b[3 * m]);
-      u1 = L.inv_theta * (L.dinv[3 * m + 1] * L.b[3 * m + 1]);
-      u2 = L.inv_theta * (L.dinv[3 * m + 2] * L.b[3 * m + 2]);
-    } else {
-      u0 = u[3 * m];
-      u1 = u[3 * m + 1];
-      u2 = u[3 * m + 2];
-    }
-    p0 = s[0] * u0 + s[1] * u1 + s[2] * u2;
-    p1 = s[3] * u0 + s[4] * u1 + s[5] * u2;
-    p2 = s[6] * u0 + s[7] * u1 + s[8] * u2;
-  }
+    T a[9];
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    p0 += __shfl_xor_sync(0xffffffffu, p0, o);
-    p1 += __shfl_xor_sync(0xffffffffu, p1, o);
-    p2 += __shfl_xor_sync(0xffffffffu, p2, o);
+    for (int q = 0; q < 9; ++q) a[q] = s[q];
+    T di0 = T(0), di1 = T(0), di2 = T(0);
+    if (FROM_B) {
+      di0 = L.inv_theta * L.dinv[3 * m];
+      di1 = L.inv_theta * L.dinv[3 * m + 1];
+      di2 = L.inv_theta * L.dinv[3 * m + 2];
+    }
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+      T u0, u1, u2;
+      if (FROM_B) {
+        const T *bc = L.b + c * ld;
+        u0 = di0 * bc[3 * m];
+        u1 = di1 * bc[3 * m + 1];
+        u2 = di2 * bc[3 * m + 2];
+      } else {
+        const T *uc = u + c * ld;
+        u0 = uc[3 * m];
+        u1 = uc[3 * m + 1];
+        u2 = uc[3 * m + 2];
+      }
+      p[c][0] = a[0] * u0 + a[1] * u1 + a[2] * u2;
+      p[c][1] = a[3] * u0 + a[4] * u1 + a[5] * u2;
+      p[c][2] = a[6] * u0 + a[7] * u1 + a[8] * u2;
+    }
   }
-  acc[0] = p0;
-  acc[1] = p1;
-  acc[2] = p2;
+  // reduce-scatter over the columns
+  int o = 16;
+#pragma unroll
+  for (int half = NB / 2; half >= 1; half /= 2, o >>= 1) {
+    const bool upper = (lane & o) != 0;
+#pragma unroll
+    for (int c = 0; c < half; ++c)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const T send = upper ? p[c][q] : p[c + half][q];
+        const T keep = upper ? p[c + half][q] : p[c][q];
+        p[c][q] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+      }
+  }
+  for (; o > 0; o >>= 1)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) p[0][q] += __shfl_xor_sync(0xffffffffu, p[0][q], o);
+  acc[0] = p[0][0];
+  acc[1] = p[0][1];
+  acc[2] = p[0][2];
 }
 
+// lanes per column group after warp_stencil, and the (column, component)
+// a lane writes: lanes with comp < 3 write
+template <int NB>
+struct LaneMap {
+  static constexpr int G = 32 / NB;
+  int col, comp;
+  __device__ explicit LaneMap(int lane) : col(lane / G), comp(lane % G) {}
+};
+
 template <typename T>
-__global__ void __launch_bounds__(kCoarseThreads)
+__device__ __forceinline__ T pick(const T a[3], int q) {
+  return q == 0 ? a[0] : (q == 1 ? a[1] : a[2]);
+}
+
+// at least 2 co-resident blocks per SM (<= 128 registers) for every width:
+// the phases are latency-bound and need the warps
+template <typename T, int NB>
+__global__ void __launch_bounds__(kCoarseThreads, NB == 1 ? 3 : 2)
     k_coarse_cycle(CoarseCycle<T> P) {
   cg::grid_group grid = cg::this_grid();
   const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
   const int lane = threadIdx.x & 31;
   const int gwarp = (int)(tid >> 5), nwarps = (int)(nthr >> 5);
+  const LaneMap<NB> lm(lane);
+  const bool writer = lm.comp < 3;
 
   // ---------------- down-sweep: pre-smooth, residual, restrict
   for (int l = 0; l < P.nlev; ++l) {
     CoarseLevel<T> &L = P.lev[l];
     const int nn = (int)L.nn;
+    const int64_t ld = 3 * L.nn;
     T *dc = L.d0, *dn = L.d1;
     if (L.deg >= 2) {
       // start (d0 = inv_theta D^-1 b, x = d0) fused with the first step
       for (int n = gwarp; n < nn; n += nwarps) {
         T a[3];
-        warp_stencil<T, true>(L, n, nullptr, lane, a);
-        if (lane < 3) {
-          const int64_t i = 3 * (int64_t)n + lane;
-          const T di = L.dinv[i];
+        warp_stencil<T, NB, true>(L, n, nullptr, lane, a);
+        if (writer) {
+          const int64_t e = 3 * (int64_t)n + lm.comp;
+          const int64_t i = lm.col * ld + e;
+          const T di = L.dinv[e];
           const T r0 = di * L.b[i];
           const T d0 = r0 * L.inv_theta;
-          const T r = r0 - di * a[lane];
+          const T r = r0 - di * pick(a, lm.comp);
           const T d = L.c1[1] * d0 + L.c2[1] * r;
           L.r[i] = r;
           dn[i] = d;
@@ -109,17 +163,18 @@ __global__ void __launch_bounds__(kCoarseThreads)
       grid.sync();
       T *t = dc; dc = dn; dn = t;
     } else {
-      for (int64_t i = tid; i < 3 * (int64_t)nn; i += nthr)
-        L.xpre[i] = L.inv_theta * (L.dinv[i] * L.b[i]);
+      for (int64_t i = tid; i < NB * ld; i += nthr)
+        L.xpre[i] = L.inv_theta * (L.dinv[i % ld] * L.b[i]);
       grid.sync();
     }
     for (int k = 2; k < L.deg; ++k) {
       for (int n = gwarp; n < nn; n += nwarps) {
         T a[3];
-        warp_stencil(L, n, dc, lane, a);
-        if (lane < 3) {
-          const int64_t i = 3 * (int64_t)n + lane;
-          const T r = L.r[i] - L.dinv[i] * a[lane];
+        warp_stencil<T, NB>(L, n, dc, lane, a);
+        if (writer) {
+          const int64_t e = 3 * (int64_t)n + lm.comp;
+          const int64_t i = lm.col * ld + e;
+          const T r = L.r[i] - L.dinv[e] * pick(a, lm.comp);
           const T d = L.c1[k] * dc[i] + L.c2[k] * r;
           L.r[i] = r;
           dn[i] = d;
@@ -131,8 +186,11 @@ __global__ void __launch_bounds__(kCoarseThreads)
     }
     for (int n = gwarp; n < nn; n += nwarps) {
       T a[3];
-      warp_stencil(L, n, L.xpre, lane, a);
-      if (lane < 3) L.res[3 * (int64_t)n + lane] = L.b[3 * (int64_t)n + lane] - a[lane];
+      warp_stencil<T, NB>(L, n, L.xpre, lane, a);
+      if (writer) {
+        const int64_t i = lm.col * ld + 3 * (int64_t)n + lm.comp;
+        L.res[i] = L.b[i] - pick(a, lm.comp);
+      }
     }
     grid.sync();
     // b_child = P^T res
@@ -145,19 +203,43 @@ __global__ void __launch_bounds__(kCoarseThreads)
     const int64_t nnc = (int64_t)cx * cy * cz;
     for (int I = (int)tid; I < (int)nnc; I += (int)nthr) {
       const int ix = I % cx, iy = (I / cx) % cy, iz = I / (cx * cy);
-      T s[3];
-      restrict_node(fx, fy, fz, ix, iy, iz, L.res, s);
-      bc[3 * I] = s[0];
-      bc[3 * I + 1] = s[1];
-      bc[3 * I + 2] = s[2];
+#pragma unroll 1
+      for (int c = 0; c < NB; ++c) {
+        T s[3];
+        restrict_node(fx, fy, fz, ix, iy, iz, L.res + c * ld, s);
+        T *o = bc + c * 3 * nnc;
+        o[3 * I] = s[0];
+        o[3 * I + 1] = s[1];
+        o[3 * I + 2] = s[2];
+      }
     }
     grid.sync();
   }
 
   // ---------------- coarsest: x = Ainv b, a warp per row, FP64 accumulation
-  for (int row = gwarp; row < (int)P.nc; row += nwarps) {
+  for (int row = gwarp; row < (int)P.nc && NB == 1; row += nwarps) {
     const double s = gemv_row(P.Ainv + (int64_t)row * P.nc, P.bc, P.nc, lane);
     if (lane == 0) P.xc[row] = static_cast<T>(s);
+  }
+  for (int row = gwarp; row < (int)P.nc && NB > 1; row += nwarps) {
+    const double *a = P.Ainv + (int64_t)row * P.nc;
+    double s[NB];
+#pragma unroll
+    for (int c = 0; c < NB; ++c) s[c] = 0.0;
+    for (int64_t k = lane; k < P.nc; k += 32) {
+      const double av = a[k];
+#pragma unroll
+      for (int c = 0; c < NB; ++c)
+        s[c] += av * static_cast<double>(P.bc[c * P.nc + k]);
+    }
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s[c] += __shfl_xor_sync(0xffffffffu, s[c], o);
+    }
+#pragma unroll
+    for (int c = 0; c < NB; ++c)
+      if (lane == c) P.xc[c * P.nc + row] = static_cast<T>(s[c]);
   }
   grid.sync();
 
@@ -165,27 +247,34 @@ __global__ void __launch_bounds__(kCoarseThreads)
   for (int l = P.nlev - 1; l >= 0; --l) {
     CoarseLevel<T> &L = P.lev[l];
     const int nn = (int)L.nn;
+    const int64_t ld = 3 * L.nn;
     const bool dense_child = (l + 1 == P.nlev);
     const T *xc = dense_child ? P.xc : P.lev[l + 1].xout;
     const int cx = dense_child ? P.cdims[0] : P.lev[l + 1].dims[0];
     const int cy = dense_child ? P.cdims[1] : P.lev[l + 1].dims[1];
     const int cz = dense_child ? P.cdims[2] : P.lev[l + 1].dims[2];
+    const int64_t ldc = 3 * (int64_t)cx * cy * cz;
     const int fx = L.dims[0], fy = L.dims[1], fz = L.dims[2];
     for (int f = (int)tid; f < nn; f += (int)nthr) {
       const int gx = f % fx, gy = (f / fx) % fy, gz = f / (fx * fy);
-      T s[3];
-      prolong_node(fx, fy, fz, cx, cy, cz, gx, gy, gz, xc, s);
-      L.xpre[3 * f] += s[0];
-      L.xpre[3 * f + 1] += s[1];
-      L.xpre[3 * f + 2] += s[2];
+#pragma unroll 1
+      for (int c = 0; c < NB; ++c) {
+        T s[3];
+        prolong_node(fx, fy, fz, cx, cy, cz, gx, gy, gz, xc + c * ldc, s);
+        T *x = L.xpre + c * ld;
+        x[3 * f] += s[0];
+        x[3 * f + 1] += s[1];
+        x[3 * f + 2] += s[2];
+      }
     }
     grid.sync();
     for (int n = gwarp; n < nn; n += nwarps) {
       T a[3];
-      warp_stencil(L, n, L.xpre, lane, a);
-      if (lane < 3) {
-        const int64_t i = 3 * (int64_t)n + lane;
-        const T r = L.dinv[i] * (L.b[i] - a[lane]);
+      warp_stencil<T, NB>(L, n, L.xpre, lane, a);
+      if (writer) {
+        const int64_t e = 3 * (int64_t)n + lm.comp;
+        const int64_t i = lm.col * ld + e;
+        const T r = L.dinv[e] * (L.b[i] - pick(a, lm.comp));
         const T d = r * L.inv_theta;
         L.r[i] = r;
         L.d0[i] = d;
@@ -197,10 +286,11 @@ __global__ void __launch_bounds__(kCoarseThreads)
     for (int k = 1; k < L.deg; ++k) {
       for (int n = gwarp; n < nn; n += nwarps) {
         T a[3];
-        warp_stencil(L, n, dc, lane, a);
-        if (lane < 3) {
-          const int64_t i = 3 * (int64_t)n + lane;
-          const T r = L.r[i] - L.dinv[i] * a[lane];
+        warp_stencil<T, NB>(L, n, dc, lane, a);
+        if (writer) {
+          const int64_t e = 3 * (int64_t)n + lm.comp;
+          const int64_t i = lm.col * ld + e;
+          const T r = L.r[i] - L.dinv[e] * pick(a, lm.comp);
           const T d = L.c1[k] * dc[i] + L.c2[k] * r;
           L.r[i] = r;
           dn[i] = d;
@@ -213,7 +303,7 @@ __global__ void __launch_bounds__(kCoarseThreads)
   }
 }
 
-template <typename T>
+template <typename T, int NB>
 int grid_size_for() {
   static int cached[64] = {0};
   int dev = 0;
@@ -221,7 +311,7 @@ int grid_size_for() {
   dev &= 63;
   if (!cached[dev]) {
     int per_sm = 0, sms = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_coarse_cycle<T>,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_coarse_cycle<T, NB>,
                                                   kCoarseThreads, 0);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cached[dev] = std::max(1, std::min(per_sm, 4)) * sms;
@@ -229,15 +319,26 @@ int grid_size_for() {
   return cached[dev];
 }
 
+template <typename T, int NB>
+cudaError_t launch_nb(const CoarseCycle<T> &P, cudaStream_t s) {
+  const int grid = grid_size_for<T, NB>();
+  void *args[] = {const_cast<CoarseCycle<T> *>(&P)};
+  return cudaLaunchCooperativeKernel((const void *)k_coarse_cycle<T, NB>, grid,
+                                     kCoarseThreads, args, 0, s);
+}
+
 }  // namespace
 
 template <typename T>
 cudaError_t launch_coarse_cycle(const CoarseCycle<T> &P, cudaStream_t s) {
   count_launch();
-  const int grid = grid_size_for<T>();
-  void *args[] = {const_cast<CoarseCycle<T> *>(&P)};
-  return cudaLaunchCooperativeKernel((const void *)k_coarse_cycle<T>, grid,
-                                     kCoarseThreads, args, 0, s);
+  switch (P.nb) {
+    case 1: return launch_nb<T, 1>(P, s);
+    case 2: return launch_nb<T, 2>(P, s);
+    case 4: return launch_nb<T, 4>(P, s);
+    case 8: return launch_nb<T, 8>(P, s);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 template cudaError_t launch_coarse_cycle<double>(const CoarseCycle<double> &,

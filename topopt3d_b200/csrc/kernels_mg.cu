@@ -13,6 +13,8 @@
 // Coarse operators are A_{l+1} = P^T A_l P (PCMG Galerkin,
 // FEAnalysis.cpp:412), stored as 27-point 3x3-block stencils in SoA form
 // S[(nb*9 + 3r + s) * nn + node].
+#include <algorithm>
+
 #include "tpo_internal.h"
 #include "transfer.cuh"
 
@@ -152,16 +154,20 @@ __global__ void k_stencil_to_half(int64_t nn, const double *__restrict__ S,
   }
 }
 
-template <typename T, bool RESID>
+// NB columns (stride ld) share every coefficient load
+template <typename T, bool RESID, int NB>
 __global__ void k_apply_stencil_sym(int nx, int ny, int nz,
                                     const T *__restrict__ H,
                                     const T *__restrict__ u,
-                                    const T *__restrict__ b, T *__restrict__ y) {
+                                    const T *__restrict__ b, T *__restrict__ y,
+                                    int64_t ld) {
   const int nn = nx * ny * nz;
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nn;
        n += gridDim.x * blockDim.x) {
     const int i = n % nx, j = (n / nx) % ny, k = n / (nx * ny);
-    T a0 = 0, a1 = 0, a2 = 0;
+    T a[NB][3];
+#pragma unroll
+    for (int col = 0; col < NB; ++col) a[col][0] = a[col][1] = a[col][2] = T(0);
 #pragma unroll
     for (int h = 0; h < 14; ++h) {
       const int nb = 13 + h;
@@ -171,11 +177,18 @@ __global__ void k_apply_stencil_sym(int nx, int ny, int nz,
         const int mi = min(i + di, nx - 1), mj = min(max(j + dj, 0), ny - 1),
                   mk = min(k + dk, nz - 1);
         const int m = (mk * ny + mj) * nx + max(mi, 0);
-        const T u0 = u[3 * m], u1 = u[3 * m + 1], u2 = u[3 * m + 2];
-        const T *s = H + (int64_t)h * 9 * nn + n;
-        a0 += s[0] * u0 + s[nn] * u1 + s[2 * (int64_t)nn] * u2;
-        a1 += s[3 * (int64_t)nn] * u0 + s[4 * (int64_t)nn] * u1 + s[5 * (int64_t)nn] * u2;
-        a2 += s[6 * (int64_t)nn] * u0 + s[7 * (int64_t)nn] * u1 + s[8 * (int64_t)nn] * u2;
+        const T *sp = H + (int64_t)h * 9 * nn + n;
+        T c[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) c[q] = sp[q * (int64_t)nn];
+#pragma unroll
+        for (int col = 0; col < NB; ++col) {
+          const T *uc = u + col * ld;
+          const T u0 = uc[3 * m], u1 = uc[3 * m + 1], u2 = uc[3 * m + 2];
+          a[col][0] += c[0] * u0 + c[1] * u1 + c[2] * u2;
+          a[col][1] += c[3] * u0 + c[4] * u1 + c[5] * u2;
+          a[col][2] += c[6] * u0 + c[7] * u1 + c[8] * u2;
+        }
       }
       // backward block A(n, n-d) = A(n-d, n)^T, stored by node n-d
       if (h > 0) {
@@ -183,21 +196,30 @@ __global__ void k_apply_stencil_sym(int nx, int ny, int nz,
         const bool in = mi >= 0 && mi < nx && mj >= 0 && mj < ny && mk >= 0 && mk < nz;
         const int m = in ? (mk * ny + mj) * nx + mi : n;
         const T w = in ? T(1) : T(0);
-        const T u0 = w * u[3 * m], u1 = w * u[3 * m + 1], u2 = w * u[3 * m + 2];
-        const T *s = H + (int64_t)h * 9 * nn + m;
-        a0 += s[0] * u0 + s[3 * (int64_t)nn] * u1 + s[6 * (int64_t)nn] * u2;
-        a1 += s[nn] * u0 + s[4 * (int64_t)nn] * u1 + s[7 * (int64_t)nn] * u2;
-        a2 += s[2 * (int64_t)nn] * u0 + s[5 * (int64_t)nn] * u1 + s[8 * (int64_t)nn] * u2;
+        const T *sp = H + (int64_t)h * 9 * nn + m;
+        T c[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) c[q] = sp[q * (int64_t)nn];
+#pragma unroll
+        for (int col = 0; col < NB; ++col) {
+          const T *uc = u + col * ld;
+          const T u0 = w * uc[3 * m], u1 = w * uc[3 * m + 1], u2 = w * uc[3 * m + 2];
+          a[col][0] += c[0] * u0 + c[3] * u1 + c[6] * u2;
+          a[col][1] += c[1] * u0 + c[4] * u1 + c[7] * u2;
+          a[col][2] += c[2] * u0 + c[5] * u1 + c[8] * u2;
+        }
       }
     }
-    if (RESID) {
-      a0 = b[3 * n] - a0;
-      a1 = b[3 * n + 1] - a1;
-      a2 = b[3 * n + 2] - a2;
+#pragma unroll
+    for (int col = 0; col < NB; ++col) {
+      T *yc = y + col * ld;
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        T v = a[col][q];
+        if (RESID) v = b[col * ld + 3 * n + q] - v;
+        yc[3 * n + q] = v;
+      }
     }
-    y[3 * n] = a0;
-    y[3 * n + 1] = a1;
-    y[3 * n + 2] = a2;
   }
 }
 
@@ -213,35 +235,43 @@ __global__ void k_stencil_diag(int64_t nn, const double *__restrict__ S,
   }
 }
 
-// b_c = P^T r_f
+// b_c = P^T r_f for nb columns (fine stride 3 nnf, coarse stride 3 nnc)
 template <typename T>
 __global__ void k_restrict(int fx, int fy, int fz, int cx, int cy, int cz,
-                           const T *__restrict__ rf, T *__restrict__ bc) {
-  const int64_t nnc = (int64_t)cx * cy * cz;
+                           const T *__restrict__ rf, T *__restrict__ bc,
+                           int nb) {
+  const int64_t nnc = (int64_t)cx * cy * cz, nnf = (int64_t)fx * fy * fz;
   for (int64_t I = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; I < nnc;
        I += (int64_t)gridDim.x * blockDim.x) {
     const int ix = I % cx, iy = (I / cx) % cy, iz = I / ((int64_t)cx * cy);
-    T s[3];
-    restrict_node(fx, fy, fz, ix, iy, iz, rf, s);
-    bc[3 * I] = s[0];
-    bc[3 * I + 1] = s[1];
-    bc[3 * I + 2] = s[2];
+    for (int col = 0; col < nb; ++col) {
+      T s[3];
+      restrict_node(fx, fy, fz, ix, iy, iz, rf + col * 3 * nnf, s);
+      T *o = bc + col * 3 * nnc;
+      o[3 * I] = s[0];
+      o[3 * I + 1] = s[1];
+      o[3 * I + 2] = s[2];
+    }
   }
 }
 
-// x_f += P x_c
+// x_f += P x_c for nb columns
 template <typename T>
 __global__ void k_prolong_add(int fx, int fy, int fz, int cx, int cy, int cz,
-                              const T *__restrict__ xc, T *__restrict__ xf) {
-  const int64_t nnf = (int64_t)fx * fy * fz;
+                              const T *__restrict__ xc, T *__restrict__ xf,
+                              int nb) {
+  const int64_t nnf = (int64_t)fx * fy * fz, nnc = (int64_t)cx * cy * cz;
   for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < nnf;
        f += (int64_t)gridDim.x * blockDim.x) {
     const int gx = f % fx, gy = (f / fx) % fy, gz = f / ((int64_t)fx * fy);
-    T s[3];
-    prolong_node(fx, fy, fz, cx, cy, cz, gx, gy, gz, xc, s);
-    xf[3 * f] += s[0];
-    xf[3 * f + 1] += s[1];
-    xf[3 * f + 2] += s[2];
+    for (int col = 0; col < nb; ++col) {
+      T s[3];
+      prolong_node(fx, fy, fz, cx, cy, cz, gx, gy, gz, xc + col * 3 * nnc, s);
+      T *o = xf + col * 3 * nnf;
+      o[3 * f] += s[0];
+      o[3 * f + 1] += s[1];
+      o[3 * f + 2] += s[2];
+    }
   }
 }
 
@@ -276,12 +306,17 @@ __global__ void k_coarse_gemv(int64_t n, const double *__restrict__ A,
 }
 
 // Chebyshev start: r = D^-1 (b or the residual already in r), d = r/theta,
-// x (+)= d
+// x (+)= d; column blockIdx.y (stride n), D^-1 shared
 template <typename T>
 __global__ void k_cheb_init(int64_t n, const T *__restrict__ dinv,
                             const T *__restrict__ b, T *__restrict__ r,
                             T *__restrict__ d, T *__restrict__ x, T inv_theta,
                             bool zero_guess) {
+  const int64_t o = blockIdx.y * n;
+  if (zero_guess) b += o;
+  r += o;
+  d += o;
+  x += o;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const T ri = dinv[i] * (zero_guess ? b[i] : r[i]);
@@ -292,11 +327,16 @@ __global__ void k_cheb_init(int64_t n, const T *__restrict__ dinv,
   }
 }
 
-// r -= D^-1 A d ; d = c1 d + c2 r ; x += d
+// r -= D^-1 A d ; d = c1 d + c2 r ; x += d; column blockIdx.y
 template <typename T>
 __global__ void k_cheb_step(int64_t n, const T *__restrict__ dinv,
                             const T *__restrict__ Ad, T *__restrict__ r,
                             T *__restrict__ d, T *__restrict__ x, T c1, T c2) {
+  const int64_t o = blockIdx.y * n;
+  Ad += o;
+  r += o;
+  d += o;
+  x += o;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const T ri = r[i] - dinv[i] * Ad[i];
@@ -328,24 +368,48 @@ template void launch_apply_stencil<float>(const Level &, const float *,
                                           const float *, const float *, float *,
                                           cudaStream_t);
 
+template <typename T, bool RESID, int NB>
+void sym_launch(const Level &v, const T *H, const T *u, const T *b, T *y,
+                cudaStream_t s) {
+  count_launch();
+  // one thread per node carries NB columns: a wider column block needs
+  // fewer threads in flight for the same bytes
+  const int g = grid_for(v.nn, 128);
+  k_apply_stencil_sym<T, RESID, NB><<<g, 128, 0, s>>>(
+      v.dims[0], v.dims[1], v.dims[2], H, u, b, y, 3 * v.nn);
+}
+
+template <typename T, bool RESID>
+void sym_dispatch(const Level &v, const T *H, const T *u, const T *b, T *y,
+                  cudaStream_t s, int nb) {
+  const int64_t ld = 3 * v.nn;
+  while (nb > 0) {
+    const int w = nb >= 8 ? 8 : nb >= 4 ? 4 : nb >= 2 ? 2 : 1;
+    if (w == 8) sym_launch<T, RESID, 8>(v, H, u, b, y, s);
+    else if (w == 4) sym_launch<T, RESID, 4>(v, H, u, b, y, s);
+    else if (w == 2) sym_launch<T, RESID, 2>(v, H, u, b, y, s);
+    else sym_launch<T, RESID, 1>(v, H, u, b, y, s);
+    u += w * ld;
+    if (b) b += w * ld;
+    y += w * ld;
+    nb -= w;
+  }
+}
+
 template <typename T>
 void launch_apply_stencil_sym(const Level &v, const T *H, const T *u,
-                              const T *b, T *y, cudaStream_t s) {
-  count_launch();
-  const int g = grid_for(v.nn, 128);
+                              const T *b, T *y, cudaStream_t s, int nb) {
   if (b)
-    k_apply_stencil_sym<T, true><<<g, 128, 0, s>>>(v.dims[0], v.dims[1],
-                                                   v.dims[2], H, u, b, y);
+    sym_dispatch<T, true>(v, H, u, b, y, s, nb);
   else
-    k_apply_stencil_sym<T, false><<<g, 128, 0, s>>>(v.dims[0], v.dims[1],
-                                                    v.dims[2], H, u, b, y);
+    sym_dispatch<T, false>(v, H, u, b, y, s, nb);
 }
 template void launch_apply_stencil_sym<double>(const Level &, const double *,
                                                const double *, const double *,
-                                               double *, cudaStream_t);
+                                               double *, cudaStream_t, int);
 template void launch_apply_stencil_sym<float>(const Level &, const float *,
                                               const float *, const float *,
-                                              float *, cudaStream_t);
+                                              float *, cudaStream_t, int);
 
 void launch_stencil_to_half(int64_t nn, const double *S, double *H64,
                             float *H32, cudaStream_t s) {
@@ -369,30 +433,32 @@ void launch_stencil_diag(const Level &v, const double *S, double *dinv64,
 
 template <typename T>
 void launch_restrict(const Level &fine, const Level &coarse, const T *rf,
-                     T *bc, cudaStream_t s) {
+                     T *bc, cudaStream_t s, int nb) {
   count_launch();
   k_restrict<T><<<grid_for(coarse.nn, 128), 128, 0, s>>>(
       fine.dims[0], fine.dims[1], fine.dims[2], coarse.dims[0], coarse.dims[1],
-      coarse.dims[2], rf, bc);
+      coarse.dims[2], rf, bc, nb);
 }
 template void launch_restrict<double>(const Level &, const Level &,
-                                      const double *, double *, cudaStream_t);
+                                      const double *, double *, cudaStream_t,
+                                      int);
 template void launch_restrict<float>(const Level &, const Level &,
-                                     const float *, float *, cudaStream_t);
+                                     const float *, float *, cudaStream_t, int);
 
 template <typename T>
 void launch_prolong_add(const Level &fine, const Level &coarse, const T *xc,
-                        T *xf, cudaStream_t s) {
+                        T *xf, cudaStream_t s, int nb) {
   count_launch();
   k_prolong_add<T><<<grid_for(fine.nn, 128), 128, 0, s>>>(
       fine.dims[0], fine.dims[1], fine.dims[2], coarse.dims[0], coarse.dims[1],
-      coarse.dims[2], xc, xf);
+      coarse.dims[2], xc, xf, nb);
 }
 template void launch_prolong_add<double>(const Level &, const Level &,
                                          const double *, double *,
-                                         cudaStream_t);
+                                         cudaStream_t, int);
 template void launch_prolong_add<float>(const Level &, const Level &,
-                                        const float *, float *, cudaStream_t);
+                                        const float *, float *, cudaStream_t,
+                                        int);
 
 void launch_to_dense(const Level &v, const double *S, double *A,
                      cudaStream_t s) {
@@ -438,46 +504,56 @@ void launch_eye(int64_t n, double *A, cudaStream_t s) {
 
 template <typename T>
 void launch_coarse_gemv(int64_t n, const double *Ainv, const T *b, T *x,
-                        cudaStream_t s) {
-  count_launch();
+                        cudaStream_t s, int nb) {
   const int64_t warps = n;
   const int threads = 256;
   int64_t blocks = (warps * 32 + threads - 1) / threads;
   if (blocks > 148 * 8) blocks = 148 * 8;
-  k_coarse_gemv<T><<<(int)blocks, threads, 0, s>>>(n, Ainv, b, x);
+  for (int col = 0; col < nb; ++col) {
+    count_launch();
+    k_coarse_gemv<T><<<(int)blocks, threads, 0, s>>>(n, Ainv, b + col * n,
+                                                     x + col * n);
+  }
 }
 template void launch_coarse_gemv<double>(int64_t, const double *,
                                          const double *, double *,
-                                         cudaStream_t);
+                                         cudaStream_t, int);
 template void launch_coarse_gemv<float>(int64_t, const double *, const float *,
-                                        float *, cudaStream_t);
+                                        float *, cudaStream_t, int);
+
+static dim3 col_grid(int64_t n, int nb) {
+  int g = grid_for(n, 256);
+  if (nb > 1) g = std::max(148, g / nb);
+  return dim3(g, nb);
+}
 
 template <typename T>
 void launch_cheb_init(int64_t n, const T *dinv, const T *b, T *r, T *d, T *x,
-                      double inv_theta, bool zero_guess, cudaStream_t s) {
+                      double inv_theta, bool zero_guess, cudaStream_t s,
+                      int nb) {
   count_launch();
-  k_cheb_init<T><<<grid_for(n, 256), 256, 0, s>>>(
+  k_cheb_init<T><<<col_grid(n, nb), 256, 0, s>>>(
       n, dinv, b, r, d, x, static_cast<T>(inv_theta), zero_guess);
 }
 template void launch_cheb_init<double>(int64_t, const double *, const double *,
                                        double *, double *, double *, double,
-                                       bool, cudaStream_t);
+                                       bool, cudaStream_t, int);
 template void launch_cheb_init<float>(int64_t, const float *, const float *,
                                       float *, float *, float *, double, bool,
-                                      cudaStream_t);
+                                      cudaStream_t, int);
 
 template <typename T>
 void launch_cheb_step(int64_t n, const T *dinv, const T *Ad, T *r, T *d, T *x,
-                      double c1, double c2, cudaStream_t s) {
+                      double c1, double c2, cudaStream_t s, int nb) {
   count_launch();
-  k_cheb_step<T><<<grid_for(n, 256), 256, 0, s>>>(
+  k_cheb_step<T><<<col_grid(n, nb), 256, 0, s>>>(
       n, dinv, Ad, r, d, x, static_cast<T>(c1), static_cast<T>(c2));
 }
 template void launch_cheb_step<double>(int64_t, const double *, const double *,
                                        double *, double *, double *, double,
-                                       double, cudaStream_t);
+                                       double, cudaStream_t, int);
 template void launch_cheb_step<float>(int64_t, const float *, const float *,
                                       float *, float *, float *, double, double,
-                                      cudaStream_t);
+                                      cudaStream_t, int);
 
 }  // namespace tpo

@@ -3,6 +3,8 @@
 // each in a fixed order, and the last block to finish (ticket counter) sums
 // the partials in a fixed tree order and writes the result to a device
 // scalar, so the CG recurrences never round-trip through the host.
+#include <algorithm>
+
 #include "tpo_internal.h"
 
 namespace tpo {
@@ -34,7 +36,9 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
   return v;   // valid in thread 0
 }
 
-// partial -> last block -> *out (previous *out moved to *shift_to if set)
+// partial -> last block -> *out (previous *out moved to *shift_to if set).
+// Column j of a block reduction owns blocks (*, j): part + j * gridDim.x
+// and ticket + j.
 __device__ __forceinline__ void finish_reduction(double v, double *part,
                                                  unsigned int *ticket,
                                                  double *out, double *shift_to) {
@@ -60,45 +64,67 @@ __device__ __forceinline__ void finish_reduction(double v, double *part,
   }
 }
 
+// a.b per column (blockIdx.y)
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads)
     k_dot(int64_t n, const T *__restrict__ a, const T *__restrict__ b,
           double *part, unsigned int *ticket, double *out, double *shift_to) {
+  const int j = blockIdx.y;
+  a += j * n;
+  b += j * n;
   double s = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
     s += static_cast<double>(a[i]) * static_cast<double>(b[i]);
-  finish_reduction(s, part, ticket, out, shift_to);
+  finish_reduction(s, part + j * gridDim.x, ticket + j, out + j * kColScal,
+                   shift_to ? shift_to + j * kColScal : nullptr);
 }
 
-// p = z (first) or p = z + (rho / rho_old) p
+// p = z (first) or p = z + (rho / rho_old) p, per column; a frozen column
+// keeps its p
 template <typename T>
 __global__ void k_cg_p(int64_t n, const T *__restrict__ z, T *__restrict__ p,
                        const double *__restrict__ scal, bool first) {
-  const T beta = first ? T(0) : static_cast<T>(scal[0] / scal[1]);
+  const int j = blockIdx.y;
+  const double *sc = scal + j * kColScal;
+  if (sc[6] != 0.0) return;
+  z += j * n;
+  p += j * n;
+  const T beta = first ? T(0) : static_cast<T>(sc[0] / sc[1]);
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
     p[i] = first ? z[i] : z[i] + beta * p[i];
 }
 
-// x += alpha p ; r -= alpha q ; rr = r.r   with alpha = rho / (p.q)
+// x += alpha p ; r -= alpha q ; rr = r.r   with alpha = rho / (p.q), per
+// column; a frozen column only recomputes rr
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads)
     k_cg_update(int64_t n, T *__restrict__ x, T *__restrict__ r,
                 const T *__restrict__ p, const T *__restrict__ q,
                 const double *__restrict__ scal, double *part,
                 unsigned int *ticket, double *rr) {
-  const double alpha_d = scal[0] / scal[2];
-  const T alpha = static_cast<T>(alpha_d);
+  const int j = blockIdx.y;
+  const double *sc = scal + j * kColScal;
+  const bool frozen = sc[6] != 0.0;
+  const T alpha = frozen ? T(0) : static_cast<T>(sc[0] / sc[2]);
+  x += j * n;
+  r += j * n;
+  p += j * n;
+  q += j * n;
   double s = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    x[i] += alpha * p[i];
-    const T ri = r[i] - alpha * q[i];
-    r[i] = ri;
+    T ri = r[i];
+    if (!frozen) {
+      x[i] += alpha * p[i];
+      ri -= alpha * q[i];
+      r[i] = ri;
+    }
     s += static_cast<double>(ri) * static_cast<double>(ri);
   }
-  finish_reduction(s, part, ticket, rr, nullptr);
+  finish_reduction(s, part + j * gridDim.x, ticket + j, rr + j * kColScal,
+                   nullptr);
 }
 
 __device__ __forceinline__ double start_value(uint64_t i) {
@@ -131,19 +157,26 @@ __global__ void k_scale_diag(int64_t n, double *w, const double *dinv) {
     w[i] *= dinv[i];
 }
 
-// b = float(a / sqrt(*nrm2))
+// b = float(a / sqrt(*nrm2)) per column (a zero column stays zero)
 __global__ void k_to_f32_scaled(int64_t n, const double *a, const double *nrm2,
                                 float *b) {
-  const double s = 1.0 / sqrt(*nrm2);
+  const int j = blockIdx.y;
+  const double nr = nrm2[j * kColScal];
+  const double s = nr > 0.0 ? 1.0 / sqrt(nr) : 0.0;
+  a += j * n;
+  b += j * n;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
     b[i] = static_cast<float>(a[i] * s);
 }
 
-// U += sqrt(*nrm2) * double(d)
+// U += sqrt(*nrm2) * double(d) per column
 __global__ void k_axpy_f32(int64_t n, double *U, const float *d,
                            const double *nrm2) {
-  const double s = sqrt(*nrm2);
+  const int j = blockIdx.y;
+  const double s = sqrt(nrm2[j * kColScal]);
+  U += j * n;
+  d += j * n;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
     U[i] += s * static_cast<double>(d[i]);
@@ -169,46 +202,55 @@ __global__ void k_fill(int64_t n, double *a, double v) {
 
 }  // namespace
 
+// elementwise grid over nb columns: about the single-column grid in total
+static dim3 col_grid(int64_t n, int nb) {
+  int g = grid_for(n, 256);
+  if (nb > 1) g = std::max(148, g / nb);
+  return dim3(g, nb);
+}
+
 template <typename T>
 void launch_dot(const Ctx &c, int64_t n, const T *a, const T *b, double *out,
-                double *shift_to, cudaStream_t s) {
+                double *shift_to, cudaStream_t s, int nb) {
   count_launch();
-  k_dot<T><<<kRedBlocks, kRedThreads, 0, s>>>(n, a, b, c.part, c.ticket, out,
-                                               shift_to);
+  k_dot<T><<<dim3(red_grid(nb), nb), kRedThreads, 0, s>>>(n, a, b, c.part,
+                                                          c.ticket, out,
+                                                          shift_to);
 }
 template void launch_dot<double>(const Ctx &, int64_t, const double *,
                                  const double *, double *, double *,
-                                 cudaStream_t);
+                                 cudaStream_t, int);
 template void launch_dot<float>(const Ctx &, int64_t, const float *,
                                 const float *, double *, double *,
-                                cudaStream_t);
+                                cudaStream_t, int);
 
 template <typename T>
 void launch_cg_p(int64_t n, const T *z, T *p, const double *scal, bool first,
-                 cudaStream_t s) {
+                 cudaStream_t s, int nb) {
   count_launch();
-  k_cg_p<T><<<grid_for(n, 256), 256, 0, s>>>(n, z, p, scal, first);
+  k_cg_p<T><<<col_grid(n, nb), 256, 0, s>>>(n, z, p, scal, first);
 }
 template void launch_cg_p<double>(int64_t, const double *, double *,
-                                  const double *, bool, cudaStream_t);
+                                  const double *, bool, cudaStream_t, int);
 template void launch_cg_p<float>(int64_t, const float *, float *,
-                                 const double *, bool, cudaStream_t);
+                                 const double *, bool, cudaStream_t, int);
 
 template <typename T>
 void launch_cg_update(const Ctx &c, int64_t n, T *x, T *r, const T *p,
                       const T *q, const double *scal, double *rr,
-                      cudaStream_t s) {
+                      cudaStream_t s, int nb) {
   count_launch();
-  k_cg_update<T><<<kRedBlocks, kRedThreads, 0, s>>>(n, x, r, p, q, scal, c.part,
-                                                     c.ticket, rr);
+  k_cg_update<T><<<dim3(red_grid(nb), nb), kRedThreads, 0, s>>>(
+      n, x, r, p, q, scal, c.part, c.ticket, rr);
 }
 template void launch_cg_update<double>(const Ctx &, int64_t, double *,
                                        double *, const double *,
                                        const double *, const double *,
-                                       double *, cudaStream_t);
+                                       double *, cudaStream_t, int);
 template void launch_cg_update<float>(const Ctx &, int64_t, float *, float *,
                                       const float *, const float *,
-                                      const double *, double *, cudaStream_t);
+                                      const double *, double *, cudaStream_t,
+                                      int);
 
 void launch_power_start(int64_t n, double *a, cudaStream_t s) {
   count_launch();
@@ -230,15 +272,15 @@ void launch_scale_diag(int64_t n, double *w, const double *dinv,
 }
 
 void launch_to_f32_scaled(int64_t n, const double *a, const double *scal,
-                          float *b, cudaStream_t s) {
+                          float *b, cudaStream_t s, int nb) {
   count_launch();
-  k_to_f32_scaled<<<grid_for(n, 256), 256, 0, s>>>(n, a, scal, b);
+  k_to_f32_scaled<<<col_grid(n, nb), 256, 0, s>>>(n, a, scal, b);
 }
 
 void launch_axpy_f32(int64_t n, double *U, const float *d, const double *scal,
-                     cudaStream_t s) {
+                     cudaStream_t s, int nb) {
   count_launch();
-  k_axpy_f32<<<grid_for(n, 256), 256, 0, s>>>(n, U, d, scal);
+  k_axpy_f32<<<col_grid(n, nb), 256, 0, s>>>(n, U, d, scal);
 }
 
 void launch_d2f(int64_t n, const double *a, float *b, cudaStream_t s) {

@@ -59,13 +59,19 @@ const float *halfS(const Level &v, float *) { return v.H32; }
 // full FP64 stencil on the persistent levels (used there only for the set-up
 // eigenvalue estimate)
 template <typename T>
-void level_apply(Ctx &c, int l, const T *u, const T *b, T *y, cudaStream_t s) {
-  if (l == 0)
-    launch_apply_fine<T>(c, fineE(c, (T *)nullptr), u, b, y, s);
-  else if (l < c.ps)
-    launch_apply_stencil_sym<T>(c.lev[l], halfS(c.lev[l], (T *)nullptr), u, b, y, s);
-  else
-    launch_apply_stencil<T>(c.lev[l], lv(c.lev[l], (T *)nullptr).S, u, b, y, s);
+void level_apply(Ctx &c, int l, const T *u, const T *b, T *y, cudaStream_t s,
+                 int nb = 1) {
+  if (l == 0) {
+    launch_apply_fine<T>(c, fineE(c, (T *)nullptr), u, b, y, s, nb);
+  } else if (l < c.ps) {
+    launch_apply_stencil_sym<T>(c.lev[l], halfS(c.lev[l], (T *)nullptr), u, b,
+                                y, s, nb);
+  } else {
+    const int64_t ld = 3 * c.lev[l].nn;
+    for (int j = 0; j < nb; ++j)
+      launch_apply_stencil<T>(c.lev[l], lv(c.lev[l], (T *)nullptr).S, u + j * ld,
+                              b ? b + j * ld : nullptr, y + j * ld, s);
+  }
 }
 
 // parameters of the persistent kernel for levels ps .. L-1 (kernels_coarse.cu)
@@ -117,15 +123,17 @@ CoarseCycle<T> coarse_cycle_params(Ctx &c, const tpo_solve_opts &o) {
 
 template <typename T>
 void vcycle_rec(Ctx &c, int l, const T *b, T *x, const tpo_solve_opts &o,
-                cudaStream_t s) {
+                cudaStream_t s, int nb) {
   if (l == c.L - 1) {
-    launch_coarse_gemv<T>(c.nc, c.Ainv, b, x, s);
+    launch_coarse_gemv<T>(c.nc, c.Ainv, b, x, s, nb);
     return;
   }
   if (l >= 1 && l == c.ps) {
     // levels ps..L-1 in one cooperative launch; b and x are this level's
     // own b and x buffers (the restriction above wrote b)
-    c.coarse_err = launch_coarse_cycle<T>(coarse_cycle_params<T>(c, o), s);
+    CoarseCycle<T> P = coarse_cycle_params<T>(c, o);
+    P.nb = nb;
+    c.coarse_err = launch_coarse_cycle<T>(P, s);
     return;
   }
   Level &v = c.lev[l];
@@ -145,63 +153,64 @@ void vcycle_rec(Ctx &c, int l, const T *b, T *x, const tpo_solve_opts &o,
     a.c1 = static_cast<T>(rn * ch.rho0);
     a.c2 = static_cast<T>(2.0 * rn / ch.delta);
     a.y = x;
-    launch_apply_fused<T>(c, E, IN_CHEB, OUT_CHEB2, a, s);   // pre-smooth
-    launch_apply_fine<T>(c, E, x, b, w.a, s);                 // residual
+    launch_apply_fused<T>(c, E, IN_CHEB, OUT_CHEB2, a, s, nb);   // pre-smooth
+    launch_apply_fine<T>(c, E, x, b, w.a, s, nb);                 // residual
     Level &cv = c.lev[l + 1];
     LV<T> cw = lv(cv, (T *)nullptr);
-    launch_restrict<T>(v, cv, w.a, cw.b, s);
-    vcycle_rec<T>(c, l + 1, cw.b, cw.x, o, s);
-    launch_prolong_add<T>(v, cv, cw.x, x, s);
+    launch_restrict<T>(v, cv, w.a, cw.b, s, nb);
+    vcycle_rec<T>(c, l + 1, cw.b, cw.x, o, s, nb);
+    launch_prolong_add<T>(v, cv, cw.x, x, s, nb);
     a.u = x;                                                  // post-smooth
     a.y = w.d;
     a.y2 = w.r;
-    launch_apply_fused<T>(c, E, IN_U, OUT_POST0, a, s);
+    launch_apply_fused<T>(c, E, IN_U, OUT_POST0, a, s, nb);
     a.u = w.d;
     a.y = x;
     a.y2 = w.r;
-    launch_apply_fused<T>(c, E, IN_U, OUT_POST1, a, s);
+    launch_apply_fused<T>(c, E, IN_U, OUT_POST1, a, s, nb);
     return;
   }
   // pre-smoothing from a zero guess
-  launch_cheb_init<T>(n, w.dinv, b, w.r, w.d, x, ch.inv_theta, true, s);
+  launch_cheb_init<T>(n, w.dinv, b, w.r, w.d, x, ch.inv_theta, true, s, nb);
   double rho = ch.rho0;
   for (int k = 1; k < o.cheb_degree; ++k) {
-    level_apply<T>(c, l, w.d, nullptr, w.a, s);
+    level_apply<T>(c, l, w.d, nullptr, w.a, s, nb);
     const double rn = 1.0 / (2.0 * ch.sigma - rho);
-    launch_cheb_step<T>(n, w.dinv, w.a, w.r, w.d, x, rn * rho, 2.0 * rn / ch.delta, s);
+    launch_cheb_step<T>(n, w.dinv, w.a, w.r, w.d, x, rn * rho, 2.0 * rn / ch.delta, s, nb);
     rho = rn;
   }
   // residual, restriction, coarse correction, prolongation
-  level_apply<T>(c, l, x, b, w.a, s);
+  level_apply<T>(c, l, x, b, w.a, s, nb);
   Level &cv = c.lev[l + 1];
   LV<T> cw = lv(cv, (T *)nullptr);
-  launch_restrict<T>(v, cv, w.a, cw.b, s);
-  vcycle_rec<T>(c, l + 1, cw.b, cw.x, o, s);
-  launch_prolong_add<T>(v, cv, cw.x, x, s);
+  launch_restrict<T>(v, cv, w.a, cw.b, s, nb);
+  vcycle_rec<T>(c, l + 1, cw.b, cw.x, o, s, nb);
+  launch_prolong_add<T>(v, cv, cw.x, x, s, nb);
   // post-smoothing from the corrected x
-  level_apply<T>(c, l, x, b, w.r, s);
-  launch_cheb_init<T>(n, w.dinv, b, w.r, w.d, x, ch.inv_theta, false, s);
+  level_apply<T>(c, l, x, b, w.r, s, nb);
+  launch_cheb_init<T>(n, w.dinv, b, w.r, w.d, x, ch.inv_theta, false, s, nb);
   rho = ch.rho0;
   for (int k = 1; k < o.cheb_degree; ++k) {
-    level_apply<T>(c, l, w.d, nullptr, w.a, s);
+    level_apply<T>(c, l, w.d, nullptr, w.a, s, nb);
     const double rn = 1.0 / (2.0 * ch.sigma - rho);
-    launch_cheb_step<T>(n, w.dinv, w.a, w.r, w.d, x, rn * rho, 2.0 * rn / ch.delta, s);
+    launch_cheb_step<T>(n, w.dinv, w.a, w.r, w.d, x, rn * rho, 2.0 * rn / ch.delta, s, nb);
     rho = rn;
   }
 }
 
-// one CG iteration after the first (p = z + beta p): V-cycle, rho, p, q,
-// pq, update.  Kept free of host synchronisation so it can be captured.
+// one CG iteration (p = z + beta p after the first): V-cycle, rho, p, q,
+// pq, update, for nb columns.  Kept free of host synchronisation so it can
+// be captured.
 template <typename T>
 void cg_body(Ctx &c, int64_t n, T *x, T *r, T *z, T *p, T *q,
-             const tpo_solve_opts &o, bool first, cudaStream_t s) {
+             const tpo_solve_opts &o, bool first, cudaStream_t s, int nb) {
   double *sc = c.scal;
-  vcycle_rec<T>(c, 0, r, z, o, s);
-  launch_dot<T>(c, n, r, z, sc + 0, sc + 1, s);
-  launch_cg_p<T>(n, z, p, sc, first, s);
-  launch_apply_fine<T>(c, fineE(c, (T *)nullptr), p, nullptr, q, s);
-  launch_dot<T>(c, n, p, q, sc + 2, nullptr, s);
-  launch_cg_update<T>(c, n, x, r, p, q, sc, sc + 3, s);
+  vcycle_rec<T>(c, 0, r, z, o, s, nb);
+  launch_dot<T>(c, n, r, z, sc + 0, sc + 1, s, nb);
+  launch_cg_p<T>(n, z, p, sc, first, s, nb);
+  launch_apply_fine<T>(c, fineE(c, (T *)nullptr), p, nullptr, q, s, nb);
+  launch_dot<T>(c, n, p, q, sc + 2, nullptr, s, nb);
+  launch_cg_update<T>(c, n, x, r, p, q, sc, sc + 3, s, nb);
 }
 
 #define CK(call)                                                       \
@@ -213,34 +222,66 @@ void cg_body(Ctx &c, int64_t n, T *x, T *r, T *z, T *p, T *q,
     }                                                                  \
   } while (0)
 
-int readback(Ctx &c, int count) {
-  CK(cudaMemcpyAsync(c.scal_h, c.scal, sizeof(double) * count,
+// copy the scalars of nb columns to the host mirror
+int readback(Ctx &c, int nb) {
+  CK(cudaMemcpyAsync(c.scal_h, c.scal, sizeof(double) * kColScal * nb,
                      cudaMemcpyDeviceToHost, c.stream));
   CK(cudaStreamSynchronize(c.stream));
   return TPO_OK;
 }
 
-// PCG on the fine operator in precision T.  x holds the initial guess and
-// r must already hold b - K x; ||r||^2 is in scal[3] on the host mirror.
-// target_rr is the squared residual norm at which to stop.
+// device scalar slot `slot` of nb columns <- host values (through pinned
+// staging after the column block of scal_h)
+int upload_slot(Ctx &c, int slot, const double *v, int nb) {
+  double *st = c.scal_h + kScalCount;
+  for (int j = 0; j < nb; ++j) st[j] = v[j];
+  CK(cudaMemcpy2DAsync(c.scal + slot, sizeof(double) * kColScal, st,
+                       sizeof(double), sizeof(double), nb,
+                       cudaMemcpyHostToDevice, c.stream));
+  return TPO_OK;
+}
+
+// device slot dst <- slot src for nb columns
+int copy_slot(Ctx &c, int dst, int src, int nb) {
+  CK(cudaMemcpy2DAsync(c.scal + dst, sizeof(double) * kColScal, c.scal + src,
+                       sizeof(double) * kColScal, sizeof(double), nb,
+                       cudaMemcpyDeviceToDevice, c.stream));
+  return TPO_OK;
+}
+
+// PCG on the fine operator in precision T for nb columns.  x holds the
+// initial guesses and r must already hold b - K x; ||r_j||^2 is in slot 3
+// of the host mirror.  Column j stops at ||r_j||^2 <= target_rr[j]; columns
+// with frozen[j] set do not iterate.  On return its[j] = iterations of
+// column j and st[j] = its status.
 template <typename T>
 int pcg_loop(Ctx &c, const tpo_solve_opts &o, T *x, T *r, T *z, T *p, T *q,
-             double target_rr, int maxit, int *its) {
+             const double *target_rr, int maxit, int nb, double *frozen,
+             int *its, int *st) {
   cudaStream_t s = c.stream;
   const int64_t n = 3 * c.nn;
   cudaGraphExec_t &g = (sizeof(T) == 8) ? c.graph64 : c.graph32;
   const void *&gx = (sizeof(T) == 8) ? c.graph64_x : c.graph32_x;
+  int &gnb = (sizeof(T) == 8) ? c.graph64_nb : c.graph32_nb;
   long long &gnodes = (sizeof(T) == 8) ? c.graph64_nodes : c.graph32_nodes;
-  int k = 0;
-  int status = TPO_NOT_CONVERGED;
-  if (c.scal_h[3] <= target_rr) {
-    *its = 0;
-    return TPO_OK;
+  int active = 0;
+  for (int j = 0; j < nb; ++j) {
+    its[j] = 0;
+    st[j] = TPO_NOT_CONVERGED;
+    if (frozen[j] == 0.0 && c.scal_h[j * kColScal + 3] <= target_rr[j]) {
+      frozen[j] = 1.0;
+      st[j] = TPO_OK;
+    }
+    if (frozen[j] != 0.0 && st[j] == TPO_NOT_CONVERGED) st[j] = TPO_OK;
+    if (frozen[j] == 0.0) ++active;
   }
-  while (k < maxit) {
+  if (!active) return TPO_OK;
+  if (int rc = upload_slot(c, 6, frozen, nb)) return rc;
+  int k = 0;
+  while (k < maxit && active) {
     const bool first = (k == 0);
     if (!first && o.use_graph) {
-      if (!g || gx != (const void *)x) {
+      if (!g || gx != (const void *)x || gnb != nb) {
         if (g) {
           cudaGraphExecDestroy(g);
           g = nullptr;
@@ -248,7 +289,7 @@ int pcg_loop(Ctx &c, const tpo_solve_opts &o, T *x, T *r, T *z, T *p, T *q,
         cudaGraph_t graph;
         const long long before = g_launches.load();
         CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        cg_body<T>(c, n, x, r, z, p, q, o, false, s);
+        cg_body<T>(c, n, x, r, z, p, q, o, false, s, nb);
         CK(cudaStreamEndCapture(s, &graph));
         // captured launches run when the graph is launched, not now
         gnodes = g_launches.load() - before;
@@ -256,29 +297,43 @@ int pcg_loop(Ctx &c, const tpo_solve_opts &o, T *x, T *r, T *z, T *p, T *q,
         CK(cudaGraphInstantiate(&g, graph, 0));
         CK(cudaGraphDestroy(graph));
         gx = x;
+        gnb = nb;
       }
       CK(cudaGraphLaunch(g, s));
       count_launch(gnodes);
     } else {
-      cg_body<T>(c, n, x, r, z, p, q, o, first, s);
+      cg_body<T>(c, n, x, r, z, p, q, o, first, s, nb);
     }
     CK(cudaGetLastError());
     CK(c.coarse_err);
     ++k;
-    if (int rc = readback(c, 4)) return rc;
-    const double rho = c.scal_h[0], pq = c.scal_h[2], rr = c.scal_h[3];
-    if (!(rho > 0) || !(pq > 0) || !std::isfinite(rr)) {
-      status = TPO_E_BREAKDOWN;
-      c.err = "CG breakdown (indefinite preconditioner/operator or non-finite residual)";
-      break;
+    if (int rc = readback(c, nb)) return rc;
+    bool changed = false;
+    for (int j = 0; j < nb; ++j) {
+      if (frozen[j] != 0.0) continue;
+      const double *h = c.scal_h + j * kColScal;
+      const double rho = h[0], pq = h[2], rr = h[3];
+      its[j] = k;
+      if (!(rho > 0) || !(pq > 0) || !std::isfinite(rr)) {
+        st[j] = TPO_E_BREAKDOWN;
+        c.err = "CG breakdown (indefinite preconditioner/operator or non-finite residual)";
+      } else if (rr <= target_rr[j]) {
+        st[j] = TPO_OK;
+      } else {
+        continue;
+      }
+      frozen[j] = 1.0;
+      changed = true;
+      --active;
     }
-    if (rr <= target_rr) {
-      status = TPO_OK;
-      break;
-    }
+    if (changed && active)
+      if (int rc = upload_slot(c, 6, frozen, nb)) return rc;
   }
-  *its = k;
-  return status;
+  int worst = TPO_OK;
+  for (int j = 0; j < nb; ++j)
+    if (st[j] < 0 ? st[j] < worst : (worst == TPO_OK && st[j] != TPO_OK))
+      worst = st[j];
+  return worst;
 }
 
 }  // namespace
@@ -288,6 +343,7 @@ void invalidate_graphs(Ctx &c) {
   if (c.graph32) cudaGraphExecDestroy(c.graph32);
   c.graph64 = c.graph32 = nullptr;
   c.graph64_x = c.graph32_x = nullptr;
+  c.graph64_nb = c.graph32_nb = 0;
 }
 
 int estimate_lambda(Ctx &c, int l, int its, double *lam) {
@@ -295,20 +351,21 @@ int estimate_lambda(Ctx &c, int l, int its, double *lam) {
   const int64_t n = 3 * v.nn;
   cudaStream_t s = c.stream;
   double *a = v.d64, *w = v.a64;
+  double *nrm = c.scal + SC_POWER;
   launch_power_start(n, a, s);
-  launch_dot<double>(c, n, a, a, c.scal + 6, nullptr, s);
-  launch_power_normalize(n, a, a, nullptr, c.scal + 6, s);
+  launch_dot<double>(c, n, a, a, nrm, nullptr, s);
+  launch_power_normalize(n, a, a, nullptr, nrm, s);
   for (int k = 0; k < its; ++k) {
     level_apply<double>(c, l, a, nullptr, w, s);
     launch_scale_diag(n, w, v.dinv64, s);
-    launch_dot<double>(c, n, w, w, c.scal + 6, nullptr, s);
-    launch_power_normalize(n, a, w, nullptr, c.scal + 6, s);
+    launch_dot<double>(c, n, w, w, nrm, nullptr, s);
+    launch_power_normalize(n, a, w, nullptr, nrm, s);
   }
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(c.scal_h + 6, c.scal + 6, sizeof(double),
+  CK(cudaMemcpyAsync(c.scal_h + SC_POWER, nrm, sizeof(double),
                      cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
-  *lam = std::sqrt(c.scal_h[6]);
+  *lam = std::sqrt(c.scal_h[SC_POWER]);
   return TPO_OK;
 }
 
@@ -394,10 +451,10 @@ int vcycle_apply(Ctx &c, const tpo_solve_opts &o, int precision,
   cudaStream_t s = c.stream;
   const int64_t n = 3 * c.nn;
   if (precision == TPO_PREC_FP64) {
-    vcycle_rec<double>(c, 0, r, z, o, s);
+    vcycle_rec<double>(c, 0, r, z, o, s, 1);
   } else {
     launch_d2f(n, r, c.r32, s);
-    vcycle_rec<float>(c, 0, c.r32, c.z32, o, s);
+    vcycle_rec<float>(c, 0, c.r32, c.z32, o, s, 1);
     launch_f2d(n, c.z32, z, s);
   }
   CK(cudaGetLastError());
@@ -405,96 +462,171 @@ int vcycle_apply(Ctx &c, const tpo_solve_opts &o, int precision,
   return TPO_OK;
 }
 
-// Solve K x = b; x holds the initial guess (device pointers, 3*nn each).
+// one V-cycle and one fine apply on nb scratch columns (for timing the
+// right-hand-side block size)
+int vcycle_block(Ctx &c, const tpo_solve_opts &o, int precision, int nb) {
+  cudaStream_t s = c.stream;
+  if (precision == TPO_PREC_FP64) {
+    vcycle_rec<double>(c, 0, c.r64, c.z64, o, s, nb);
+    launch_apply_fine<double>(c, c.E64, c.z64, nullptr, c.q64, s, nb);
+  } else {
+    vcycle_rec<float>(c, 0, c.r32, c.z32, o, s, nb);
+    launch_apply_fine<float>(c, c.E32, c.z32, nullptr, c.q32, s, nb);
+  }
+  CK(cudaGetLastError());
+  CK(c.coarse_err);
+  return TPO_OK;
+}
+
+// Solve K x_j = b_j for nb columns (stride 3 nn); x holds the initial
+// guesses.  Column j converges at ||b_j - K x_j|| <= rtol ||b_j||.  info
+// aggregates the block (iterations and outer steps summed over columns,
+// the largest relative residual, the worst status); col, if given, gets
+// one record per column.
 int solve(Ctx &c, const tpo_solve_opts &o, const double *b, double *x,
-          tpo_solve_info *info) {
+          tpo_solve_info *info, int nb, tpo_solve_info *col) {
   const double t0 = now_ms();
   cudaStream_t s = c.stream;
   const int64_t n = 3 * c.nn;
   double *sc = c.scal;
-  int its_total = 0, outer = 0, status = TPO_NOT_CONVERGED;
-  double bn = 0, rn = 0;
+  if (nb < 1 || nb > kMaxBatch || nb > c.nb_cap) {
+    c.err = "right-hand-side block exceeds the allocated columns";
+    return TPO_E_ARG;
+  }
+  double bn[kMaxBatch], rn[kMaxBatch], target[kMaxBatch], tgt2[kMaxBatch];
+  double frozen[kMaxBatch];
+  int its_total[kMaxBatch], outer[kMaxBatch], status[kMaxBatch];
+  int its[kMaxBatch], st[kMaxBatch];
 
-  launch_dot<double>(c, n, b, b, sc + 4, nullptr, s);
-  launch_apply_fine<double>(c, c.E64, x, b, c.r64, s);
-  launch_dot<double>(c, n, c.r64, c.r64, sc + 5, nullptr, s);
+  launch_dot<double>(c, n, b, b, sc + 4, nullptr, s, nb);
+  launch_apply_fine<double>(c, c.E64, x, b, c.r64, s, nb);
+  launch_dot<double>(c, n, c.r64, c.r64, sc + 5, nullptr, s, nb);
   CK(cudaGetLastError());
-  if (int rc = readback(c, 6)) return rc;
-  bn = std::sqrt(c.scal_h[4]);
-  rn = std::sqrt(c.scal_h[5]);
-  const double target = o.rtol * bn;
-  if (bn == 0.0) {
-    CK(cudaMemsetAsync(x, 0, sizeof(double) * n, s));
-    status = TPO_OK;
-    rn = 0;
-  } else if (rn <= target) {
-    status = TPO_OK;
-  } else if (o.precision == TPO_PREC_FP64) {
-    // r = b - K x already in r64 and ||r||^2 in scal[5]
-    c.scal_h[3] = c.scal_h[5];
-    CK(cudaMemcpyAsync(sc + 3, sc + 5, sizeof(double), cudaMemcpyDeviceToDevice, s));
-    int its = 0;
-    status = pcg_loop<double>(c, o, x, c.r64, c.z64, c.p64, c.q64,
-                              target * target, o.maxit, &its);
-    its_total = its;
-    outer = 1;
+  if (int rc = readback(c, nb)) return rc;
+  int active = 0;
+  for (int j = 0; j < nb; ++j) {
+    bn[j] = std::sqrt(c.scal_h[j * kColScal + 4]);
+    rn[j] = std::sqrt(c.scal_h[j * kColScal + 5]);
+    target[j] = o.rtol * bn[j];
+    tgt2[j] = target[j] * target[j];
+    its_total[j] = outer[j] = 0;
+    status[j] = TPO_NOT_CONVERGED;
+    frozen[j] = 0.0;
+    if (bn[j] == 0.0) {
+      CK(cudaMemsetAsync(x + j * n, 0, sizeof(double) * n, s));
+      rn[j] = 0.0;
+      status[j] = TPO_OK;
+      frozen[j] = 1.0;
+    } else if (rn[j] <= target[j]) {
+      status[j] = TPO_OK;
+      frozen[j] = 1.0;
+    } else {
+      ++active;
+    }
+  }
+  if (active && o.precision == TPO_PREC_FP64) {
+    // r = b - K x already in r64 and ||r||^2 in slot 5
+    for (int j = 0; j < nb; ++j) c.scal_h[j * kColScal + 3] = c.scal_h[j * kColScal + 5];
+    if (int rc = copy_slot(c, 3, 5, nb)) return rc;
+    pcg_loop<double>(c, o, x, c.r64, c.z64, c.p64, c.q64, tgt2, o.maxit, nb,
+                     frozen, its, st);
     // report the true residual
-    launch_apply_fine<double>(c, c.E64, x, b, c.r64, s);
-    launch_dot<double>(c, n, c.r64, c.r64, sc + 5, nullptr, s);
-    if (int rc = readback(c, 6)) return rc;
-    rn = std::sqrt(c.scal_h[5]);
-  } else {
-    // mixed: FP32 PCG+GMG on K d = r/||r|| inside FP64 defect correction
-    while (outer < o.max_outer) {
-      if (rn <= target) {
-        status = TPO_OK;
-        break;
+    launch_apply_fine<double>(c, c.E64, x, b, c.r64, s, nb);
+    launch_dot<double>(c, n, c.r64, c.r64, sc + 5, nullptr, s, nb);
+    if (int rc = readback(c, nb)) return rc;
+    for (int j = 0; j < nb; ++j) {
+      if (status[j] == TPO_OK) continue;   // converged before the loop
+      its_total[j] = its[j];
+      outer[j] = 1;
+      status[j] = st[j];
+      rn[j] = std::sqrt(c.scal_h[j * kColScal + 5]);
+    }
+  } else if (active) {
+    // mixed: FP32 PCG+GMG on K d_j = r_j/||r_j|| inside FP64 defect
+    // correction, all columns of the block together
+    int round = 0;
+    while (round < o.max_outer) {
+      double tgt_in[kMaxBatch];
+      double inner_frozen[kMaxBatch];
+      int live = 0;
+      for (int j = 0; j < nb; ++j) {
+        const bool done = status[j] == TPO_OK || status[j] == TPO_E_BREAKDOWN ||
+                          rn[j] <= target[j] || its_total[j] >= o.maxit;
+        inner_frozen[j] = done ? 1.0 : 0.0;
+        if (!done) ++live;
       }
-      if (its_total >= o.maxit) break;
-      launch_to_f32_scaled(n, c.r64, sc + 5, c.r32, s);
-      CK(cudaMemsetAsync(c.x32, 0, sizeof(float) * n, s));
-      launch_dot<float>(c, n, c.r32, c.r32, sc + 3, nullptr, s);
-      if (int rc = readback(c, 4)) return rc;
-      // ask the FP32 solve for the reduction that reaches the target with a
-      // 3x margin, but never below the FP32-attainable floor inner_rtol
-      const double eta = std::max(o.inner_rtol, 0.3 * target / rn);
-      const double tgt = eta * eta * c.scal_h[3];
-      int its = 0;
-      const int st = pcg_loop<float>(c, o, c.x32, c.r32, c.z32, c.p32, c.q32,
-                                     tgt, o.maxit - its_total, &its);
-      its_total += its;
-      ++outer;
-      launch_axpy_f32(n, x, c.x32, sc + 5, s);
-      launch_apply_fine<double>(c, c.E64, x, b, c.r64, s);
-      launch_dot<double>(c, n, c.r64, c.r64, sc + 5, nullptr, s);
-      if (int rc = readback(c, 6)) return rc;
-      const double rn_new = std::sqrt(c.scal_h[5]);
-      if (st == TPO_E_BREAKDOWN && !(rn_new < rn)) {
-        status = TPO_E_BREAKDOWN;
-        rn = rn_new;
-        break;
+      if (!live) break;
+      launch_to_f32_scaled(n, c.r64, sc + 5, c.r32, s, nb);
+      CK(cudaMemsetAsync(c.x32, 0, sizeof(float) * n * nb, s));
+      launch_dot<float>(c, n, c.r32, c.r32, sc + 3, nullptr, s, nb);
+      if (int rc = readback(c, nb)) return rc;
+      int maxit_in = 0;
+      for (int j = 0; j < nb; ++j) {
+        // ask the FP32 solve for the reduction that reaches the target with
+        // a 3x margin, but never below the FP32-attainable floor inner_rtol
+        const double eta = std::max(o.inner_rtol, 0.3 * target[j] / std::max(rn[j], 1e-300));
+        tgt_in[j] = eta * eta * c.scal_h[j * kColScal + 3];
+        if (inner_frozen[j] == 0.0) maxit_in = std::max(maxit_in, o.maxit - its_total[j]);
       }
-      rn = rn_new;
-      if (!std::isfinite(rn)) {
-        status = TPO_E_BREAKDOWN;
-        c.err = "non-finite residual in defect correction";
-        break;
+      pcg_loop<float>(c, o, c.x32, c.r32, c.z32, c.p32, c.q32, tgt_in, maxit_in,
+                      nb, inner_frozen, its, st);
+      ++round;
+      // columns that were done before this round get a zero correction
+      // (their x32 stays zero)
+      launch_axpy_f32(n, x, c.x32, sc + 5, s, nb);
+      launch_apply_fine<double>(c, c.E64, x, b, c.r64, s, nb);
+      launch_dot<double>(c, n, c.r64, c.r64, sc + 5, nullptr, s, nb);
+      if (int rc = readback(c, nb)) return rc;
+      for (int j = 0; j < nb; ++j) {
+        const double rn_new = std::sqrt(c.scal_h[j * kColScal + 5]);
+        const bool was_live = !(status[j] == TPO_OK || status[j] == TPO_E_BREAKDOWN ||
+                                rn[j] <= target[j] || its_total[j] >= o.maxit);
+        if (!was_live) {
+          rn[j] = rn_new;
+          continue;
+        }
+        its_total[j] += its[j];
+        ++outer[j];
+        if (st[j] == TPO_E_BREAKDOWN && !(rn_new < rn[j])) status[j] = TPO_E_BREAKDOWN;
+        rn[j] = rn_new;
+        if (!std::isfinite(rn_new)) {
+          status[j] = TPO_E_BREAKDOWN;
+          c.err = "non-finite residual in defect correction";
+        }
       }
     }
-    if (rn <= target) status = TPO_OK;
+    for (int j = 0; j < nb; ++j)
+      if (status[j] != TPO_E_BREAKDOWN) status[j] = rn[j] <= target[j] ? TPO_OK : TPO_NOT_CONVERGED;
   }
   CK(cudaGetLastError());
-  if (info) {
-    info->status = status;
-    info->iterations = its_total;
-    info->outer = outer;
-    info->relres = bn > 0 ? rn / bn : 0.0;
-    info->solve_ms = now_ms() - t0;
-    info->setup_ms = c.setup_ms;
+  const double ms = now_ms() - t0;
+  int worst = TPO_OK;
+  tpo_solve_info acc{};
+  for (int j = 0; j < nb; ++j) {
+    if (status[j] < 0 ? status[j] < worst : (worst == TPO_OK && status[j] != TPO_OK))
+      worst = status[j];
+    const double rel = bn[j] > 0 ? rn[j] / bn[j] : 0.0;
+    acc.iterations += its_total[j];
+    acc.outer += outer[j];
+    acc.relres = std::max(acc.relres, rel);
+    if (col) {
+      col[j].status = status[j];
+      col[j].iterations = its_total[j];
+      col[j].outer = outer[j];
+      col[j].relres = rel;
+      col[j].solve_ms = ms;
+      col[j].setup_ms = c.setup_ms;
+    }
   }
-  if (status == TPO_NOT_CONVERGED && c.err.empty())
+  if (info) {
+    acc.status = worst;
+    acc.solve_ms = ms;
+    acc.setup_ms = c.setup_ms;
+    *info = acc;
+  }
+  if (worst == TPO_NOT_CONVERGED && c.err.empty())
     c.err = "solver reached its iteration limit";
-  return status;
+  return worst;
 }
 
 }  // namespace tpo

@@ -10,7 +10,8 @@ int estimate_lambda(Ctx &c, int level, int its, double *lam);
 int setup_hierarchy(Ctx &c, const tpo_solve_opts &o);
 int vcycle_apply(Ctx &c, const tpo_solve_opts &o, int precision,
                  const double *r, double *z);
+int vcycle_block(Ctx &c, const tpo_solve_opts &o, int precision, int nb);
 int solve(Ctx &c, const tpo_solve_opts &o, const double *b, double *x,
-          tpo_solve_info *info);
+          tpo_solve_info *info, int nb = 1, tpo_solve_info *col = nullptr);
 
 }  // namespace tpo

@@ -74,8 +74,9 @@ struct Level {
   double *dinv64 = nullptr;
   float *dinv32 = nullptr;
   double lam = 0.0;
-  // V-cycle work vectors (3*nn each); e = second Chebyshev direction and
-  // w = pre-smoothed iterate of the levels run by the persistent kernel
+  // V-cycle work vectors (3*nn per column, Ctx::nb_cap columns); e = second
+  // Chebyshev direction and w = pre-smoothed iterate of the levels run by
+  // the persistent kernel
   double *b64 = nullptr, *x64 = nullptr, *r64 = nullptr, *d64 = nullptr,
          *a64 = nullptr, *e64 = nullptr, *w64 = nullptr;
   float *b32 = nullptr, *x32 = nullptr, *r32 = nullptr, *d32 = nullptr,
@@ -88,6 +89,8 @@ struct Ctx {
   int64_t ne = 0, nn = 0;
   int L = 0;
   int ps = 0;   // first level run by the persistent coarse-cycle kernel
+  int nb_cap = 1;   // columns the level and solver work vectors hold
+  int rhs_block_tuned = 0;   // autotuned right-hand-side block (0: not yet)
   cudaError_t coarse_err = cudaSuccess;   // last cooperative launch status
   std::vector<Level> lev;
   int device = 0;
@@ -125,7 +128,8 @@ struct Ctx {
   FilterTaps *taps_d = nullptr;
   double *finv = nullptr;   // 1 / row sum per element
 
-  // solver work (fine level, FP64 and FP32)
+  // solver work (fine level, FP64 and FP32; r, z, p, q and x32 hold
+  // nb_cap columns, w64 one)
   double *r64 = nullptr, *z64 = nullptr, *p64 = nullptr, *q64 = nullptr,
          *w64 = nullptr;
   float *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *q32 = nullptr,
@@ -136,6 +140,7 @@ struct Ctx {
   unsigned int *ticket = nullptr;
   double *tmpe = nullptr, *tmpe2 = nullptr;   // element-sized scratch
   double *io_a = nullptr, *io_b = nullptr;    // staging for host buffers
+  double *io_ba = nullptr, *io_bb = nullptr;  // the same for column blocks
   double *oc_ws = nullptr;                    // OC update workspace (6 nElem)
   size_t io_bytes = 0;
 
@@ -146,9 +151,10 @@ struct Ctx {
   size_t solver_work_n = 0;
   int *dev_info = nullptr;
 
-  // CUDA graphs of the CG iteration bodies
+  // CUDA graphs of the CG iteration bodies, keyed on (x, columns)
   cudaGraphExec_t graph64 = nullptr, graph32 = nullptr;
   const void *graph64_x = nullptr, *graph32_x = nullptr;
+  int graph64_nb = 0, graph32_nb = 0;
   long long graph64_nodes = 0, graph32_nodes = 0;
 };
 
@@ -162,26 +168,48 @@ inline void count_launch(long long n = 1) {
 
 constexpr int kRedBlocks = 592;   // 4 x 148 SMs: fixed grid for reductions
 
+// Right-hand sides are processed in blocks of up to kMaxBatch columns:
+// column j of a block vector lives at offset j * (3 * nn_level).  Each
+// column has kColScal device scalars at scal + j * kColScal:
+//   0 rho = r.z, 1 rho of the previous iteration, 2 p.q, 3 r.r (current
+//   PCG), 4 b.b, 5 r.r of the FP64 residual, 6 frozen flag (non-zero: the
+//   column has converged and its CG updates are skipped), 7 spare.
+// Scalars of the design-side calls follow the column block at kScalMisc.
+constexpr int kMaxBatch = 8;
+constexpr int kColScal = 8;
+constexpr int kScalMisc = kMaxBatch * kColScal;   // 64
+constexpr int kScalCount = kScalMisc + 16;
+enum { SC_COMPLIANCE = kScalMisc, SC_VOLUME, SC_OC_DG, SC_OC_CHANGE, SC_POWER };
+
+// fixed reduction grid (blocks per column) for a block of nb columns
+inline int red_grid(int nb) {
+  return nb <= 1 ? kRedBlocks : (kRedBlocks / nb < 148 ? 148 : kRedBlocks / nb);
+}
+constexpr int kPartCount = 2048;   // >= red_grid(nb) * nb for nb <= kMaxBatch
+
 // fine matrix-free operator: y = M K M u + (1-M) u, or y = b - (that)
 template <typename T>
 void launch_apply_fine(const Ctx &c, const T *E, const T *u, const T *b, T *y,
-                       cudaStream_t s);
+                       cudaStream_t s, int nb = 1);
 
 // fused fine-level variants: how the input is formed and what the epilogue
 // writes (kernels_apply_staged.cu, finish_dof)
 enum { IN_U = 0, IN_CHEB = 1 };
 enum { OUT_Y = 0, OUT_RESID = 1, OUT_CHEB2 = 2, OUT_POST0 = 3, OUT_POST1 = 4 };
 
+// u, b, y, y2 are per column (stride ld); dinv is shared by the columns
 template <typename T>
 struct ApplyArgs {
   const T *u, *b, *dinv;
   T *y, *y2;
   T invtheta, theta, c1, c2;
+  int64_t ld;    // column stride (3 * nn), set by the launcher
+  int nchunk;    // z chunks per column, set by the launcher
 };
 
 template <typename T>
 void launch_apply_fused(const Ctx &c, const T *E, int in, int out,
-                        const ApplyArgs<T> &args, cudaStream_t s);
+                        const ApplyArgs<T> &args, cudaStream_t s, int nb = 1);
 void launch_fine_diag(const Ctx &c, double *dinv64, float *dinv32,
                       cudaStream_t s);
 void launch_fine_stencil(const Ctx &c, double *S, cudaStream_t s);
@@ -192,7 +220,7 @@ void launch_apply_stencil(const Level &v, const T *S, const T *u, const T *b,
                           T *y, cudaStream_t s);
 template <typename T>
 void launch_apply_stencil_sym(const Level &v, const T *H, const T *u,
-                              const T *b, T *y, cudaStream_t s);
+                              const T *b, T *y, cudaStream_t s, int nb = 1);
 void launch_stencil_to_half(int64_t nn, const double *S, double *H64,
                             float *H32, cudaStream_t s);
 void launch_galerkin(const Level &fine, const double *Sf, const Level &coarse,
@@ -201,10 +229,10 @@ void launch_stencil_diag(const Level &v, const double *S, double *dinv64,
                          float *dinv32, cudaStream_t s);
 template <typename T>
 void launch_restrict(const Level &fine, const Level &coarse, const T *rf,
-                     T *bc, cudaStream_t s);
+                     T *bc, cudaStream_t s, int nb = 1);
 template <typename T>
 void launch_prolong_add(const Level &fine, const Level &coarse, const T *xc,
-                        T *xf, cudaStream_t s);
+                        T *xf, cudaStream_t s, int nb = 1);
 void launch_to_dense(const Level &v, const double *S, double *A,
                      cudaStream_t s);
 void launch_eye(int64_t n, double *A, cudaStream_t s);
@@ -213,27 +241,30 @@ void launch_soa_to_aos(int64_t nn, const double *S, double *A64, float *A32,
                        cudaStream_t s);
 template <typename T>
 void launch_coarse_gemv(int64_t n, const double *Ainv, const T *b, T *x,
-                        cudaStream_t s);
+                        cudaStream_t s, int nb = 1);
 
 // Chebyshev smoother pieces
 template <typename T>
 void launch_cheb_init(int64_t n, const T *dinv, const T *b, T *r, T *d, T *x,
-                      double inv_theta, bool zero_guess, cudaStream_t s);
+                      double inv_theta, bool zero_guess, cudaStream_t s,
+                      int nb = 1);
 template <typename T>
 void launch_cheb_step(int64_t n, const T *dinv, const T *Ad, T *r, T *d, T *x,
-                      double c1, double c2, cudaStream_t s);
+                      double c1, double c2, cudaStream_t s, int nb = 1);
 
-// vectors and reductions (FP64 accumulation; results in device scalars)
+// vectors and reductions (FP64 accumulation; results in device scalars).
+// With nb columns, n is the length of one column and the scalars of column
+// j are at (pointer) + j * kColScal.
 template <typename T>
 void launch_dot(const Ctx &c, int64_t n, const T *a, const T *b, double *out,
-                double *shift_to, cudaStream_t s);
+                double *shift_to, cudaStream_t s, int nb = 1);
 template <typename T>
 void launch_cg_p(int64_t n, const T *z, T *p, const double *scal, bool first,
-                 cudaStream_t s);
+                 cudaStream_t s, int nb = 1);
 template <typename T>
 void launch_cg_update(const Ctx &c, int64_t n, T *x, T *r, const T *p,
                       const T *q, const double *scal, double *rr,
-                      cudaStream_t s);
+                      cudaStream_t s, int nb = 1);
 void launch_power_normalize(int64_t n, double *a, const double *w,
                             const double *dinv, const double *nrm2,
                             cudaStream_t s);
@@ -241,9 +272,9 @@ void launch_power_start(int64_t n, double *a, cudaStream_t s);
 void launch_scale_diag(int64_t n, double *w, const double *dinv,
                        cudaStream_t s);
 void launch_to_f32_scaled(int64_t n, const double *a, const double *scal,
-                          float *b, cudaStream_t s);
+                          float *b, cudaStream_t s, int nb = 1);
 void launch_axpy_f32(int64_t n, double *U, const float *d, const double *scal,
-                     cudaStream_t s);
+                     cudaStream_t s, int nb = 1);
 void launch_d2f(int64_t n, const double *a, float *b, cudaStream_t s);
 void launch_f2d(int64_t n, const float *a, double *b, cudaStream_t s);
 void launch_fill(int64_t n, double *a, double v, cudaStream_t s);

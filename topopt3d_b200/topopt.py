@@ -395,3 +395,39 @@ class OC:
             return True
         self.iter += 1
         return self.iter >= self.maxiter
+
+
+def optimize(topOpt, optmma, penalties=None, opts=None, callback=None):
+    """The optimisation loop of Main.cpp:130-170: per penalty, MatIntFnc ->
+    FEAssemble -> FESolve -> Function_Call, then Update + re-evaluate until
+    Check() (a do-while, so maxiter updates and maxiter + 1 evaluations).
+    FESolve warm-starts from the previous U (FEAnalysis.cpp:389).
+
+    Returns one record per evaluation (the fields StepOut prints,
+    TopOpt.cpp:372-405, plus the solver outcome)."""
+    hist = []
+    penalties = [topOpt.penal] if penalties is None else list(penalties)
+
+    def evaluate(it):
+        topOpt.MatIntFnc(optmma.xval)
+        topOpt.FEAssemble(opts)
+        info = topOpt.FESolve(opts)
+        f, dfdx, g, dgdx = Function_Base.Function_Call(topOpt)
+        rec = {"penal": topOpt.penal, "iter": it, "f": f, "g": g.tolist(),
+               "values": [fn.values[0] for fn in topOpt.function_list],
+               "change": optmma.Change, "solve": info}
+        hist.append(rec)
+        if callback is not None:
+            callback(rec)
+        return dfdx, g, dgdx
+
+    for p in penalties:
+        topOpt.penal = float(p)
+        optmma.iter = 0
+        dfdx, g, dgdx = evaluate(0)
+        while True:
+            optmma.Update(topOpt, dfdx, g, dgdx)
+            dfdx, g, dgdx = evaluate(optmma.iter + 1)
+            if optmma.Check():
+                break
+    return hist
