@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-multi-rhs", action="store_true")
+    ap.add_argument("--no-buckling", action="store_true")
     # profiling case: set up `--config` and launch one operation `--reps`
     # times with nothing else around it (for ncu captures; prints no line)
     ap.add_argument("--kernel", default=None,
@@ -318,6 +319,8 @@ def run_ours(args, rank, world, local):
     t.set_stream(None)
     if not args.no_multi_rhs:
         line["multi_rhs"] = run_multi_rhs(args, T, P, torch, dev, stream)
+    if not args.no_buckling:
+        line["buckling"] = run_buckling(args, T, P, torch, dev, stream)
 
     if not args.no_e2e:
         line["e2e"] = run_e2e(args, T, P, t, x, world, dev, torch)
@@ -366,6 +369,43 @@ def run_multi_rhs(args, T, P, torch, dev, stream, nrhs=8, reps=3):
             max(v["value"] for k, v in res.items() if k != "block1")
             / res["block1"]["value"], 3)
         out[pname] = res
+    t.set_stream(None)
+    return out
+
+
+def run_buckling(args, T, P, torch, dev, stream, reps=2):
+    """Linear buckling of the 96x48x48 column (698,691 dof): Ks from the
+    FP64 solution and the 6 largest lambda of Ks phi = lambda K phi (block
+    12, relative residual 1e-6), preconditioned by an FP64 or an FP32
+    V-cycle.  Timed per call (Ks assembly + eigensolve) with CUDA events."""
+    cfg = "cfg4"
+    c = P.CONFIGS[cfg]
+    t = build_problem(T, P, cfg)
+    t.set_stream(stream.cuda_stream)
+    t.MatIntFnc(torch.tensor(P.design(cfg), device=dev))
+    o = T.default_opts(rtol=1e-12, maxit=5000)
+    t.FEAssemble(o)
+    t.FESolve(o)
+    out = {"workload": f"{c['nel'][0]}x{c['nel'][1]}x{c['nel'][2]} column, "
+                       f"{3 * t.nNode} dof, 6 largest lambda, block 12, tol 1e-6",
+           "unit": "ms"}
+    for pc, name in ((T.PREC_FP64, "fp64_vcycle"), (T.PREC_MIXED, "fp32_vcycle")):
+        times = []
+        for r in range(reps + 1):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            t.ks_assemble()
+            lam = t.buckling(nev=6, block=12, precond=pc)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            if r:
+                times.append(e0.elapsed_time(e1))
+        out[name] = {"ms": round(statistics.median(times), 2),
+                     "iterations": t.last_eig["iterations"],
+                     "status": t.last_eig["status"],
+                     "max_resid": t.last_eig["max_resid"],
+                     "lambda": [round(float(v), 12) for v in lam]}
     t.set_stream(None)
     return out
 

@@ -170,6 +170,47 @@ TPO_API int tpo_vcycle(tpo_ctx *ctx, const double *r, double *z, int32_t precisi
 /* lambda_max(D^-1 A_l) estimate used by the Chebyshev smoother */
 TPO_API int tpo_level_lambda(const tpo_ctx *ctx, int32_t level, double *lambda);
 
+/* ---- linear buckling (Stability, Buckling.cpp:15-414) ------------------- */
+
+typedef struct {
+  int32_t nev;        /* eigenvalues wanted: the largest of Ks phi = lambda K phi
+                         (target LR, Buckling.cpp:69-70) (6) */
+  int32_t block;      /* block size, nev <= block <= 32 (12) */
+  int32_t maxit;      /* iterations (500, Buckling.cpp:71) */
+  double tol;         /* converged when ||Ks x - lambda K x|| <= tol |lambda|
+                         ||K x|| for the nev leading pairs (1e-6) */
+  int32_t precond;    /* preconditioner: one GMG V-cycle in TPO_PREC_FP64 or
+                         TPO_PREC_MIXED (FP32) arithmetic (FP64) */
+  uint64_t seed;      /* start block seed (1) */
+} tpo_eig_opts;
+
+typedef struct {
+  int32_t status;     /* TPO_OK, TPO_NOT_CONVERGED or TPO_E_BREAKDOWN */
+  int32_t iterations;
+  int32_t nconv;      /* leading pairs within tol */
+  double max_resid;   /* largest relative residual of the nev pairs */
+  double solve_ms;    /* host wall time of the eigensolve */
+} tpo_eig_info;
+
+TPO_API void tpo_default_eig_opts(tpo_eig_opts *opts);
+
+/* Stability::StressFnc (Buckling.cpp:291-361) and the Dirichlet fix of
+ * Buckling.cpp:29-30: Ks = sum_e -Es_e ks_e(U) from the context's current
+ * U (after tpo_fe_solve) and Es = rho^p of the last tpo_mat_int_fnc (E
+ * itself after tpo_set_moduli), fixed rows and columns zero. */
+TPO_API int tpo_ks_assemble(tpo_ctx *ctx);
+/* y = Ks u, nrhs columns (the reference MatMult(Ks)) */
+TPO_API int tpo_ks_apply(tpo_ctx *ctx, const double *u, double *y, int32_t nrhs,
+                 int mem);
+/* the opts->nev largest eigenvalues of Ks phi = lambda K phi, descending,
+ * in lambda[nev] (host); phi (optional, 3*nNode x nev column-major,
+ * K-orthonormal, in `mem`) the eigenvectors.  Replaces the LOPGMRES call of
+ * Stability::Function (Buckling.cpp:58-86) by block LOBPCG preconditioned
+ * with the GMG V-cycle of tpo_fe_assemble.  Needs tpo_fe_assemble and
+ * tpo_ks_assemble. */
+TPO_API int tpo_buckling(tpo_ctx *ctx, const tpo_eig_opts *opts, double *lambda,
+                 double *phi, int mem, tpo_eig_info *info);
+
 /* U, F, x, rho, E, dEdz accessors: which = "U","F","x","rho","E","dEdz" */
 TPO_API int tpo_get_vector(const tpo_ctx *ctx, const char *which, double *out, int mem);
 TPO_API int tpo_set_vector(tpo_ctx *ctx, const char *which, const double *in, int mem);

@@ -47,6 +47,7 @@ class TopOpt {
     status_ = tpo_create(&p, &ctx_);
     if (ctx_) tpo_sizes(ctx_, &nElem, &nNode, &levels);
     tpo_default_solve_opts(&opts);
+    tpo_default_eig_opts(&eig);
   }
   ~TopOpt() { tpo_destroy(ctx_); }
   TopOpt(const TopOpt &) = delete;
@@ -86,6 +87,15 @@ class TopOpt {
     }
     return 0;
   }
+  // Stability (Buckling.cpp:15-361): Ks from the current U, then the
+  // eig.nev largest eigenvalues of Ks phi = lambda K phi (descending)
+  int StressFnc() { return tpo_ks_assemble(ctx_); }
+  int Buckling(std::vector<double> &lambda) {
+    lambda.assign(eig.nev, 0.0);
+    const int rc = tpo_buckling(ctx_, &eig, lambda.data(), nullptr, TPO_MEM_HOST,
+                                &eig_info);
+    return rc < 0 ? rc : 0;
+  }
   std::vector<double> get(const char *which) const {
     const bool nodal = which[0] == 'U' || which[0] == 'F';
     std::vector<double> out(nodal ? 3 * nNode : nElem);
@@ -99,6 +109,8 @@ class TopOpt {
   double eps = 1e-10;            // Material_Interpolation.cpp:28
   tpo_solve_opts opts{};
   tpo_solve_info info{};
+  tpo_eig_opts eig{};
+  tpo_eig_info eig_info{};
   int KUF_reason = 0;
 
  private:

@@ -108,6 +108,11 @@ def _declare(L):
     L.tor_oc_update.restype = C.c_double
     L.tor_oc_update.argtypes = [C.c_int64, _dp, _dp, _dp, _dp, C.c_double, _dp,
                                 C.c_double]
+    L.tor_stress_stiffness_element.argtypes = [_dp, C.c_double, C.c_double, _dp,
+                                               _dp]
+    L.tor_ks_assemble.argtypes = [vp, _dp]
+    L.tor_ks_apply.argtypes = [vp, _dp, _dp]
+    L.tor_get_es.argtypes = [vp, _dp]
 
 
 def _ptr(a):
@@ -272,6 +277,20 @@ class Problem:
                               C.byref(c), _ptr(dx), _ptr(dr))
         return c.value, dx, dr
 
+    # buckling (Buckling.cpp:15-361)
+    def ks_assemble(self, U):
+        self.L.tor_ks_assemble(self.h, np.ascontiguousarray(U, np.float64))
+
+    def ks_apply(self, u):
+        y = np.zeros(3 * self.nn)
+        self.L.tor_ks_apply(self.h, np.ascontiguousarray(u, np.float64), y)
+        return y
+
+    def es(self):
+        out = np.zeros(self.ne)
+        self.L.tor_get_es(self.h, out)
+        return out
+
     def volume(self):
         v = C.c_double(0)
         dv = np.zeros(self.ne)
@@ -283,6 +302,53 @@ class Problem:
         self.L.tor_filter(self.h, np.ascontiguousarray(v, np.float64), out,
                           int(bool(transpose)))
         return out
+
+
+def stress_stiffness_element(u, dx=(1.0, 1.0, 1.0), E0=1.0, nu=0.3):
+    """ks (24x24) of one element for its displacements u (24, reference
+    local node order), Buckling.cpp:313-327."""
+    ks = np.zeros(576)
+    lib().tor_stress_stiffness_element(np.asarray(dx, np.float64), E0, nu,
+                                       np.ascontiguousarray(u, np.float64), ks)
+    return ks.reshape(24, 24)
+
+
+def dense(apply, n):
+    """Dense matrix of a linear operator on R^n by columns (small n)."""
+    A = np.zeros((n, n))
+    e = np.zeros(n)
+    for j in range(n):
+        e[j] = 1.0
+        A[:, j] = apply(e)
+        e[j] = 0.0
+    return A
+
+
+def buckling(pb, nev=6, ncv=None, tol=1e-12, solve_rtol=1e-13, v0_seed=0):
+    """The nev largest eigenvalues of Ks phi = lambda K phi (the target LR
+    of Buckling.cpp:63-70) for an assembled problem whose Ks has been built
+    (ks_assemble).  Independent of the CUDA path's eigensolver: ARPACK
+    Lanczos (scipy eigsh, generalized mode with M = K) whose M^-1 is the
+    oracle's PCG + GMG solve to solve_rtol.  Returns (lambda descending,
+    phi as rows, K-normalised)."""
+    import scipy.sparse.linalg as spl
+    n = 3 * pb.nn
+    o = default_opts(rtol=solve_rtol, maxit=5000)
+    A = spl.LinearOperator((n, n), matvec=pb.ks_apply, dtype=np.float64)
+    M = spl.LinearOperator((n, n), matvec=pb.apply, dtype=np.float64)
+
+    def minv(b):
+        U, st, _, _ = pb.solve(b=np.ascontiguousarray(b, np.float64).ravel(), opts=o)
+        if st != 0:
+            raise RuntimeError(f"oracle solve failed (status {st})")
+        return U
+
+    Minv = spl.LinearOperator((n, n), matvec=minv, dtype=np.float64)
+    v0 = np.random.default_rng(v0_seed).standard_normal(n)
+    lam, phi = spl.eigsh(A, k=nev, M=M, Minv=Minv, which="LA", tol=tol,
+                         ncv=ncv or max(2 * nev + 1, 20), v0=v0)
+    order = np.argsort(lam)[::-1]
+    return lam[order], phi[:, order].T
 
 
 def oc_update(x, dfdx, g, dgdx, move, xmin=None, xmax=None):

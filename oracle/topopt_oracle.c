@@ -372,6 +372,8 @@ struct tor_problem {
   double *fval;
   /* material */
   double *x, *rho, *E, *dEdz;
+  double *Es;         /* rho^p without E_min (Material_Interpolation.cpp:69) */
+  bsr3 Ks;            /* stress stiffness (Buckling.cpp:291-361) */
   /* hierarchy */
   int L;
   level_t *lev;
@@ -399,6 +401,7 @@ tor_problem *tor_create(const tor_params *p)
   P->rho = (double *)calloc(P->ne, sizeof(double));
   P->E = (double *)calloc(P->ne, sizeof(double));
   P->dEdz = (double *)calloc(P->ne, sizeof(double));
+  P->Es = (double *)calloc(P->ne, sizeof(double));
   P->L = p->mg_levels < 1 ? 1 : p->mg_levels;
   P->lev = (level_t *)calloc(P->L, sizeof(level_t));
   return P;
@@ -426,7 +429,8 @@ void tor_destroy(tor_problem *P)
   free(P->lev);
   free(P->fix); free(P->F);
   free(P->frow); free(P->fcol); free(P->fval);
-  free(P->x); free(P->rho); free(P->E); free(P->dEdz);
+  free(P->x); free(P->rho); free(P->E); free(P->dEdz); free(P->Es);
+  bsr_free(&P->Ks);
   free(P);
 }
 
@@ -476,7 +480,7 @@ void tor_set_design(tor_problem *P, const double *x, double penal, double eps)
   /* MatIntFnc (Material_Interpolation.cpp:20-75), vdMin <= 0 */
   memcpy(P->x, x, sizeof(double) * P->ne);
   tor_csr_mult(P->ne, P->frow, P->fcol, P->fval, P->x, P->rho);   /* :35 */
-  tor_simp(P->ne, P->rho, penal, eps, P->E, P->dEdz, NULL, NULL);
+  tor_simp(P->ne, P->rho, penal, eps, P->E, P->dEdz, P->Es, NULL);
 }
 
 void tor_get_material(const tor_problem *P, double *rho, double *E, double *dEdz)
@@ -1086,4 +1090,181 @@ double tor_oc_update(int64_t n, double *x, const double *xmin, const double *xma
   }
   free(xold);
   return change;
+}
+
+/* ------------------------------------------------------------------------ */
+/* stress stiffness (buckling)                                               */
+/* ------------------------------------------------------------------------ */
+
+void tor_stress_stiffness_element(const double dx[3], double E0, double nu,
+                                  const double u[24], double ks[576])
+{
+  /* Stability::StressFnc (Buckling.cpp:313-327): ks = sum_q W_q G_q^T
+   * sigtos(d B_q u) G_q detJ, with G from TopOpt::AssignG
+   * (FEAnalysis.cpp:1062-1081): row 3i + j, column 3n + i holds dN_n/dx_j,
+   * i.e. G u stacks the gradients of the three displacement components;
+   * sigtos (Buckling.cpp:371-414) repeats the 3x3 stress tensor of the
+   * Voigt vector [xx, yy, zz, xy, yz, xz] on the diagonal.  u is in the
+   * reference's local node order (dN, FEAnalysis.cpp:955-986). */
+  double D[36];
+  tor_constitutive(E0, nu, D);
+  double coords[8][3];
+  for (int n = 0; n < 8; n++)
+    for (int d = 0; d < 3; d++) coords[n][d] = kNodeSign[n][d] > 0 ? dx[d] : 0.0;
+  memset(ks, 0, 576 * sizeof(double));
+  const double g = 1.0 / sqrt(3.0);
+  for (int q = 0; q < 8; q++) {
+    double xi = kNodeSign[q][0] * g, eta = kNodeSign[q][1] * g,
+           zeta = kNodeSign[q][2] * g;
+    double dNdxi[3][8];
+    for (int n = 0; n < 8; n++) {
+      double a = kNodeSign[n][0], b = kNodeSign[n][1], c = kNodeSign[n][2];
+      dNdxi[0][n] = a * (1 + b * eta) * (1 + c * zeta) / 8.0;
+      dNdxi[1][n] = b * (1 + a * xi) * (1 + c * zeta) / 8.0;
+      dNdxi[2][n] = c * (1 + a * xi) * (1 + b * eta) / 8.0;
+    }
+    double J[9] = {0}, iJ[9];
+    for (int r = 0; r < 3; r++)
+      for (int cc = 0; cc < 3; cc++)
+        for (int n = 0; n < 8; n++) J[3 * r + cc] += dNdxi[r][n] * coords[n][cc];
+    double detJ = det3(J);
+    inv3(J, iJ);
+    double dNdx[3][8];
+    for (int r = 0; r < 3; r++)
+      for (int n = 0; n < 8; n++) {
+        double t = 0;
+        for (int k = 0; k < 3; k++) t += iJ[3 * r + k] * dNdxi[k][n];
+        dNdx[r][n] = t;
+      }
+    /* B (AssignB, FEAnalysis.cpp:1024-1046) and sigma = d B u */
+    double B[6][24];
+    memset(B, 0, sizeof(B));
+    for (int n = 0; n < 8; n++) {
+      B[0][3 * n] = dNdx[0][n];
+      B[1][3 * n + 1] = dNdx[1][n];
+      B[2][3 * n + 2] = dNdx[2][n];
+      B[3][3 * n] = dNdx[1][n];
+      B[3][3 * n + 1] = dNdx[0][n];
+      B[4][3 * n + 1] = dNdx[2][n];
+      B[4][3 * n + 2] = dNdx[1][n];
+      B[5][3 * n] = dNdx[2][n];
+      B[5][3 * n + 2] = dNdx[0][n];
+    }
+    double eps_v[6], sig[6];
+    for (int r = 0; r < 6; r++) {
+      double t = 0;
+      for (int c = 0; c < 24; c++) t += B[r][c] * u[c];
+      eps_v[r] = t;
+    }
+    for (int r = 0; r < 6; r++) {
+      double t = 0;
+      for (int k = 0; k < 6; k++) t += D[6 * r + k] * eps_v[k];
+      sig[r] = t;
+    }
+    /* sigtos */
+    double S[9][9];
+    memset(S, 0, sizeof(S));
+    double s3[3][3] = {{sig[0], sig[3], sig[5]},
+                       {sig[3], sig[1], sig[4]},
+                       {sig[5], sig[4], sig[2]}};
+    for (int b = 0; b < 3; b++)
+      for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) S[3 * b + r][3 * b + c] = s3[r][c];
+    /* G (AssignG) */
+    double G[9][24];
+    memset(G, 0, sizeof(G));
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++)
+        for (int n = 0; n < 8; n++) G[3 * i + j][3 * n + i] = dNdx[j][n];
+    double SG[9][24];
+    for (int r = 0; r < 9; r++)
+      for (int c = 0; c < 24; c++) {
+        double t = 0;
+        for (int k = 0; k < 9; k++) t += S[r][k] * G[k][c];
+        SG[r][c] = t;
+      }
+    for (int r = 0; r < 24; r++)
+      for (int c = 0; c < 24; c++) {
+        double t = 0;
+        for (int k = 0; k < 9; k++) t += G[k][r] * SG[k][c];
+        ks[24 * r + c] += t * detJ;   /* W[q] = 1 */
+      }
+  }
+}
+
+void tor_ks_assemble(tor_problem *P, const double *U)
+{
+  /* Ks = sum_e -Es_e ks_e (Buckling.cpp:329-352, Es without E_min, :343),
+   * then MatZeroRowsColumns(Ks, fixedDof, 0.0) (:29-30).  Same block
+   * pattern as K; elements are visited in 8 parity classes so that the
+   * elements of one class touch disjoint blocks (parallel without races). */
+  const int *nel = P->prm.nel;
+  int64_t Nx = nel[0] + 1, Ny = nel[1] + 1, Nz = nel[2] + 1, nn = P->nn;
+  bsr3 *A = &P->Ks;
+  bsr_free(A);
+  A->n = nn;
+  A->rowptr = (int64_t *)malloc(sizeof(int64_t) * (nn + 1));
+  A->rowptr[0] = 0;
+  for (int64_t n = 0; n < nn; n++) {
+    int64_t i = n % Nx, j = (n / Nx) % Ny, k = n / (Nx * Ny);
+    int cx = 1 + (i > 0) + (i < Nx - 1), cy = 1 + (j > 0) + (j < Ny - 1),
+        cz = 1 + (k > 0) + (k < Nz - 1);
+    A->rowptr[n + 1] = A->rowptr[n] + cx * cy * cz;
+  }
+  A->col = (int32_t *)malloc(sizeof(int32_t) * A->rowptr[nn]);
+  A->val = (double *)calloc(9 * (size_t)A->rowptr[nn], sizeof(double));
+  for (int64_t n = 0; n < nn; n++) {
+    int64_t i = n % Nx, j = (n / Nx) % Ny, k = n / (Nx * Ny);
+    int64_t t = A->rowptr[n];
+    for (int dk = -1; dk <= 1; dk++)
+      for (int dj = -1; dj <= 1; dj++)
+        for (int di = -1; di <= 1; di++) {
+          int64_t mi = i + di, mj = j + dj, mk = k + dk;
+          if (mi < 0 || mi >= Nx || mj < 0 || mj >= Ny || mk < 0 || mk >= Nz)
+            continue;
+          A->col[t++] = (int32_t)(mi + mj * Nx + mk * Nx * Ny);
+        }
+  }
+  for (int color = 0; color < 8; color++) {
+    int pi = color & 1, pj = (color >> 1) & 1, pk = (color >> 2) & 1;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t ek = pk; ek < nel[2]; ek += 2)
+      for (int64_t ej = pj; ej < nel[1]; ej += 2)
+        for (int64_t ei = pi; ei < nel[0]; ei += 2) {
+          int64_t e = ei + ej * nel[0] + ek * (int64_t)nel[0] * nel[1];
+          int64_t nodes[8];
+          tor_element_nodes(nel, e, nodes);
+          double u[24], ks[576];
+          for (int a = 0; a < 8; a++)
+            for (int d = 0; d < 3; d++) u[3 * a + d] = U[3 * nodes[a] + d];
+          tor_stress_stiffness_element(P->prm.dx, P->prm.E0, P->prm.nu, u, ks);
+          double w = -P->Es[e];
+          for (int a = 0; a < 8; a++)
+            for (int b = 0; b < 8; b++) {
+              double *blk = (double *)bsr_find(A, nodes[a], nodes[b]);
+              for (int r = 0; r < 3; r++)
+                for (int c = 0; c < 3; c++)
+                  blk[3 * r + c] += w * ks[24 * (3 * a + r) + 3 * b + c];
+            }
+        }
+  }
+#pragma omp parallel for schedule(static)
+  for (int64_t n = 0; n < nn; n++)
+    for (int64_t t = A->rowptr[n]; t < A->rowptr[n + 1]; t++) {
+      int64_t m = A->col[t];
+      double *blk = A->val + 9 * t;
+      for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++)
+          if (((P->fix[n] >> r) & 1) || ((P->fix[m] >> c) & 1)) blk[3 * r + c] = 0.0;
+    }
+}
+
+void tor_ks_apply(const tor_problem *P, const double *u, double *y)
+{
+  bsr_mult(&P->Ks, u, y);
+}
+
+void tor_get_es(const tor_problem *P, double *Es)
+{
+  memcpy(Es, P->Es, sizeof(double) * P->ne);
 }

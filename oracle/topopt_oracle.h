@@ -152,6 +152,18 @@ double tor_oc_update(int64_t n, double *x, const double *xmin,
                      const double *xmax, double *dfdx, double g,
                      const double *dgdx, double move);
 
+
+/* ---- buckling ------------------------------------------------------------ */
+/* element stress stiffness ks (24x24, row-major, reference local node order)
+ * for element displacements u (Buckling.cpp:313-327) */
+void tor_stress_stiffness_element(const double dx[3], double E0, double nu,
+                                  const double u[24], double ks[576]);
+/* Ks = sum_e -Es_e ks_e(U) with the Dirichlet rows/columns zeroed
+ * (Buckling.cpp:22-30, 291-361) */
+void tor_ks_assemble(tor_problem *P, const double *U);
+void tor_ks_apply(const tor_problem *P, const double *u, double *y);
+void tor_get_es(const tor_problem *P, double *Es);
+
 #ifdef __cplusplus
 }
 #endif

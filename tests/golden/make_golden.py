@@ -125,6 +125,37 @@ def oc_trajectory(name, cfg, iters, volfrac=0.3, rtol=1e-10):
           f"V[-1] = {h['V'][-1]:.12g}")
 
 
+def buckling_fixture(name, cfg, nel=None, levels=None, nev=6, dense_check=False):
+    """The oracle's buckling eigenvalues (ARPACK over the oracle's Ks and
+    PCG + GMG solves) of a configuration's column; small cases are
+    cross-checked against a dense generalized eigensolve at generation."""
+    import scipy.linalg as sla
+    c = P.CONFIGS[cfg]
+    nel = nel or c["nel"]
+    levels = levels or c["levels"]
+    pb = O.Problem(nel, rmin=c["rmin"], mg_levels=levels)
+    P.apply_bcs(pb, P.bcs(cfg, nel))
+    pb.set_design(P.design(cfg, nel), 3.0, 1e-10)
+    o = O.default_opts(rtol=1e-12, maxit=5000)
+    pb.assemble(o)
+    U, st, its, rr = pb.solve(opts=o)
+    assert st == 0, (name, st)
+    C, _, _ = pb.compliance(U)
+    pb.ks_assemble(U)
+    lam, phi = O.buckling(pb, nev=nev)
+    out = dict(cfg=cfg, nel=np.array(nel), levels=levels, nev=nev, lam=lam, C=C,
+               solve_rtol=1e-12)
+    if dense_check:
+        n = 3 * pb.nn
+        w = sla.eigh(O.dense(pb.ks_apply, n), O.dense(pb.apply, n),
+                     eigvals_only=True)[::-1][:nev]
+        err = np.max(np.abs(w - lam) / np.abs(w))
+        assert err < 1e-10, (name, err)
+        out["dense_err"] = err
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(f"{name}: lambda = {np.array2string(lam, precision=12)}")
+
+
 def main():
     nel = (12, 6, 6)
     x = np.random.default_rng(7).uniform(0.1, 1.0, int(np.prod(nel)))
@@ -135,6 +166,9 @@ def main():
     nel = P.CONFIGS["cfg0"]["nel"]
     case("cfg0_48x24x24", nel, 3, 1.5, P.design("cfg0"), P.bcs("cfg0"), False)
     oc_trajectory("oc_cfg3_64x32x32", "cfg3", 50)
+    buckling_fixture("buckling_column_8x4x8", "cfg4", nel=(8, 4, 8), levels=2,
+                     dense_check=True)
+    buckling_fixture("buckling_cfg4_96x48x48", "cfg4")
 
 
 if __name__ == "__main__":

@@ -1,0 +1,167 @@
+"""Linear buckling (Stability, Buckling.cpp:15-414): the stress stiffness Ks
+and the largest eigenvalues of Ks phi = lambda K phi.
+
+CPU: the oracle's literal element ks (G and sigtos as the reference builds
+them) against an independent numpy form (the scalar matrix
+H = sum_q grad N^T sigma grad N detJ, ks = H (x) I_3), and the oracle's
+eigenvalues against the committed fixtures (tests/golden/make_golden.py:
+ARPACK over the oracle, cross-checked by a dense generalized eigensolve on
+the small column).
+
+GPU: Ks apply against the oracle's assembled Ks to round-off, and the
+LOBPCG eigenvalues against the fixtures to 1e-6 relative (the bar for the
+96x48x48 column; in practice they agree far closer), with the eigenpair
+residuals checked through the C ABI.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from topopt3d_b200 import problems as P
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def fixture(name):
+    return dict(np.load(os.path.join(GOLD, name + ".npz")))
+
+
+def numpy_ks(u, E0=1.0, nu=0.3):
+    """Independent element stress stiffness for u in the reference local
+    node order: H (x) I_3 with H = sum_q grad N^T sigma grad N detJ."""
+    c = E0 / ((1 + nu) * (1 - 2 * nu))
+    lam_, mu = nu * c, E0 / (2 * (1 + nu))
+    sg = np.array([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1],
+                   [-1, -1, 1], [1, -1, 1], [1, 1, 1], [-1, 1, 1]], float)
+    g = 1 / np.sqrt(3)
+    U = u.reshape(8, 3)
+    H = np.zeros((8, 8))
+    for q in sg * g:
+        dN = np.array([[s[0] * (1 + s[1] * q[1]) * (1 + s[2] * q[2]),
+                        s[1] * (1 + s[0] * q[0]) * (1 + s[2] * q[2]),
+                        s[2] * (1 + s[0] * q[0]) * (1 + s[1] * q[1])]
+                       for s in sg]).T / 8 * 2      # 3 x 8, unit cube
+        F = U.T @ dN.T                               # F[c][a] = du_c/dx_a
+        eps = 0.5 * (F + F.T)
+        sig = lam_ * np.trace(eps) * np.eye(3) + 2 * mu * eps
+        H += dN.T @ sig @ dN / 8.0                   # detJ = 1/8
+    return np.kron(H, np.eye(3))
+
+
+def test_oracle_ks_element_matches_numpy(oracle):
+    rng = np.random.default_rng(11)
+    for _ in range(3):
+        u = rng.standard_normal(24)
+        ks = oracle.stress_stiffness_element(u)
+        ref = numpy_ks(u)
+        assert np.abs(ks - ref).max() < 1e-13 * np.abs(ref).max()
+    # a rigid translation carries no stress
+    assert np.abs(oracle.stress_stiffness_element(np.tile([1.0, -2.0, 0.5], 8))).max() < 1e-14
+
+
+def test_oracle_buckling_reproduces_fixture(oracle):
+    g = fixture("buckling_column_8x4x8")
+    nel = tuple(int(v) for v in g["nel"])
+    c = P.CONFIGS[str(g["cfg"])]
+    pb = oracle.Problem(nel, rmin=c["rmin"], mg_levels=int(g["levels"]))
+    P.apply_bcs(pb, P.bcs(str(g["cfg"]), nel))
+    pb.set_design(P.design(str(g["cfg"]), nel), 3.0, 1e-10)
+    o = oracle.default_opts(rtol=float(g["solve_rtol"]), maxit=5000)
+    pb.assemble(o)
+    U, st, _, _ = pb.solve(opts=o)
+    pb.ks_assemble(U)
+    lam, _ = oracle.buckling(pb, nev=int(g["nev"]))
+    np.testing.assert_allclose(lam, g["lam"], rtol=1e-9)
+    assert float(g["dense_err"]) < 1e-10
+
+
+def gpu_problem(T, g, precision_rtol=1e-12):
+    nel = tuple(int(v) for v in g["nel"])
+    cfg = str(g["cfg"])
+    c = P.CONFIGS[cfg]
+    t = T.TopOpt(nel, rmin=c["rmin"], mg_levels=int(g["levels"]))
+    P.apply_bcs(t, P.bcs(cfg, nel))
+    t.FEInitialize()
+    t.MatIntFnc(P.design(cfg, nel))
+    o = T.default_opts(rtol=precision_rtol, maxit=5000)
+    t.FEAssemble(o)
+    info = t.FESolve(o)
+    assert info["status"] == 0
+    t.ks_assemble()
+    return t
+
+
+@pytest.mark.gpu
+def test_ks_apply_matches_oracle(T, oracle):
+    """Ks from the same U on both sides, applied to 5 random columns."""
+    nel = (10, 6, 9)
+    spec = P.column_bcs(nel)
+    x = np.random.default_rng(21).uniform(0.2, 1.0, int(np.prod(nel)))
+    ref = oracle.Problem(nel, rmin=1.5, mg_levels=2)
+    P.apply_bcs(ref, spec)
+    ref.set_design(x, 3.0, 1e-10)
+    o = oracle.default_opts(rtol=1e-13, maxit=2000)
+    ref.assemble(o)
+    U, st, _, _ = ref.solve(opts=o)
+    ref.ks_assemble(U)
+    t = T.TopOpt(nel, rmin=1.5, mg_levels=2)
+    P.apply_bcs(t, spec)
+    t.FEInitialize()
+    t.MatIntFnc(x)
+    t.set("U", U)
+    t.ks_assemble()
+    rng = np.random.default_rng(5)
+    u = rng.standard_normal((5, 3 * t.nNode))
+    y = np.zeros_like(u)
+    t.ks_apply(u, y, nrhs=5)
+    for j in range(5):
+        yo = ref.ks_apply(u[j])
+        assert np.abs(y[j] - yo).max() <= 1e-12 * np.abs(yo).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precond", ["fp64", "mixed"])
+def test_buckling_small_column(T, precond):
+    g = fixture("buckling_column_8x4x8")
+    t = gpu_problem(T, g)
+    pc = T.PREC_FP64 if precond == "fp64" else T.PREC_MIXED
+    lam, phi = t.buckling(want_vectors=True, nev=int(g["nev"]), block=12,
+                          tol=1e-8, precond=pc)
+    assert t.last_eig["status"] == 0, t.last_eig
+    np.testing.assert_allclose(lam, g["lam"], rtol=1e-9)
+    # eigenpair residuals and K-orthonormality through the ABI
+    n = phi.shape[1]
+    A = np.zeros_like(phi)
+    B = np.zeros_like(phi)
+    t.ks_apply(phi, A, nrhs=phi.shape[0])
+    t.apply(phi, B, nrhs=phi.shape[0])
+    for j in range(phi.shape[0]):
+        r = A[j] - lam[j] * B[j]
+        assert np.linalg.norm(r) <= 1e-7 * abs(lam[j]) * np.linalg.norm(B[j])
+    G = phi @ B.T
+    assert np.abs(G - np.eye(phi.shape[0])).max() < 1e-8
+    assert n == 3 * t.nNode
+
+
+@pytest.mark.gpu
+def test_buckling_cfg4(T):
+    """The 96x48x48 column (698,691 dof): the 6 largest lambda, block 12,
+    against the oracle's ARPACK eigenvalues to 1e-6 relative."""
+    g = fixture("buckling_cfg4_96x48x48")
+    t = gpu_problem(T, g)
+    lam = t.buckling(nev=int(g["nev"]), block=12)
+    assert t.last_eig["status"] == 0, t.last_eig
+    np.testing.assert_allclose(lam, g["lam"], rtol=1e-6)
+
+
+@pytest.mark.gpu
+def test_stability_function(T):
+    g = fixture("buckling_column_8x4x8")
+    t = gpu_problem(T, g)
+    f = T.Stability([1.0], 0.0, 1.0, objective=True)
+    f.Compute(t)
+    expect = np.sum(np.asarray(g["lam"]) ** 8) ** (1 / 8)
+    assert abs(f.values[0] - expect) <= 1e-8 * expect
+    with pytest.raises(T.TopOptError):
+        T.Stability([1.0], 0.0, 1.0, calc_gradient=True)

@@ -6,11 +6,13 @@ implements the SIMP hex8 stiffness apply, the GMG-preconditioned CG solve
 filter.  ``TopOpt`` mirrors the reference's call surface.
 """
 from ._lib import (BC_LOAD, BC_SUPPORT, MEM_DEVICE, MEM_HOST, PREC_FP64,
-                   PREC_MIXED, SolveInfo, SolveOpts, default_opts, load)
-from .topopt import (OC, Compliance, Function_Base, TopOpt, TopOptError, Volume,
-                     optimize)
+                   PREC_MIXED, EigInfo, EigOpts, SolveInfo, SolveOpts,
+                   default_eig_opts, default_opts, load)
+from .topopt import (OC, Compliance, Function_Base, Stability, TopOpt,
+                     TopOptError, Volume, optimize)
 
 __all__ = ["TopOpt", "TopOptError", "Compliance", "Volume", "Function_Base",
-           "OC", "optimize", "SolveOpts", "SolveInfo", "default_opts", "load",
+           "OC", "optimize", "Stability", "EigOpts", "EigInfo",
+           "default_eig_opts", "SolveOpts", "SolveInfo", "default_opts", "load",
            "PREC_FP64", "PREC_MIXED", "MEM_HOST", "MEM_DEVICE", "BC_SUPPORT",
            "BC_LOAD"]

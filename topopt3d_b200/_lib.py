@@ -33,7 +33,8 @@ EXPORTS = (
     "tpo_apply_level", "tpo_vcycle", "tpo_level_lambda", "tpo_get_vector",
     "tpo_set_vector", "tpo_compliance", "tpo_volume", "tpo_filter",
     "tpo_oc_update", "tpo_sync", "tpo_set_stream", "tpo_kernel_launches",
-    "tpo_sensitivity_noalloc",
+    "tpo_sensitivity_noalloc", "tpo_default_eig_opts", "tpo_ks_assemble",
+    "tpo_ks_apply", "tpo_buckling",
 )
 NOALLOC_MAX_ELEMS = 1 << 20
 
@@ -57,6 +58,20 @@ class SolveInfo(C.Structure):
     _fields_ = [("status", C.c_int32), ("iterations", C.c_int32),
                 ("outer", C.c_int32), ("relres", C.c_double),
                 ("solve_ms", C.c_double), ("setup_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class EigOpts(C.Structure):
+    _fields_ = [("nev", C.c_int32), ("block", C.c_int32), ("maxit", C.c_int32),
+                ("tol", C.c_double), ("precond", C.c_int32), ("seed", C.c_uint64)]
+
+
+class EigInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("iterations", C.c_int32),
+                ("nconv", C.c_int32), ("max_resid", C.c_double),
+                ("solve_ms", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -110,6 +125,11 @@ def load(path: str | None = None):
         "tpo_kernel_launches": (C.c_int64, []),
         "tpo_sensitivity_noalloc": (C.c_int, [C.POINTER(i32), dp, d, d, d, vp, vp,
                                               vp, vp, C.c_char_p, i32]),
+        "tpo_default_eig_opts": (None, [C.POINTER(EigOpts)]),
+        "tpo_ks_assemble": (C.c_int, [vp]),
+        "tpo_ks_apply": (C.c_int, [vp, vp, vp, i32, C.c_int]),
+        "tpo_buckling": (C.c_int, [vp, C.POINTER(EigOpts), dp, vp, C.c_int,
+                                   C.POINTER(EigInfo)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -122,6 +142,16 @@ def load(path: str | None = None):
 def default_opts(**kw) -> SolveOpts:
     o = SolveOpts()
     load().tpo_default_solve_opts(C.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise AttributeError(k)
+        setattr(o, k, v)
+    return o
+
+
+def default_eig_opts(**kw) -> EigOpts:
+    o = EigOpts()
+    load().tpo_default_eig_opts(C.byref(o))
     for k, v in kw.items():
         if not hasattr(o, k):
             raise AttributeError(k)

@@ -1,6 +1,7 @@
 // The C ABI (include/topopt_b200.h): context life cycle, boundary
 // conditions, the TopOpt call surface and data movement between caller
 // buffers and the context's HBM-resident state.
+#include <cublas_v2.h>
 #include <cusolverDn.h>
 
 #include <algorithm>
@@ -153,16 +154,6 @@ void free_columns(Ctx &c) {
   dfree(c.io_ba); dfree(c.io_bb);
 }
 
-// room for nb columns: the column vectors are re-allocated for kMaxBatch
-// columns the first time a block of more than one is asked for
-int ensure_columns(Ctx &c, int nb) {
-  if (nb <= c.nb_cap) return TPO_OK;
-  CK(cudaStreamSynchronize(c.stream));
-  tpo::invalidate_graphs(c);
-  free_columns(c);
-  c.nb_cap = tpo::kMaxBatch;
-  return alloc_columns(c);
-}
 
 int alloc_solver(Ctx &c) {
   int rc = 0;
@@ -206,6 +197,10 @@ void free_all(Ctx &c) {
   dfree(c.Ainv); dfree(c.Adense); dfree(c.solver_work); dfree(c.dev_info);
   dfree(c.finv); dfree(c.taps_d);
   dfree(c.w64);
+  dfree(c.Es64); dfree(c.ks_S); dfree(c.ks_H); dfree(c.eig_buf);
+  c.eig_n = 0;
+  if (c.cublas) cublasDestroy(static_cast<cublasHandle_t>(c.cublas));
+  c.cublas = nullptr;
   dfree(c.scal); dfree(c.part); dfree(c.ticket); dfree(c.tmpe); dfree(c.tmpe2);
   dfree(c.io_a); dfree(c.io_b);
   dfree(c.oc_ws);
@@ -229,6 +224,21 @@ double *vec_ptr(Ctx &c, const char *which, size_t *n) {
 }
 
 }  // namespace
+
+namespace tpo {
+// room for nb columns: the column vectors are re-allocated for kMaxBatch
+// columns the first time a block of more than one is asked for
+int ensure_columns(Ctx &c, int nb) {
+  if (nb <= c.nb_cap) return TPO_OK;
+  CK(cudaStreamSynchronize(c.stream));
+  tpo::invalidate_graphs(c);
+  free_columns(c);
+  c.nb_cap = tpo::kMaxBatch;
+  return alloc_columns(c);
+}
+}  // namespace tpo
+
+using tpo::ensure_columns;
 
 extern "C" {
 
@@ -332,6 +342,7 @@ int tpo_create(const tpo_mesh_params *p, tpo_ctx **out) {
   A(c.taps_d, 1);
   A(c.finv, c.ne); A(c.K0lex, 576);
   A(c.x, c.ne); A(c.rho, c.ne); A(c.E64, c.ne); A(c.dEdz, c.ne); A(c.E32, c.ne);
+  A(c.Es64, c.ne);
   A(c.fix, c.nn); A(c.F, 3 * c.nn); A(c.U, 3 * c.nn);
   A(c.scal, tpo::kScalCount); A(c.part, tpo::kPartCount); A(c.ticket, tpo::kMaxBatch);
   A(c.tmpe, c.ne); A(c.tmpe2, c.ne); A(c.dev_info, 1);
@@ -492,6 +503,8 @@ int tpo_set_moduli(tpo_ctx *ctx, const double *E, const double *dEdz, int mem) {
   CK(cudaMemcpyAsync(c.E64, E, sizeof(double) * c.ne, k, c.stream));
   if (dEdz) CK(cudaMemcpyAsync(c.dEdz, dEdz, sizeof(double) * c.ne, k, c.stream));
   tpo::launch_d2f(c.ne, c.E64, c.E32, c.stream);
+  // given moduli carry no E_min split: the stress stiffness uses E itself
+  CK(cudaMemcpyAsync(c.Es64, c.E64, sizeof(double) * c.ne, cudaMemcpyDeviceToDevice, c.stream));
   CK(cudaStreamSynchronize(c.stream));
   c.have_material = true;
   c.assembled = false;
@@ -657,6 +670,74 @@ int tpo_apply(tpo_ctx *ctx, const double *u, double *y, int32_t nrhs,
     j0 += nb;
   }
   return finish(c, TPO_OK);
+}
+
+void tpo_default_eig_opts(tpo_eig_opts *o) {
+  if (!o) return;
+  o->nev = 6;
+  o->block = 12;
+  o->maxit = 500;
+  o->tol = 1e-6;
+  o->precond = TPO_PREC_FP64;
+  o->seed = 1;
+}
+
+int tpo_ks_assemble(tpo_ctx *ctx) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  REQUIRE(c.initialized && c.have_material, "mesh not initialised or no material");
+  if (!c.ks_S) CK(cudaMalloc(&c.ks_S, sizeof(double) * 27 * c.nn));
+  if (!c.ks_H) CK(cudaMalloc(&c.ks_H, sizeof(double) * 36 * c.ne));
+  tpo::launch_ks_assemble(c, c.stream);
+  CK(cudaStreamSynchronize(c.stream));
+  c.ks_ready = true;
+  return finish(c, TPO_OK);
+}
+
+int tpo_ks_apply(tpo_ctx *ctx, const double *u, double *y, int32_t nrhs, int mem) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = check_mem(c, mem)) return rc;
+  REQUIRE(u && y && nrhs >= 1, "invalid apply arguments");
+  REQUIRE(c.ks_ready, "tpo_ks_assemble must be called first");
+  const size_t n = 3 * c.nn;
+  for (int j0 = 0; j0 < nrhs;) {
+    const int nb = std::min<int>(nrhs - j0, tpo::kMaxBatch);
+    if (int rc = ensure_columns(c, nb)) return rc;
+    const double *du = u + j0 * n;
+    double *dy = y + j0 * n;
+    if (mem != TPO_MEM_DEVICE) {
+      double *sa = nb > 1 ? c.io_ba : c.io_a;
+      CK(cudaMemcpyAsync(sa, du, sizeof(double) * n * nb, cudaMemcpyHostToDevice, c.stream));
+      du = sa;
+      dy = nb > 1 ? c.io_bb : c.io_b;
+    }
+    tpo::launch_ks_apply(c, du, dy, nb);
+    if (int rc = copy_out(c, y + j0 * n, dy, n * nb, mem)) return rc;
+    j0 += nb;
+  }
+  return finish(c, TPO_OK);
+}
+
+int tpo_buckling(tpo_ctx *ctx, const tpo_eig_opts *opts, double *lambda,
+                 double *phi, int mem, tpo_eig_info *info) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = check_mem(c, mem)) return rc;
+  tpo_eig_opts o;
+  if (opts) o = *opts; else tpo_default_eig_opts(&o);
+  REQUIRE(lambda, "null lambda");
+  REQUIRE(c.assembled, "tpo_fe_assemble must be called first (preconditioner)");
+  REQUIRE(c.ks_ready, "tpo_ks_assemble must be called first");
+  REQUIRE(o.nev >= 1 && o.block >= o.nev && o.block <= 32, "need 1 <= nev <= block <= 32");
+  REQUIRE(o.tol > 0 && o.maxit >= 0, "invalid tol/maxit");
+  REQUIRE(o.precond == TPO_PREC_FP64 || o.precond == TPO_PREC_MIXED, "invalid precond");
+  REQUIRE((int64_t)o.block <= 3 * c.nn, "block exceeds the number of dofs");
+  tpo_eig_info one{};
+  const int rc = tpo::buckling(c, o, lambda, phi, mem, &one);
+  if (info) *info = one;
+  if (rc < 0 && rc != TPO_E_BREAKDOWN) return finish(c, rc);
+  return finish(c, rc);
 }
 
 int tpo_apply_f32(tpo_ctx *ctx, const float *u, float *y) {

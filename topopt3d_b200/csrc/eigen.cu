@@ -1,0 +1,459 @@
+// Linear buckling eigenproblem: the nev largest lambda of
+//   Ks phi = lambda K phi
+// (Stability::Function, Buckling.cpp:63-75: target LR of (Ks, K), with the
+// KUF preconditioner, Buckling.cpp:63-64).  The reference runs its own
+// preconditioned eigensolver (LOPGMRES over PRINVIT, single-vector
+// expansion); here the same family -- a locally optimal preconditioned
+// method -- runs as BLOCK LOBPCG so every operator application is a column
+// block: Ks (kernels_ks.cu) and K (the matrix-free apply) on m columns, and
+// the GMG V-cycle (the solve's own preconditioner) in blocks of <= 8.
+//
+// Per iteration, with X the m current Ritz vectors (AX = Ks X, BX = K X):
+//   R = AX - BX diag(theta);  W = mask(T R)  (T = one V-cycle)
+//   Rayleigh-Ritz of (Ks, K) on span[X W P]: Gram blocks by DGEMM, the
+//   small generalized problem solved on the host by SVQB (eigen-
+//   decomposition of the diagonally scaled K-Gram, directions below a
+//   relative 1e-13 dropped) and Jacobi;
+//   X <- [X W P] C,  P <- [0 W P] C  (images AX, BX, AP, BP updated by the
+//   same coefficients; recomputed from scratch every 20 iterations).
+// Fixed degrees of freedom are masked out of every block (their rows and
+// columns are zero in Ks and identity in K, i.e. lambda = 0 there).
+#include <cublas_v2.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <numeric>
+#include <vector>
+
+#include "solver.h"
+
+namespace tpo {
+
+namespace {
+
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(
+             std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+int grid_for(int64_t n, int threads) {
+  int64_t g = (n + threads - 1) / threads;
+  if (g > 148 * 32) g = 148 * 32;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+__device__ __forceinline__ double seeded_value(uint64_t i) {
+  uint64_t z = i + 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z = z ^ (z >> 31);
+  return (double)(z >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+}
+
+// X[:, j] = seeded values on the free dofs, 0 on the fixed ones
+__global__ void k_eig_start(int64_t n, int m, const uint8_t *__restrict__ fix,
+                            uint64_t seed, double *X) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * m;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = t % n;
+    const bool fixed = (fix[i / 3] >> (i % 3)) & 1u;
+    X[t] = fixed ? 0.0 : seeded_value(seed * 0x100000001B3ull + (uint64_t)t);
+  }
+}
+
+// zero the fixed dofs of m columns
+__global__ void k_mask(int64_t n, int m, const uint8_t *__restrict__ fix,
+                       double *X) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * m;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = t % n;
+    if ((fix[i / 3] >> (i % 3)) & 1u) X[t] = 0.0;
+  }
+}
+
+struct Theta {
+  double v[32];
+};
+
+// R[:, j] = AX[:, j] - theta_j BX[:, j]
+__global__ void k_resid(int64_t n, int m, const double *__restrict__ AX,
+                        const double *__restrict__ BX, Theta th, double *R) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * m;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int j = (int)(t / n);
+    R[t] = AX[t] - th.v[j] * BX[t];
+  }
+}
+
+// ---- small dense symmetric eigenproblems on the host ----------------------
+
+// cyclic Jacobi: A (n x n, column-major, symmetric) -> eigenvalues w
+// (descending) and eigenvectors V (columns)
+void jacobi_eig(int n, std::vector<double> A, std::vector<double> &w,
+                std::vector<double> &V) {
+  V.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) V[(size_t)i * n + i] = 1.0;
+  auto a = [&](int i, int j) -> double & { return A[(size_t)j * n + i]; };
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    double off = 0.0, tot = 0.0;
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        tot += a(i, j) * a(i, j);
+        if (i != j) off += a(i, j) * a(i, j);
+      }
+    if (off <= 1e-30 * tot || off == 0.0) break;
+    for (int p = 0; p < n - 1; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = a(p, q);
+        if (apq == 0.0) continue;
+        const double app = a(p, p), aqq = a(q, q);
+        const double tau = (aqq - app) / (2.0 * apq);
+        const double t = (tau >= 0 ? 1.0 : -1.0) /
+                         (std::fabs(tau) + std::sqrt(1.0 + tau * tau));
+        const double cs = 1.0 / std::sqrt(1.0 + t * t), sn = t * cs;
+        for (int k = 0; k < n; ++k) {   // A <- A J
+          const double akp = a(k, p), akq = a(k, q);
+          a(k, p) = cs * akp - sn * akq;
+          a(k, q) = sn * akp + cs * akq;
+        }
+        for (int k = 0; k < n; ++k) {   // A <- J^T A
+          const double apk = a(p, k), aqk = a(q, k);
+          a(p, k) = cs * apk - sn * aqk;
+          a(q, k) = sn * apk + cs * aqk;
+        }
+        for (int k = 0; k < n; ++k) {   // V <- V J
+          const double vkp = V[(size_t)p * n + k], vkq = V[(size_t)q * n + k];
+          V[(size_t)p * n + k] = cs * vkp - sn * vkq;
+          V[(size_t)q * n + k] = sn * vkp + cs * vkq;
+        }
+      }
+  }
+  std::vector<int> idx(n);
+  std::iota(idx.begin(), idx.end(), 0);
+  std::sort(idx.begin(), idx.end(), [&](int x, int y) { return a(x, x) > a(y, y); });
+  std::vector<double> Vs((size_t)n * n);
+  w.resize(n);
+  for (int j = 0; j < n; ++j) {
+    w[j] = a(idx[j], idx[j]);
+    for (int i = 0; i < n; ++i) Vs[(size_t)j * n + i] = V[(size_t)idx[j] * n + i];
+  }
+  V.swap(Vs);
+}
+
+// Rayleigh-Ritz of (H, G) (k x k, column-major): C (k x m) and the m
+// largest Ritz values.  Returns the rank kept, or < m on failure.
+int rayleigh_ritz(int k, int m, const std::vector<double> &H,
+                  const std::vector<double> &G, std::vector<double> &C,
+                  std::vector<double> &theta) {
+  std::vector<double> d(k);
+  for (int i = 0; i < k; ++i) {
+    const double g = G[(size_t)i * k + i];
+    d[i] = g > 0 ? 1.0 / std::sqrt(g) : 0.0;
+  }
+  std::vector<double> Gs((size_t)k * k);
+  for (int j = 0; j < k; ++j)
+    for (int i = 0; i < k; ++i) Gs[(size_t)j * k + i] = d[i] * G[(size_t)j * k + i] * d[j];
+  std::vector<double> gw, Q;
+  jacobi_eig(k, Gs, gw, Q);
+  const double gmax = gw.empty() ? 0.0 : gw[0];
+  int r = 0;
+  while (r < k && gw[r] > 1e-13 * gmax) ++r;
+  if (r < m) return r;
+  // Z = diag(d) Q_r diag(gw^-1/2)  (k x r)
+  std::vector<double> Z((size_t)k * r);
+  for (int j = 0; j < r; ++j) {
+    const double s = 1.0 / std::sqrt(gw[j]);
+    for (int i = 0; i < k; ++i) Z[(size_t)j * k + i] = d[i] * Q[(size_t)j * k + i] * s;
+  }
+  // Hr = Z^T H Z
+  std::vector<double> HZ((size_t)k * r), Hr((size_t)r * r);
+  for (int j = 0; j < r; ++j)
+    for (int i = 0; i < k; ++i) {
+      double s = 0;
+      for (int l = 0; l < k; ++l) s += H[(size_t)l * k + i] * Z[(size_t)j * k + l];
+      HZ[(size_t)j * k + i] = s;
+    }
+  for (int j = 0; j < r; ++j)
+    for (int i = 0; i < r; ++i) {
+      double s = 0;
+      for (int l = 0; l < k; ++l) s += Z[(size_t)i * k + l] * HZ[(size_t)j * k + l];
+      Hr[(size_t)j * r + i] = s;
+    }
+  for (int j = 0; j < r; ++j)      // symmetrise
+    for (int i = 0; i < j; ++i) {
+      const double v = 0.5 * (Hr[(size_t)j * r + i] + Hr[(size_t)i * r + j]);
+      Hr[(size_t)j * r + i] = Hr[(size_t)i * r + j] = v;
+    }
+  std::vector<double> hw, Y;
+  jacobi_eig(r, Hr, hw, Y);
+  C.assign((size_t)k * m, 0.0);
+  theta.assign(m, 0.0);
+  for (int j = 0; j < m; ++j) {
+    theta[j] = hw[j];
+    for (int i = 0; i < k; ++i) {
+      double s = 0;
+      for (int l = 0; l < r; ++l) s += Z[(size_t)l * k + i] * Y[(size_t)j * r + l];
+      C[(size_t)j * k + i] = s;
+    }
+  }
+  return r;
+}
+
+#define CK(call)                                                       \
+  do {                                                                 \
+    cudaError_t e_ = (call);                                           \
+    if (e_ != cudaSuccess) {                                           \
+      c.err = std::string(#call) + ": " + cudaGetErrorString(e_);      \
+      return TPO_E_CUDA;                                               \
+    }                                                                  \
+  } while (0)
+
+#define CB(call)                                                       \
+  do {                                                                 \
+    if ((call) != CUBLAS_STATUS_SUCCESS) {                             \
+      c.err = std::string(#call) + " failed";                          \
+      return TPO_E_CUDA;                                               \
+    }                                                                  \
+  } while (0)
+
+struct Blocks {
+  double *X, *AX, *BX, *W, *AW, *BW, *P, *AP, *BP;
+  double *Xn, *AXn, *BXn, *Pn, *APn, *BPn, *R;
+};
+
+}  // namespace
+
+// W = T R on m columns (T = one V-cycle in the requested precision), masked
+static int precondition(Ctx &c, const tpo_solve_opts &so, int precision,
+                        double *R, double *W, int m) {
+  const int64_t n = 3 * c.nn;
+  cudaStream_t s = c.stream;
+  for (int j0 = 0; j0 < m;) {
+    const int nb = (m - j0) >= 8 ? 8 : (m - j0) >= 4 ? 4 : (m - j0) >= 2 ? 2 : 1;
+    if (int rc = vcycle_cols(c, so, precision, R + j0 * n, W + j0 * n, nb)) return rc;
+    j0 += nb;
+  }
+  count_launch();
+  k_mask<<<grid_for(n * m, 256), 256, 0, s>>>(n, m, c.fix, W);
+  return TPO_OK;
+}
+
+int buckling(Ctx &c, const tpo_eig_opts &o, double *lambda, double *phi,
+             int phi_mem, tpo_eig_info *info) {
+  const double t0 = now_ms();
+  const int64_t n = 3 * c.nn;
+  const int m = o.block, nev = o.nev;
+  cudaStream_t s = c.stream;
+  cublasHandle_t h = static_cast<cublasHandle_t>(c.cublas);
+  if (!h) {
+    if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) {
+      c.err = "cublasCreate failed";
+      return TPO_E_CUDA;
+    }
+    c.cublas = h;
+  }
+  CB(cublasSetStream(h, s));
+  CB(cublasSetPointerMode(h, CUBLAS_POINTER_MODE_HOST));
+  // workspace: 16 blocks of n x m and the small Gram/coefficient matrices
+  const size_t blk = (size_t)n * m;
+  const size_t need = 16 * blk + 2 * (size_t)(3 * m) * (3 * m) + (size_t)(3 * m) * m + 2 * m;
+  if (c.eig_n < need) {
+    if (c.eig_buf) cudaFree(c.eig_buf);
+    c.eig_buf = nullptr;
+    c.eig_n = 0;
+    CK(cudaMalloc(&c.eig_buf, sizeof(double) * need));
+    c.eig_n = need;
+  }
+  double *base = c.eig_buf;
+  Blocks b;
+  double **slots[16] = {&b.X, &b.AX, &b.BX, &b.W, &b.AW, &b.BW, &b.P, &b.AP,
+                        &b.BP, &b.Xn, &b.AXn, &b.BXn, &b.Pn, &b.APn, &b.BPn, &b.R};
+  for (int i = 0; i < 16; ++i) *slots[i] = base + i * blk;
+  const int K3 = 3 * m;
+  double *dH = base + 16 * blk, *dG = dH + K3 * K3, *dC = dG + K3 * K3,
+         *dnrm = dC + K3 * m;
+  if (int rc = ensure_columns(c, kMaxBatch)) return rc;
+  tpo_solve_opts so = c.setup_opts;
+
+  auto applyAB = [&](const double *V, double *AV, double *BV) {
+    launch_ks_apply(c, V, AV, m);
+    for (int j0 = 0; j0 < m;) {
+      const int nb = std::min(m - j0, kMaxBatch);
+      launch_apply_fine<double>(c, c.E64, V + j0 * n, nullptr, BV + j0 * n, s, nb);
+      j0 += nb;
+    }
+  };
+  // Gram blocks of the basis [X W P] (first nblk of them): out (k x k)
+  std::vector<double> Hh, Gh;
+  auto gram = [&](int nblk) -> int {
+    const double *V[3] = {b.X, b.W, b.P};
+    const double *AV[3] = {b.AX, b.AW, b.AP};
+    const double *BV[3] = {b.BX, b.BW, b.BP};
+    const int k = nblk * m;
+    const double one = 1.0, zero = 0.0;
+    for (int bi = 0; bi < nblk; ++bi)
+      for (int bj = bi; bj < nblk; ++bj) {
+        CB(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, m, m, (int)n, &one, V[bi], (int)n,
+                       AV[bj], (int)n, &zero, dH + (size_t)bj * m * k + bi * m, k));
+        CB(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, m, m, (int)n, &one, V[bi], (int)n,
+                       BV[bj], (int)n, &zero, dG + (size_t)bj * m * k + bi * m, k));
+      }
+    Hh.assign((size_t)k * k, 0.0);
+    Gh.assign((size_t)k * k, 0.0);
+    CK(cudaMemcpyAsync(Hh.data(), dH, sizeof(double) * k * k, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(Gh.data(), dG, sizeof(double) * k * k, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    // the upper block triangle was formed; mirror it
+    for (int bi = 0; bi < nblk; ++bi)
+      for (int bj = 0; bj < bi; ++bj)
+        for (int jj = 0; jj < m; ++jj)
+          for (int ii = 0; ii < m; ++ii) {
+            const int r = bi * m + ii, q = bj * m + jj;
+            Hh[(size_t)q * k + r] = Hh[(size_t)r * k + q];
+            Gh[(size_t)q * k + r] = Gh[(size_t)r * k + q];
+          }
+    for (int j = 0; j < k; ++j)   // symmetrise the diagonal blocks
+      for (int i = 0; i < j; ++i) {
+        const double hv = 0.5 * (Hh[(size_t)j * k + i] + Hh[(size_t)i * k + j]);
+        const double gv = 0.5 * (Gh[(size_t)j * k + i] + Gh[(size_t)i * k + j]);
+        Hh[(size_t)j * k + i] = Hh[(size_t)i * k + j] = hv;
+        Gh[(size_t)j * k + i] = Gh[(size_t)i * k + j] = gv;
+      }
+    return TPO_OK;
+  };
+  // out = sum over the basis blocks of V_b C_b (rows of C of block b),
+  // skipping block 0 when with_x is false
+  auto combine = [&](int nblk, const double *Cd, int k, bool with_x,
+                     const double *const V[3], double *out) -> int {
+    const double one = 1.0, zero = 0.0;
+    bool first = true;
+    for (int bi = with_x ? 0 : 1; bi < nblk; ++bi) {
+      CB(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, m, m, &one, V[bi], (int)n,
+                     Cd + bi * m, k, first ? &zero : &one, out, (int)n));
+      first = false;
+    }
+    if (first) CK(cudaMemsetAsync(out, 0, sizeof(double) * blk, s));
+    return TPO_OK;
+  };
+
+  // ---- start block and its Rayleigh-Ritz
+  count_launch();
+  k_eig_start<<<grid_for(n * m, 256), 256, 0, s>>>(n, m, c.fix, o.seed, b.X);
+  applyAB(b.X, b.AX, b.BX);
+  CK(cudaGetLastError());
+  std::vector<double> C, theta;
+  if (int rc = gram(1)) return rc;
+  if (rayleigh_ritz(m, m, Hh, Gh, C, theta) < m) {
+    c.err = "eigensolver start block is rank deficient";
+    return TPO_E_BREAKDOWN;
+  }
+  CK(cudaMemcpyAsync(dC, C.data(), sizeof(double) * m * m, cudaMemcpyHostToDevice, s));
+  {
+    const double one = 1.0, zero = 0.0;
+    CB(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, m, m, &one, b.X, (int)n, dC, m,
+                   &zero, b.Xn, (int)n));
+    CB(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, m, m, &one, b.AX, (int)n, dC, m,
+                   &zero, b.AXn, (int)n));
+    CB(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, m, m, &one, b.BX, (int)n, dC, m,
+                   &zero, b.BXn, (int)n));
+    std::swap(b.X, b.Xn);
+    std::swap(b.AX, b.AXn);
+    std::swap(b.BX, b.BXn);
+  }
+
+  int it = 0, nconv = 0, status = TPO_NOT_CONVERGED;
+  bool haveP = false;
+  double max_res = 0.0;
+  std::vector<double> nrm(2 * m);
+  for (;;) {
+    // residuals and their relative norms
+    Theta th{};
+    for (int j = 0; j < m; ++j) th.v[j] = theta[j];
+    count_launch();
+    k_resid<<<grid_for(n * m, 256), 256, 0, s>>>(n, m, b.AX, b.BX, th, b.R);
+    CB(cublasSetPointerMode(h, CUBLAS_POINTER_MODE_DEVICE));
+    for (int j = 0; j < m; ++j) {
+      CB(cublasDnrm2(h, (int)n, b.R + j * n, 1, dnrm + j));
+      CB(cublasDnrm2(h, (int)n, b.BX + j * n, 1, dnrm + m + j));
+    }
+    CB(cublasSetPointerMode(h, CUBLAS_POINTER_MODE_HOST));
+    CK(cudaMemcpyAsync(nrm.data(), dnrm, sizeof(double) * 2 * m, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    nconv = 0;
+    max_res = 0.0;
+    for (int j = 0; j < nev; ++j) {
+      const double rel = nrm[j] / std::max(std::fabs(theta[j]) * nrm[m + j], 1e-300);
+      max_res = std::max(max_res, rel);
+      if (rel <= o.tol && nconv == j) ++nconv;
+    }
+    if (nconv >= nev) {
+      status = TPO_OK;
+      break;
+    }
+    if (it >= o.maxit) break;
+    ++it;
+    // W = T R and its images
+    if (int rc = precondition(c, so, o.precond, b.R, b.W, m)) return rc;
+    applyAB(b.W, b.AW, b.BW);
+    CK(cudaGetLastError());
+    // Rayleigh-Ritz on [X W P] (without P if that basis is degenerate)
+    int nblk = haveP ? 3 : 2;
+    if (int rc = gram(nblk)) return rc;
+    int r = rayleigh_ritz(nblk * m, m, Hh, Gh, C, theta);
+    if (r < m && nblk == 3) {
+      nblk = 2;
+      if (int rc = gram(nblk)) return rc;
+      r = rayleigh_ritz(nblk * m, m, Hh, Gh, C, theta);
+    }
+    if (r < m) {
+      status = TPO_E_BREAKDOWN;
+      c.err = "eigensolver basis lost rank";
+      break;
+    }
+    const int k = nblk * m;
+    CK(cudaMemcpyAsync(dC, C.data(), sizeof(double) * k * m, cudaMemcpyHostToDevice, s));
+    const double *V[3] = {b.X, b.W, b.P};
+    const double *AV[3] = {b.AX, b.AW, b.AP};
+    const double *BV[3] = {b.BX, b.BW, b.BP};
+    if (int rc = combine(nblk, dC, k, true, V, b.Xn)) return rc;
+    if (int rc = combine(nblk, dC, k, true, AV, b.AXn)) return rc;
+    if (int rc = combine(nblk, dC, k, true, BV, b.BXn)) return rc;
+    if (int rc = combine(nblk, dC, k, false, V, b.Pn)) return rc;
+    if (int rc = combine(nblk, dC, k, false, AV, b.APn)) return rc;
+    if (int rc = combine(nblk, dC, k, false, BV, b.BPn)) return rc;
+    std::swap(b.X, b.Xn);
+    std::swap(b.AX, b.AXn);
+    std::swap(b.BX, b.BXn);
+    std::swap(b.P, b.Pn);
+    std::swap(b.AP, b.APn);
+    std::swap(b.BP, b.BPn);
+    haveP = true;
+    if (it % 20 == 0) {   // refresh the images against drift
+      applyAB(b.X, b.AX, b.BX);
+      applyAB(b.P, b.AP, b.BP);
+    }
+  }
+  CK(cudaGetLastError());
+  for (int j = 0; j < nev; ++j) lambda[j] = theta[j];
+  if (phi)
+    CK(cudaMemcpyAsync(phi, b.X, sizeof(double) * n * nev,
+                       phi_mem == TPO_MEM_DEVICE ? cudaMemcpyDeviceToDevice
+                                                 : cudaMemcpyDeviceToHost,
+                       s));
+  CK(cudaStreamSynchronize(s));
+  if (info) {
+    info->status = status;
+    info->iterations = it;
+    info->nconv = nconv;
+    info->max_resid = max_res;
+    info->solve_ms = now_ms() - t0;
+  }
+  if (status == TPO_NOT_CONVERGED && c.err.empty())
+    c.err = "eigensolver reached its iteration limit";
+  return status;
+}
+
+}  // namespace tpo

@@ -110,8 +110,33 @@ void element_stiffness(const double dx[3], double E0, double nu,
 
 }  // namespace
 
+// Gauss-point gradients of the trilinear shape functions of a box element
+// for the stress stiffness: corner l (lexicographic, sign s_d = +1 when bit
+// d of l is set), Gauss point q at xi_d = s_d(q) / sqrt(3);
+// dN_l/dx_a = s_a(l)/8 prod_{d != a} (1 + s_d(l) xi_d) * 2/dx_a and
+// detJ = dx dy dz / 8 (the box-element case of FEAnalysis.cpp:869-990)
+static void build_ks_constants(Ctx &c) {
+  const double g = 1.0 / std::sqrt(3.0);
+  auto sg = [](int l, int d) { return ((l >> d) & 1) ? 1.0 : -1.0; };
+  for (int q = 0; q < 8; ++q)
+    for (int a = 0; a < 3; ++a)
+      for (int l = 0; l < 8; ++l) {
+        double v = sg(l, a) / 8.0 * 2.0 / c.prm.dx[a];
+        for (int d = 0; d < 3; ++d)
+          if (d != a) v *= 1.0 + sg(l, d) * sg(q, d) * g;
+        c.ksc.g[q][a][l] = v;
+      }
+  const double E0 = c.prm.E0, nu = c.prm.nu;
+  const double cc = E0 / ((1 + nu) * (1 - 2 * nu));
+  c.ksc.t1 = (1 - nu) * cc;
+  c.ksc.t3 = nu * cc;
+  c.ksc.t2 = E0 / (2 * (1 + nu));
+  c.ksc.detJ = c.prm.dx[0] * c.prm.dx[1] * c.prm.dx[2] / 8.0;
+}
+
 int build_element_constants(Ctx &c) {
   element_stiffness(c.prm.dx, c.prm.E0, c.prm.nu, c.K0);
+  build_ks_constants(c);
   // K0 in lexicographic corner order
   double Kl[24][24];
   for (int a = 0; a < 8; ++a)

@@ -478,6 +478,22 @@ int vcycle_block(Ctx &c, const tpo_solve_opts &o, int precision, int nb) {
   return TPO_OK;
 }
 
+int vcycle_cols(Ctx &c, const tpo_solve_opts &o, int precision, const double *r,
+                double *z, int nb) {
+  cudaStream_t s = c.stream;
+  const int64_t n = 3 * c.nn;
+  if (precision == TPO_PREC_FP64) {
+    vcycle_rec<double>(c, 0, r, z, o, s, nb);
+  } else {
+    launch_d2f(n * nb, r, c.r32, s);
+    vcycle_rec<float>(c, 0, c.r32, c.z32, o, s, nb);
+    launch_f2d(n * nb, c.z32, z, s);
+  }
+  CK(cudaGetLastError());
+  CK(c.coarse_err);
+  return TPO_OK;
+}
+
 // Solve K x_j = b_j for nb columns (stride 3 nn); x holds the initial
 // guesses.  Column j converges at ||b_j - K x_j|| <= rtol ||b_j||.  info
 // aggregates the block (iterations and outer steps summed over columns,

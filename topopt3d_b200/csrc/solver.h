@@ -11,6 +11,14 @@ int setup_hierarchy(Ctx &c, const tpo_solve_opts &o);
 int vcycle_apply(Ctx &c, const tpo_solve_opts &o, int precision,
                  const double *r, double *z);
 int vcycle_block(Ctx &c, const tpo_solve_opts &o, int precision, int nb);
+// z = V-cycle(r) on nb <= kMaxBatch columns (FP64 or FP32 arithmetic)
+int vcycle_cols(Ctx &c, const tpo_solve_opts &o, int precision, const double *r,
+                double *z, int nb);
+// room for nb columns in the level and solver work vectors (capi.cu)
+int ensure_columns(Ctx &c, int nb);
+// the nev largest eigenvalues of Ks phi = lambda K phi (eigen.cu)
+int buckling(Ctx &c, const tpo_eig_opts &o, double *lambda, double *phi,
+             int phi_mem, tpo_eig_info *info);
 int solve(Ctx &c, const tpo_solve_opts &o, const double *b, double *x,
           tpo_solve_info *info, int nb = 1, tpo_solve_info *col = nullptr);
 

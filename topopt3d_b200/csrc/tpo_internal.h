@@ -48,6 +48,15 @@ struct K0Diag {
   T v[24];
 };
 
+// stress-stiffness constants: shape-function gradients g[q][a][l] =
+// dN_l/dx_a at Gauss point q (corners l in lexicographic order), the
+// isotropic D entries (t1 = (1-nu) c, t3 = nu c, t2 = shear modulus) and
+// detJ (FEAnalysis.cpp:869-1050, RecMesh.cpp:453-462)
+struct KsConst {
+  double g[8][3][8];
+  double t1, t2, t3, detJ;
+};
+
 // density filter template: offsets and raw weights 1 - d/R (Filter.cpp:43-52)
 constexpr int kMaxFilterTaps = 512;
 
@@ -117,6 +126,7 @@ struct Ctx {
   uint8_t *fix = nullptr;   // per-node fixed-component bitmask
   double *F = nullptr, *U = nullptr;
   double *x = nullptr, *rho = nullptr, *E64 = nullptr, *dEdz = nullptr;
+  double *Es64 = nullptr;   // rho^p without E_min (stress stiffness)
   float *E32 = nullptr;
   double *S0 = nullptr;     // fine-level assembled stencil (setup only)
   double *K0lex = nullptr;  // K0 in lexicographic corner order (576)
@@ -150,6 +160,16 @@ struct Ctx {
   double *solver_work = nullptr;
   size_t solver_work_n = 0;
   int *dev_info = nullptr;
+
+  // stress stiffness: 27-point scalar stencil S[d * nn + n] and the
+  // per-element scratch (36 x ne) it is gathered from
+  KsConst ksc{};
+  double *ks_S = nullptr, *ks_H = nullptr;
+  bool ks_ready = false;
+  // eigensolver: cuBLAS handle and the block workspace
+  void *cublas = nullptr;
+  double *eig_buf = nullptr;
+  size_t eig_n = 0;
 
   // CUDA graphs of the CG iteration bodies, keyed on (x, columns)
   cudaGraphExec_t graph64 = nullptr, graph32 = nullptr;
@@ -287,6 +307,10 @@ void launch_filter(const Ctx &c, const double *in, double *out, bool transpose,
 void launch_filter_adj_uniform(const Ctx &c, double value, double *out,
                                cudaStream_t s);
 void launch_simp(const Ctx &c, double penal, double eps, cudaStream_t s);
+// stress stiffness from c.U and c.Es64 (kernels_ks.cu)
+void launch_ks_assemble(const Ctx &c, cudaStream_t s);
+// y = Ks u for nb columns (stride 3 nn), on c.stream
+void launch_ks_apply(const Ctx &c, const double *u, double *y, int nb);
 void launch_sensitivity(const Ctx &c, const double *U, double *dc,
                         cudaStream_t s);
 void launch_oc_step(const Ctx &c, int64_t n, double *x, const double *xold,

@@ -270,6 +270,33 @@ class TopOpt:
             self._h, None if stream_handle is None else C.c_void_p(stream_handle)),
             "set_stream")
 
+    # -- linear buckling (Buckling.cpp:15-414) ------------------------------
+    def ks_assemble(self):
+        """Stability::StressFnc from the current U and material."""
+        self._check(self._lib.tpo_ks_assemble(self._h), "ks_assemble")
+
+    def ks_apply(self, u, y, nrhs=1):
+        up, mem, k1 = _buf(u, 3 * self.nNode * nrhs)
+        yp, _, k2 = _buf(y, 3 * self.nNode * nrhs, writable=True)
+        self._check(self._lib.tpo_ks_apply(self._h, up, yp, nrhs, mem), "ks_apply")
+        return y
+
+    def buckling(self, opts=None, want_vectors=False, **kw):
+        """The largest eigenvalues of Ks phi = lambda K phi (descending) and,
+        if asked, the K-orthonormal eigenvectors as rows; the solver record
+        is kept in last_eig."""
+        o = opts or L.default_eig_opts(**kw)
+        lam = np.zeros(o.nev)
+        phi = np.zeros((o.nev, 3 * self.nNode)) if want_vectors else None
+        info = L.EigInfo()
+        rc = self._check(self._lib.tpo_buckling(
+            self._h, C.byref(o), lam.ctypes.data_as(C.POINTER(C.c_double)),
+            None if phi is None else phi.ctypes.data_as(C.c_void_p), L.MEM_HOST,
+            C.byref(info)), "buckling")
+        self.last_eig = info.as_dict()
+        self.last_eig["rc"] = rc
+        return (lam, phi) if want_vectors else lam
+
     def volume(self, gradient=True):
         v = C.c_double()
         dv = np.zeros(self.nElem) if gradient else None
@@ -348,6 +375,28 @@ class Volume(Function_Base):
         v, dv = topOpt.volume(gradient=self.calc_gradient)
         self.values[0] = v
         self.gradients = dv
+
+
+class Stability(Function_Base):
+    """Stability::Function (Buckling.cpp:15-88): the buckling eigenvalues
+    of Ks phi = lambda K phi aggregated as (sum lambda^p)^(1/p), p = 8
+    (:87-88).  The eigenvalue sensitivities (:113-272) are not computed:
+    only calc_gradient = False is supported."""
+
+    def __init__(self, values, min_val, max_val, objective=True,
+                 calc_gradient=False, nev=6, block=12):
+        if calc_gradient:
+            raise TopOptError(-4, "buckling sensitivities are not implemented")
+        super().__init__(values, min_val, max_val, objective, False)
+        self.nev, self.block = nev, block
+        self.lam = None
+
+    def Function(self, topOpt):
+        topOpt.ks_assemble()
+        self.lam = topOpt.buckling(nev=self.nev, block=self.block)
+        p = 8.0
+        self.values[0] = float(np.sum(self.lam ** p) ** (1.0 / p))
+        self.gradients = None
 
 
 @dataclass
