@@ -110,6 +110,11 @@ int copy_out(Ctx &c, double *dst, const double *src, size_t n, int mem) {
   return TPO_OK;
 }
 
+// the identity-row mask follows E and the fixed mask
+void refresh_idm(Ctx &c) {
+  if (c.have_material) tpo::launch_identity_mask(c, c.stream);
+}
+
 int check_mem(Ctx &c, int mem) {
   REQUIRE(mem == TPO_MEM_HOST || mem == TPO_MEM_DEVICE, "mem must be TPO_MEM_HOST or TPO_MEM_DEVICE");
   return TPO_OK;
@@ -159,7 +164,9 @@ int alloc_solver(Ctx &c) {
   int rc = 0;
 #define A(p, n) \
   if ((rc = dalloc(c, &(p), (n))) != TPO_OK) return rc
-  A(c.S0, 243 * c.nn);
+  // the assembled fine stencil is only the coarsest operator of a
+  // one-level hierarchy; level 1 is formed from the element moduli
+  if (c.L == 1) A(c.S0, 243 * c.nn);
   for (int l = 0; l < c.L; ++l) {
     tpo::Level &v = c.lev[l];
     const size_t n = 3 * v.nn;
@@ -192,8 +199,10 @@ void free_all(Ctx &c) {
     dfree(v.S64); dfree(v.S32); dfree(v.dinv64); dfree(v.dinv32);
     dfree(v.A64); dfree(v.A32); dfree(v.H64); dfree(v.H32);
   }
-  dfree(c.fix); dfree(c.F); dfree(c.U); dfree(c.x); dfree(c.rho);
+  dfree(c.fix); dfree(c.idm); dfree(c.F); dfree(c.U); dfree(c.x); dfree(c.rho);
   dfree(c.E64); dfree(c.dEdz); dfree(c.E32); dfree(c.S0); dfree(c.K0lex);
+  dfree(c.GMi); dfree(c.gk_slot); dfree(c.gk_elem); dfree(c.gk_count);
+  dfree(c.gk_G); c.gk_cap = 0;
   dfree(c.Ainv); dfree(c.Adense); dfree(c.solver_work); dfree(c.dev_info);
   dfree(c.finv); dfree(c.taps_d);
   dfree(c.w64);
@@ -208,6 +217,15 @@ void free_all(Ctx &c) {
   c.scal_h = nullptr;
   if (c.cusolver) cusolverDnDestroy(static_cast<cusolverDnHandle_t>(c.cusolver));
   c.cusolver = nullptr;
+  if (c.aux_stream) cudaStreamSynchronize(c.aux_stream);
+  for (cudaEvent_t &e : c.lev_ev) {
+    if (e) cudaEventDestroy(e);
+    e = nullptr;
+  }
+  if (c.aux_ev) cudaEventDestroy(c.aux_ev);
+  c.aux_ev = nullptr;
+  if (c.aux_stream) cudaStreamDestroy(c.aux_stream);
+  c.aux_stream = nullptr;
   if (c.own_stream) cudaStreamDestroy(c.own_stream);
   c.own_stream = c.stream = nullptr;
 }
@@ -336,15 +354,25 @@ int tpo_create(const tpo_mesh_params *p, tpo_ctx **out) {
     delete ctx;
     return code;
   };
+  if (cudaStreamCreateWithFlags(&c.aux_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c.aux_ev, cudaEventDisableTiming) != cudaSuccess)
+    return fail(TPO_E_CUDA);
+  for (cudaEvent_t &e : c.lev_ev)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+      return fail(TPO_E_CUDA);
   const size_t nio = std::max<size_t>(3 * c.nn, c.ne);
 #define A(p, n) \
   if (dalloc(c, &(p), (n)) != TPO_OK) return fail(TPO_E_CUDA)
   A(c.taps_d, 1);
-  A(c.finv, c.ne); A(c.K0lex, 576);
+  A(c.finv, c.ne); A(c.K0lex, 576); A(c.GMi, 8 * 8 * 8 * 9);
+  {
+    const size_t nce = (size_t)((c.nel[0] + 1) / 2) * ((c.nel[1] + 1) / 2) * ((c.nel[2] + 1) / 2);
+    A(c.gk_slot, nce); A(c.gk_elem, nce); A(c.gk_count, 1);
+  }
   A(c.x, c.ne); A(c.rho, c.ne); A(c.E64, c.ne); A(c.dEdz, c.ne); A(c.E32, c.ne);
   A(c.Es64, c.ne);
-  A(c.fix, c.nn); A(c.F, 3 * c.nn); A(c.U, 3 * c.nn);
-  A(c.scal, tpo::kScalCount); A(c.part, tpo::kPartCount); A(c.ticket, tpo::kMaxBatch);
+  A(c.fix, c.nn); A(c.idm, c.nn); A(c.F, 3 * c.nn); A(c.U, 3 * c.nn);
+  A(c.scal, tpo::kScalCount); A(c.part, tpo::kPartCount); A(c.ticket, 2 * tpo::kMaxBatch);
   A(c.tmpe, c.ne); A(c.tmpe2, c.ne); A(c.dev_info, 1);
   A(c.io_a, nio); A(c.io_b, nio);
 #undef A
@@ -361,6 +389,7 @@ int tpo_create(const tpo_mesh_params *p, tpo_ctx **out) {
           Kl[24 * (3 * a + r) + 3 * b + q] =
               c.K0[24 * (3 * kLexToLocal[a] + r) + 3 * kLexToLocal[b] + q];
   if (cudaMemcpyAsync(c.K0lex, Kl, sizeof(Kl), cudaMemcpyHostToDevice, c.stream) != cudaSuccess ||
+      cudaMemcpyAsync(c.GMi, c.GMi_h, sizeof(c.GMi_h), cudaMemcpyHostToDevice, c.stream) != cudaSuccess ||
       cudaMemcpyAsync(c.taps_d, &c.taps, sizeof(c.taps), cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
     return fail(TPO_E_CUDA);
   tpo::launch_filter_rowsum(c, c.stream);
@@ -430,6 +459,7 @@ int tpo_add_bc(tpo_ctx *ctx, int32_t type, const double center[3],
     cudaSetDevice(c.device);
     CK(cudaMemcpyAsync(c.fix, c.fix_h.data(), c.nn, cudaMemcpyHostToDevice, c.stream));
     CK(cudaMemcpyAsync(c.F, c.F_h.data(), sizeof(double) * 3 * c.nn, cudaMemcpyHostToDevice, c.stream));
+    refresh_idm(c);
     CK(cudaStreamSynchronize(c.stream));
     c.assembled = false;
   }
@@ -446,6 +476,7 @@ int tpo_set_bc(tpo_ctx *ctx, const uint8_t *fixmask, const double *F, int mem) {
   if (c.initialized) {
     CK(cudaMemcpyAsync(c.fix, c.fix_h.data(), c.nn, cudaMemcpyHostToDevice, c.stream));
     CK(cudaMemcpyAsync(c.F, c.F_h.data(), sizeof(double) * 3 * c.nn, cudaMemcpyHostToDevice, c.stream));
+    refresh_idm(c);
     CK(cudaStreamSynchronize(c.stream));
     c.assembled = false;
   }
@@ -470,6 +501,7 @@ int tpo_fe_initialize(tpo_ctx *ctx) {
   CK(cudaMemcpyAsync(c.fix, c.fix_h.data(), c.nn, cudaMemcpyHostToDevice, c.stream));
   CK(cudaMemcpyAsync(c.F, c.F_h.data(), sizeof(double) * 3 * c.nn, cudaMemcpyHostToDevice, c.stream));
   CK(cudaMemsetAsync(c.U, 0, sizeof(double) * 3 * c.nn, c.stream));
+  refresh_idm(c);
   CK(cudaStreamSynchronize(c.stream));
   c.initialized = true;
   c.assembled = false;
@@ -490,6 +522,7 @@ int tpo_mat_int_fnc(tpo_ctx *ctx, const double *x, double penal, double eps,
   tpo::launch_filter(c, c.x, c.rho, false, c.stream);   // rho = P x (:35)
   tpo::launch_simp(c, penal, eps, c.stream);
   c.have_material = true;
+  refresh_idm(c);
   c.assembled = false;
   return finish(c, TPO_OK);
 }
@@ -505,8 +538,9 @@ int tpo_set_moduli(tpo_ctx *ctx, const double *E, const double *dEdz, int mem) {
   tpo::launch_d2f(c.ne, c.E64, c.E32, c.stream);
   // given moduli carry no E_min split: the stress stiffness uses E itself
   CK(cudaMemcpyAsync(c.Es64, c.E64, sizeof(double) * c.ne, cudaMemcpyDeviceToDevice, c.stream));
-  CK(cudaStreamSynchronize(c.stream));
   c.have_material = true;
+  refresh_idm(c);
+  CK(cudaStreamSynchronize(c.stream));
   c.assembled = false;
   return finish(c, TPO_OK);
 }
@@ -818,6 +852,7 @@ int tpo_set_vector(tpo_ctx *ctx, const char *which, const double *in, int mem) {
     // new moduli invalidate the hierarchy
     tpo::launch_d2f(c.ne, c.E64, c.E32, c.stream);
     c.have_material = true;
+    refresh_idm(c);
     c.assembled = false;
   }
   CK(cudaStreamSynchronize(c.stream));

@@ -134,6 +134,37 @@ static void build_ks_constants(Ctx &c) {
   c.ksc.detJ = c.prm.dx[0] * c.prm.dx[1] * c.prm.dx[2] / 8.0;
 }
 
+// Level-1 Galerkin blocks of an interior fine element: the fine element at
+// offset i = (ax, ay, az) inside its coarse element has corner p at fine
+// coordinate t_d = a_d + bit_d(p) in {0, 1, 2} from the coarse element's
+// origin; the trilinear weight of coarse corner k is W[t][bit_d(k)] with
+// W = {{1, 0}, {1/2, 1/2}, {0, 1}} per dimension (Interpolation.cpp:135,
+// 157; interior rows need no normalisation).  GMi[i][ln][lm] =
+// sum_{p,q} w(p->ln) w(q->lm) K0[p][q] (3x3 blocks, lexicographic corners).
+static void build_galerkin_blocks(Ctx &c, const double Kl[24][24]) {
+  static const double W[3][2] = {{1.0, 0.0}, {0.5, 0.5}, {0.0, 1.0}};
+  for (int i = 0; i < 8; ++i) {
+    double w[8][8];   // w[p][k]
+    for (int p = 0; p < 8; ++p)
+      for (int k = 0; k < 8; ++k) {
+        double v = 1.0;
+        for (int d = 0; d < 3; ++d)
+          v *= W[((i >> d) & 1) + ((p >> d) & 1)][(k >> d) & 1];
+        w[p][k] = v;
+      }
+    for (int ln = 0; ln < 8; ++ln)
+      for (int lm = 0; lm < 8; ++lm)
+        for (int r = 0; r < 3; ++r)
+          for (int s = 0; s < 3; ++s) {
+            double v = 0.0;
+            for (int p = 0; p < 8; ++p)
+              for (int q = 0; q < 8; ++q)
+                v += w[p][ln] * w[q][lm] * Kl[3 * p + r][3 * q + s];
+            c.GMi_h[((i * 8 + ln) * 8 + lm) * 9 + 3 * r + s] = v;
+          }
+  }
+}
+
 int build_element_constants(Ctx &c) {
   element_stiffness(c.prm.dx, c.prm.E0, c.prm.nu, c.K0);
   build_ks_constants(c);
@@ -146,6 +177,7 @@ int build_element_constants(Ctx &c) {
           Kl[3 * a + r][3 * b + s] =
               c.K0[24 * (3 * kLexToLocal[a] + r) + 3 * kLexToLocal[b] + s];
   for (int i = 0; i < 24; ++i) c.kd64.v[i] = Kl[i][i];
+  build_galerkin_blocks(c, Kl);
   // Kh = T K T^T / 64 indexed (3q + c)
   auto sgn = [](int l, int q) {
     int s = 1;

@@ -89,6 +89,40 @@ __global__ void k_fine_stencil(int nelx, int nely, int nelz,
   }
 }
 
+// Identity-row mask of the fine operator: bit c of node n is set when dof
+// (n, c) has an identity row and column -- fixed (MatZeroRowsColumns,
+// FEAnalysis.cpp:473) or with an assembled diagonal <= 0, which the
+// reference replaces by 1 (:476-484).  Such a diagonal means E = 0 on every
+// element around the node, so the row and column are zero apart from it.
+// A NaN diagonal is left alone: the reference sets it to 1 but keeps the
+// NaN off-diagonals, so the solve fails there as here.
+__global__ void k_identity_mask(int nelx, int nely, int nelz,
+                                const double *__restrict__ E,
+                                const uint8_t *__restrict__ fix,
+                                const K0Diag<double> kd, uint8_t *idm) {
+  const int Nx = nelx + 1, Ny = nely + 1, Nz = nelz + 1;
+  const int64_t nn = (int64_t)Nx * Ny * Nz;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
+       n += (int64_t)gridDim.x * blockDim.x) {
+    const int i = n % Nx, j = (n / Nx) % Ny, k = n / ((int64_t)Nx * Ny);
+    double d[3] = {0, 0, 0};
+    for (int bz = 0; bz < 2; ++bz)
+      for (int by = 0; by < 2; ++by)
+        for (int bx = 0; bx < 2; ++bx) {
+          const int ei = i - 1 + bx, ej = j - 1 + by, ek = k - 1 + bz;
+          if (ei < 0 || ej < 0 || ek < 0 || ei >= nelx || ej >= nely || ek >= nelz)
+            continue;
+          const int l = (1 - bx) + 2 * (1 - by) + 4 * (1 - bz);
+          const double Ee = E[((int64_t)ek * nely + ej) * nelx + ei];
+          for (int c = 0; c < 3; ++c) d[c] += Ee * kd.v[3 * l + c];
+        }
+    unsigned m = fix[n];
+    for (int c = 0; c < 3; ++c)
+      if (d[c] <= 0) m |= 1u << c;
+    idm[n] = (uint8_t)m;
+  }
+}
+
 int grid_for(int64_t n, int threads) {
   int64_t g = (n + threads - 1) / threads;
   if (g > 148 * 32) g = 148 * 32;
@@ -104,6 +138,12 @@ void launch_fine_diag(const Ctx &c, double *dinv64, float *dinv32,
   k_fine_diag<<<grid_for(c.nn, 256), 256, 0, s>>>(c.nel[0], c.nel[1], c.nel[2],
                                                    c.E64, c.fix, c.kd64, dinv64,
                                                    dinv32);
+}
+
+void launch_identity_mask(const Ctx &c, cudaStream_t s) {
+  count_launch();
+  k_identity_mask<<<grid_for(c.nn, 256), 256, 0, s>>>(c.nel[0], c.nel[1], c.nel[2],
+                                                       c.E64, c.fix, c.kd64, c.idm);
 }
 
 void launch_fine_stencil(const Ctx &c, double *S, cudaStream_t s) {

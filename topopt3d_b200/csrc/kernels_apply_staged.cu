@@ -370,10 +370,10 @@ void launch_mode(const Ctx &c, const T *E, const ApplyArgs<T> &args_in,
   count_launch();
   if (nb == 1)
     k_apply_staged<T, kTY, IN, OUT, false><<<grid, dim3(32, kTY), staged_smem<T>(), s>>>(
-        c.nel[0], c.nel[1], c.nel[2], zchunk, E, c.fix, args, kh);
+        c.nel[0], c.nel[1], c.nel[2], zchunk, E, c.idm, args, kh);
   else
     k_apply_staged<T, kTY, IN, OUT, true><<<grid, dim3(32, kTY), staged_smem<T>(), s>>>(
-        c.nel[0], c.nel[1], c.nel[2], zchunk, E, c.fix, args, kh);
+        c.nel[0], c.nel[1], c.nel[2], zchunk, E, c.idm, args, kh);
 }
 
 }  // namespace

@@ -39,6 +39,167 @@ __device__ __forceinline__ double pw1(int f, int c, int Nf) {
   return (f + 1 <= Nf - 1) ? 0.5 : 1.0;
 }
 
+// ---- level 1 straight from the element moduli ----------------------------
+//
+// A_1 = P^T A_0 P with A_0 = M (sum_e E_e K0_e) M + (I - M), M the mask of
+// dofs without an identity row (idm).  Every fine element lies inside one
+// level-1 coarse element (2x2x2 fine elements) and its 8 nodes interpolate
+// from that coarse element's 8 nodes, so
+//   A_1 = sum_E sum_{e in E} E_e Q_e^T (M K0 M) Q_e + P^T (I - M) P.
+// For a fine element without identity dofs at offset i of a coarse element
+// with all 8 corners, Q_e^T K0 Q_e is one of 8 fixed 24x24 matrices (GMi,
+// element.cpp); the 3x3 block (ln, lm) of the coarse stencil is then
+// sum_i E_{e_i} GMi[i][ln][lm].  Coarse elements whose closed fine box holds
+// an identity dof, or that miss a corner (odd element counts), take the
+// general path: masked K0 with the interpolation weights of pw1.
+
+// slot[E] >= 0: level-1 coarse element E needs the general path (an
+// identity dof in its closed fine box, or a missing corner); slots are
+// handed out by an atomic counter (their order does not affect any value)
+__global__ void k_coarse_elem_flags(int nelx, int nely, int nelz,
+                                    const uint8_t *__restrict__ idm,
+                                    int *__restrict__ slot,
+                                    int *__restrict__ slot_elem,
+                                    unsigned int *__restrict__ count) {
+  const int fx = nelx + 1, fy = nely + 1, fz = nelz + 1;
+  const int ncx = (nelx + 1) / 2, ncy = (nely + 1) / 2, ncz = (nelz + 1) / 2;
+  const int64_t nce = (int64_t)ncx * ncy * ncz;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nce;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int ex = (int)(t % ncx), ey = (int)((t / ncx) % ncy), ez = (int)(t / ((int64_t)ncx * ncy));
+    unsigned any = (2 * ex + 2 > fx - 1) || (2 * ey + 2 > fy - 1) || (2 * ez + 2 > fz - 1);
+    for (int z = 2 * ez; z <= min(2 * ez + 2, fz - 1) && !any; ++z)
+      for (int y = 2 * ey; y <= min(2 * ey + 2, fy - 1); ++y)
+        for (int x = 2 * ex; x <= min(2 * ex + 2, fx - 1); ++x)
+          any |= idm[((int64_t)z * fy + y) * fx + x];
+    int sl = -1;
+    if (any) {
+      sl = (int)atomicAdd(count, 1u);
+      slot_elem[sl] = (int)t;
+    }
+    slot[t] = sl;
+  }
+}
+
+// general path, one thread per (flagged coarse element, ln, lm): the 3x3
+// block sum_{fine e in E} E_e sum_{p,q} w(p->ln) w(q->lm) (M K0 M)_pq with
+// the interpolation weights of pw1 and the identity-dof masks
+__global__ void k_galerkin_general(int nelx, int nely, int nelz, int nslots,
+                                   const double *__restrict__ E,
+                                   const uint8_t *__restrict__ idm,
+                                   const int *__restrict__ slot_elem,
+                                   const double *__restrict__ K0lex,
+                                   double *__restrict__ G) {
+  const int fx = nelx + 1, fy = nely + 1, fz = nelz + 1;
+  const int ncx = (nelx + 1) / 2, ncy = (nely + 1) / 2;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 64 * (int64_t)nslots;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int sl = (int)(t / 64), pr = (int)(t % 64), ln = pr / 8, lm = pr % 8;
+    const int ce = slot_elem[sl];
+    const int EI = ce % ncx, EJ = (ce / ncx) % ncy, EK = ce / (ncx * ncy);
+    // coarse corner coordinates (the far ones may not exist: pw1 gives 0)
+    const int ix = EI + (ln & 1), iy = EJ + ((ln >> 1) & 1), iz = EK + ((ln >> 2) & 1);
+    const int jx = EI + (lm & 1), jy = EJ + ((lm >> 1) & 1), jz = EK + ((lm >> 2) & 1);
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < 8; ++i) {
+      const int ex = 2 * EI + (i & 1), ey = 2 * EJ + ((i >> 1) & 1), ez = 2 * EK + ((i >> 2) & 1);
+      if (ex >= nelx || ey >= nely || ez >= nelz) continue;
+      const double Ee = E[((int64_t)ez * nely + ey) * nelx + ex];
+      double wn[8], wm[8];
+      unsigned msk[8];
+#pragma unroll
+      for (int p = 0; p < 8; ++p) {
+        const int gx = ex + (p & 1), gy = ey + ((p >> 1) & 1), gz = ez + ((p >> 2) & 1);
+        wn[p] = pw1(gx, ix, fx) * pw1(gy, iy, fy) * pw1(gz, iz, fz);
+        wm[p] = pw1(gx, jx, fx) * pw1(gy, jy, fy) * pw1(gz, jz, fz);
+        msk[p] = idm[((int64_t)gz * fy + gy) * fx + gx];
+      }
+      for (int p = 0; p < 8; ++p) {
+        if (wn[p] == 0.0) continue;
+        for (int q = 0; q < 8; ++q) {
+          const double w = Ee * wn[p] * wm[q];
+          if (w == 0.0) continue;
+          const double *k0 = K0lex + 24 * (3 * p) + 3 * q;
+          for (int r = 0; r < 3; ++r) {
+            if ((msk[p] >> r) & 1u) continue;
+            for (int s2 = 0; s2 < 3; ++s2)
+              if (!((msk[q] >> s2) & 1u)) acc[3 * r + s2] += w * k0[24 * r + s2];
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) G[(int64_t)t * 9 + q] = acc[q];
+  }
+}
+
+// the level-1 stencil: per (coarse node, neighbour) block, the fast-path
+// element sums, the general-path blocks of flagged elements and the
+// P^T (I - M) P term of the identity dofs
+__global__ void k_galerkin_fine(int nelx, int nely, int nelz,
+                                const double *__restrict__ E,
+                                const uint8_t *__restrict__ idm,
+                                const int *__restrict__ slot,
+                                const double *__restrict__ G,
+                                const double *__restrict__ GMi,
+                                double *__restrict__ Sc) {
+  const int fx = nelx + 1, fy = nely + 1, fz = nelz + 1;
+  const int cx = (fx + 1) / 2, cy = (fy + 1) / 2, cz = (fz + 1) / 2;
+  const int ncx = (nelx + 1) / 2, ncy = (nely + 1) / 2, ncz = (nelz + 1) / 2;
+  const int64_t nnc = (int64_t)cx * cy * cz;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 27 * nnc;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int nb = (int)(t / nnc);
+    const int64_t I = t - (int64_t)nb * nnc;
+    const int ix = (int)(I % cx), iy = (int)((I / cx) % cy), iz = (int)(I / ((int64_t)cx * cy));
+    const int jx = ix + nb % 3 - 1, jy = iy + (nb / 3) % 3 - 1, jz = iz + nb / 9 - 1;
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (jx >= 0 && jx < cx && jy >= 0 && jy < cy && jz >= 0 && jz < cz) {
+      bool anyflag = false;
+      for (int EK = max(iz, jz) - 1; EK <= min(iz, jz); ++EK)
+        for (int EJ = max(iy, jy) - 1; EJ <= min(iy, jy); ++EJ)
+          for (int EI = max(ix, jx) - 1; EI <= min(ix, jx); ++EI) {
+            if (EI < 0 || EJ < 0 || EK < 0 || EI >= ncx || EJ >= ncy || EK >= ncz)
+              continue;
+            const int ln = (ix - EI) + 2 * (iy - EJ) + 4 * (iz - EK);
+            const int lm = (jx - EI) + 2 * (jy - EJ) + 4 * (jz - EK);
+            const int sl = slot[((int64_t)EK * ncy + EJ) * ncx + EI];
+            if (sl >= 0) {
+              anyflag = true;
+              const double *g = G + ((int64_t)sl * 64 + ln * 8 + lm) * 9;
+#pragma unroll
+              for (int q = 0; q < 9; ++q) acc[q] += g[q];
+              continue;
+            }
+            for (int i = 0; i < 8; ++i) {
+              const int ex = 2 * EI + (i & 1), ey = 2 * EJ + ((i >> 1) & 1),
+                        ez = 2 * EK + ((i >> 2) & 1);
+              const double Ee = E[((int64_t)ez * nely + ey) * nelx + ex];
+              const double *m = GMi + ((i * 8 + ln) * 8 + lm) * 9;
+#pragma unroll
+              for (int q = 0; q < 9; ++q) acc[q] += Ee * __ldg(m + q);
+            }
+          }
+      if (anyflag) {
+        // P^T (I - M) P: identity dofs in the support of both N and M
+        for (int gz = max(2 * iz, 2 * jz) - 1; gz <= min(2 * iz, 2 * jz) + 1; ++gz)
+          for (int gy = max(2 * iy, 2 * jy) - 1; gy <= min(2 * iy, 2 * jy) + 1; ++gy)
+            for (int gx = max(2 * ix, 2 * jx) - 1; gx <= min(2 * ix, 2 * jx) + 1; ++gx) {
+              if (gx < 0 || gy < 0 || gz < 0 || gx >= fx || gy >= fy || gz >= fz) continue;
+              const unsigned bits = idm[((int64_t)gz * fy + gy) * fx + gx];
+              if (!bits) continue;
+              const double w = pw1(gx, ix, fx) * pw1(gy, iy, fy) * pw1(gz, iz, fz) *
+                               pw1(gx, jx, fx) * pw1(gy, jy, fy) * pw1(gz, jz, fz);
+              for (int c = 0; c < 3; ++c)
+                if ((bits >> c) & 1u) acc[4 * c] += w;
+            }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) Sc[(int64_t)(nb * 9 + q) * nnc + I] = acc[q];
+  }
+}
+
 // A_c(I, I+delta) = sum_f sum_g P(f,I) A_f(f,g) P(g,I+delta); one thread
 // per (coarse node, delta) block.  Fine nodes f run over the support of I
 // and g over the stencil of f intersected with the support of J, both in
@@ -415,6 +576,39 @@ void launch_stencil_to_half(int64_t nn, const double *S, double *H64,
                             float *H32, cudaStream_t s) {
   count_launch();
   k_stencil_to_half<<<grid_for(126 * nn, 256), 256, 0, s>>>(nn, S, H64, H32);
+}
+
+int launch_galerkin_fine(Ctx &c, double *Sc, cudaStream_t s) {
+  const int64_t nce = (int64_t)((c.nel[0] + 1) / 2) * ((c.nel[1] + 1) / 2) *
+                      ((c.nel[2] + 1) / 2);
+  count_launch(1);
+  if (cudaMemsetAsync(c.gk_count, 0, sizeof(unsigned int), s) != cudaSuccess) return TPO_E_CUDA;
+  k_coarse_elem_flags<<<grid_for(nce, 128), 128, 0, s>>>(c.nel[0], c.nel[1], c.nel[2],
+                                                          c.idm, c.gk_slot, c.gk_elem,
+                                                          c.gk_count);
+  unsigned int nslots = 0;
+  if (cudaMemcpyAsync(&nslots, c.gk_count, sizeof(unsigned int), cudaMemcpyDeviceToHost, s) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return TPO_E_CUDA;
+  if ((size_t)nslots * 576 > c.gk_cap) {
+    if (c.gk_G) cudaFree(c.gk_G);
+    c.gk_G = nullptr;
+    c.gk_cap = 0;
+    const size_t cap = std::max<size_t>((size_t)nslots * 576, 576);
+    if (cudaMalloc(&c.gk_G, sizeof(double) * cap) != cudaSuccess) return TPO_E_CUDA;
+    c.gk_cap = cap;
+  }
+  if (nslots) {
+    count_launch();
+    k_galerkin_general<<<grid_for(64 * (int64_t)nslots, 128, 1 << 20), 128, 0, s>>>(
+        c.nel[0], c.nel[1], c.nel[2], (int)nslots, c.E64, c.idm, c.gk_elem, c.K0lex,
+        c.gk_G);
+  }
+  count_launch();
+  k_galerkin_fine<<<grid_for(27 * c.lev[1].nn, 128, 1 << 20), 128, 0, s>>>(
+      c.nel[0], c.nel[1], c.nel[2], c.E64, c.idm, c.gk_slot, c.gk_G, c.GMi, Sc);
+  return TPO_OK;
 }
 
 void launch_galerkin(const Level &fine, const double *Sf, const Level &coarse,

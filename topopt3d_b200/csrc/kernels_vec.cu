@@ -211,18 +211,18 @@ static dim3 col_grid(int64_t n, int nb) {
 
 template <typename T>
 void launch_dot(const Ctx &c, int64_t n, const T *a, const T *b, double *out,
-                double *shift_to, cudaStream_t s, int nb) {
+                double *shift_to, cudaStream_t s, int nb, double *part,
+                unsigned int *ticket) {
   count_launch();
-  k_dot<T><<<dim3(red_grid(nb), nb), kRedThreads, 0, s>>>(n, a, b, c.part,
-                                                          c.ticket, out,
-                                                          shift_to);
+  k_dot<T><<<dim3(red_grid(nb), nb), kRedThreads, 0, s>>>(
+      n, a, b, part ? part : c.part, ticket ? ticket : c.ticket, out, shift_to);
 }
 template void launch_dot<double>(const Ctx &, int64_t, const double *,
                                  const double *, double *, double *,
-                                 cudaStream_t, int);
+                                 cudaStream_t, int, double *, unsigned int *);
 template void launch_dot<float>(const Ctx &, int64_t, const float *,
                                 const float *, double *, double *,
-                                cudaStream_t, int);
+                                cudaStream_t, int, double *, unsigned int *);
 
 template <typename T>
 void launch_cg_p(int64_t n, const T *z, T *p, const double *scal, bool first,

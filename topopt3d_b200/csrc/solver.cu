@@ -346,39 +346,72 @@ void invalidate_graphs(Ctx &c) {
   c.graph64_nb = c.graph32_nb = 0;
 }
 
-int estimate_lambda(Ctx &c, int l, int its, double *lam) {
+// power iteration for lambda_max(D^-1 A_l) on stream s, no host sync: the
+// squared norm of the last iterate ends in scal[SC_POWER + l].  The start
+// vector is the splitmix64 sequence the oracle shares.
+void power_iteration(Ctx &c, int l, int its, cudaStream_t s, double *part,
+                     unsigned int *ticket) {
   Level &v = c.lev[l];
   const int64_t n = 3 * v.nn;
-  cudaStream_t s = c.stream;
   double *a = v.d64, *w = v.a64;
-  double *nrm = c.scal + SC_POWER;
+  double *nrm = c.scal + SC_POWER + l;
   launch_power_start(n, a, s);
-  launch_dot<double>(c, n, a, a, nrm, nullptr, s);
+  launch_dot<double>(c, n, a, a, nrm, nullptr, s, 1, part, ticket);
   launch_power_normalize(n, a, a, nullptr, nrm, s);
   for (int k = 0; k < its; ++k) {
     level_apply<double>(c, l, a, nullptr, w, s);
     launch_scale_diag(n, w, v.dinv64, s);
-    launch_dot<double>(c, n, w, w, nrm, nullptr, s);
+    launch_dot<double>(c, n, w, w, nrm, nullptr, s, 1, part, ticket);
     launch_power_normalize(n, a, w, nullptr, nrm, s);
   }
+}
+
+int estimate_lambda(Ctx &c, int l, int its, double *lam) {
+  cudaStream_t s = c.stream;
+  power_iteration(c, l, its, s, nullptr, nullptr);
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(c.scal_h + SC_POWER, nrm, sizeof(double),
+  CK(cudaMemcpyAsync(c.scal_h + SC_POWER + l, c.scal + SC_POWER + l, sizeof(double),
                      cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
-  *lam = std::sqrt(c.scal_h[SC_POWER]);
+  *lam = std::sqrt(c.scal_h[SC_POWER + l]);
   return TPO_OK;
 }
 
 int setup_hierarchy(Ctx &c, const tpo_solve_opts &o) {
   const double t0 = now_ms();
-  cudaStream_t s = c.stream;
+  cudaStream_t s = c.stream, s2 = c.aux_stream;
   invalidate_graphs(c);
-  // fine level: Jacobi diagonal and the assembled stencil for Galerkin
+  // Chebyshev bounds (power iterations) of each smoothed level run on the
+  // side stream s2 as soon as that level's operator is built on s, with
+  // their own reduction scratch; the Galerkin chain and the coarsest
+  // factorisation proceed on s meanwhile
+  double *part2 = c.part + kAuxPart;
+  unsigned int *ticket2 = c.ticket + kMaxBatch;
+  auto level_ready = [&](int l) -> int {
+    if (l + 1 >= c.L) return TPO_OK;   // the coarsest level is not smoothed
+    CK(cudaEventRecord(c.lev_ev[l], s));
+    CK(cudaStreamWaitEvent(s2, c.lev_ev[l], 0));
+    power_iteration(c, l, o.power_its, s2, part2, ticket2);
+    return TPO_OK;
+  };
+  auto join = [&]() {
+    cudaEventRecord(c.aux_ev, s2);
+    cudaStreamWaitEvent(s, c.aux_ev, 0);
+  };
+  // fine level: Jacobi diagonal (and the assembled stencil when it is the
+  // only level)
   launch_fine_diag(c, c.lev[0].dinv64, c.lev[0].dinv32, s);
-  if (c.L > 1 || true) launch_fine_stencil(c, c.S0, s);
+  if (c.L == 1) launch_fine_stencil(c, c.S0, s);
+  if (int rc = level_ready(0)) return rc;
   for (int l = 0; l + 1 < c.L; ++l) {
-    const double *Sf = (l == 0) ? c.S0 : c.lev[l].S64;
-    launch_galerkin(c.lev[l], Sf, c.lev[l + 1], c.lev[l + 1].S64, s);
+    if (l == 0) {
+      if (launch_galerkin_fine(c, c.lev[1].S64, s) != TPO_OK) {
+        join();
+        c.err = "level-1 Galerkin product failed";
+        return TPO_E_CUDA;
+      }
+    } else
+      launch_galerkin(c.lev[l], c.lev[l].S64, c.lev[l + 1], c.lev[l + 1].S64, s);
     launch_stencil_diag(c.lev[l + 1], c.lev[l + 1].S64, c.lev[l + 1].dinv64,
                         c.lev[l + 1].dinv32, s);
     if (l + 1 < c.ps)
@@ -387,6 +420,10 @@ int setup_hierarchy(Ctx &c, const tpo_solve_opts &o) {
     if (l + 1 >= c.ps && l + 1 < c.L - 1)
       launch_soa_to_aos(c.lev[l + 1].nn, c.lev[l + 1].S64, c.lev[l + 1].A64,
                         c.lev[l + 1].A32, s);
+    if (int rc = level_ready(l + 1)) {
+      join();
+      return rc;
+    }
   }
   CK(cudaGetLastError());
   // coarsest level: dense Cholesky, then the explicit inverse for a
@@ -402,6 +439,7 @@ int setup_hierarchy(Ctx &c, const tpo_solve_opts &o) {
   if (!h) {
     if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) {
       c.err = "cusolverDnCreate failed";
+      join();
       return TPO_E_CUDA;
     }
     c.cusolver = h;
@@ -411,6 +449,7 @@ int setup_hierarchy(Ctx &c, const tpo_solve_opts &o) {
   if (cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, (int)nc, c.Adense,
                                   (int)nc, &lwork) != CUSOLVER_STATUS_SUCCESS) {
     c.err = "cusolverDnDpotrf_bufferSize failed";
+    join();
     return TPO_E_CUDA;
   }
   if ((size_t)lwork > c.solver_work_n) {
@@ -424,6 +463,7 @@ int setup_hierarchy(Ctx &c, const tpo_solve_opts &o) {
       cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, (int)nc, (int)nc, c.Adense,
                        (int)nc, c.Ainv, (int)nc, c.dev_info) != CUSOLVER_STATUS_SUCCESS) {
     c.err = "coarse Cholesky factorisation failed";
+    join();
     return TPO_E_CUDA;
   }
   int info_h = 0;
@@ -432,14 +472,15 @@ int setup_hierarchy(Ctx &c, const tpo_solve_opts &o) {
   if (info_h != 0) {
     c.err = "coarsest operator is not positive definite (potrf info " +
             std::to_string(info_h) + ")";
+    join();
     return TPO_E_BREAKDOWN;
   }
-  // Chebyshev bounds
-  for (int l = 0; l + 1 < c.L; ++l) {
-    double lam = 0;
-    if (int rc = estimate_lambda(c, l, o.power_its, &lam)) return rc;
-    c.lev[l].lam = lam;
-  }
+  // Chebyshev bounds from the side stream
+  join();
+  CK(cudaMemcpyAsync(c.scal_h + SC_POWER, c.scal + SC_POWER, sizeof(double) * c.L,
+                     cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  for (int l = 0; l + 1 < c.L; ++l) c.lev[l].lam = std::sqrt(c.scal_h[SC_POWER + l]);
   c.setup_opts = o;
   c.assembled = true;
   c.setup_ms = now_ms() - t0;

@@ -105,6 +105,11 @@ struct Ctx {
   int device = 0;
   cudaStream_t stream = nullptr;      // stream all work is issued on
   cudaStream_t own_stream = nullptr;  // the context's own stream
+  // set-up side stream (Chebyshev bound estimates overlap the Galerkin
+  // chain) and its events
+  cudaStream_t aux_stream = nullptr;
+  cudaEvent_t lev_ev[16] = {};
+  cudaEvent_t aux_ev = nullptr;
   std::string err;
 
   // element constants
@@ -124,12 +129,27 @@ struct Ctx {
 
   // device state
   uint8_t *fix = nullptr;   // per-node fixed-component bitmask
+  // identity-row mask of the fine operator: fix | non-positive diagonal
+  // (kernels_apply.cu, k_identity_mask); refreshed whenever E or fix change
+  uint8_t *idm = nullptr;
   double *F = nullptr, *U = nullptr;
   double *x = nullptr, *rho = nullptr, *E64 = nullptr, *dEdz = nullptr;
   double *Es64 = nullptr;   // rho^p without E_min (stress stiffness)
   float *E32 = nullptr;
   double *S0 = nullptr;     // fine-level assembled stencil (setup only)
   double *K0lex = nullptr;  // K0 in lexicographic corner order (576)
+  // level-1 Galerkin blocks of interior fine elements, [i][ln][lm][9]
+  // (element.cpp, build_galerkin_blocks), and the per-coarse-element
+  // general-path flags
+  double *GMi = nullptr;
+  double GMi_h[8 * 8 * 8 * 9];
+  // general-path coarse elements of the level-1 Galerkin product: slot per
+  // coarse element (-1: fast path), the element of each slot, the count,
+  // and the 64 blocks of 9 per slot
+  int *gk_slot = nullptr, *gk_elem = nullptr;
+  unsigned int *gk_count = nullptr;
+  double *gk_G = nullptr;
+  size_t gk_cap = 0;
   double *Ainv = nullptr;   // dense inverse of the coarsest operator
   int64_t nc = 0;
 
@@ -205,7 +225,9 @@ enum { SC_COMPLIANCE = kScalMisc, SC_VOLUME, SC_OC_DG, SC_OC_CHANGE, SC_POWER };
 inline int red_grid(int nb) {
   return nb <= 1 ? kRedBlocks : (kRedBlocks / nb < 148 ? 148 : kRedBlocks / nb);
 }
-constexpr int kPartCount = 2048;   // >= red_grid(nb) * nb for nb <= kMaxBatch
+constexpr int kPartCount = 4096;   // >= kAuxPart + red_grid(1), and red_grid(nb) * nb <= kAuxPart
+// the set-up side stream's reductions use part + kAuxPart, ticket + kMaxBatch
+constexpr int kAuxPart = 2048;
 
 // fine matrix-free operator: y = M K M u + (1-M) u, or y = b - (that)
 template <typename T>
@@ -233,6 +255,7 @@ void launch_apply_fused(const Ctx &c, const T *E, int in, int out,
 void launch_fine_diag(const Ctx &c, double *dinv64, float *dinv32,
                       cudaStream_t s);
 void launch_fine_stencil(const Ctx &c, double *S, cudaStream_t s);
+void launch_identity_mask(const Ctx &c, cudaStream_t s);
 
 // stencil levels
 template <typename T>
@@ -245,6 +268,9 @@ void launch_stencil_to_half(int64_t nn, const double *S, double *H64,
                             float *H32, cudaStream_t s);
 void launch_galerkin(const Level &fine, const double *Sf, const Level &coarse,
                      double *Sc, cudaStream_t s);
+// level 1 = P^T A_0 P from the element moduli (no fine stencil); syncs
+// the stream once (the general-path element count)
+int launch_galerkin_fine(Ctx &c, double *Sc, cudaStream_t s);
 void launch_stencil_diag(const Level &v, const double *S, double *dinv64,
                          float *dinv32, cudaStream_t s);
 template <typename T>
@@ -275,9 +301,12 @@ void launch_cheb_step(int64_t n, const T *dinv, const T *Ad, T *r, T *d, T *x,
 // vectors and reductions (FP64 accumulation; results in device scalars).
 // With nb columns, n is the length of one column and the scalars of column
 // j are at (pointer) + j * kColScal.
+// part/ticket: reduction scratch other than the context's (for a reduction
+// that runs concurrently with others); null = the context's
 template <typename T>
 void launch_dot(const Ctx &c, int64_t n, const T *a, const T *b, double *out,
-                double *shift_to, cudaStream_t s, int nb = 1);
+                double *shift_to, cudaStream_t s, int nb = 1,
+                double *part = nullptr, unsigned int *ticket = nullptr);
 template <typename T>
 void launch_cg_p(int64_t n, const T *z, T *p, const double *scal, bool first,
                  cudaStream_t s, int nb = 1);
