@@ -184,6 +184,7 @@ int alloc_solver(Ctx &c) {
       }
     }
   }
+  if (c.L > 2) A(c.gd_tmp, tpo::galerkin_dims_scratch(c.lev[1]));
   const int64_t nc = 3 * c.lev[c.L - 1].nn;
   A(c.Adense, (size_t)(nc * nc));
   A(c.Ainv, (size_t)(nc * nc));
@@ -202,7 +203,7 @@ void free_all(Ctx &c) {
   dfree(c.fix); dfree(c.idm); dfree(c.F); dfree(c.U); dfree(c.x); dfree(c.rho);
   dfree(c.E64); dfree(c.dEdz); dfree(c.E32); dfree(c.S0); dfree(c.K0lex);
   dfree(c.GMi); dfree(c.gk_slot); dfree(c.gk_elem); dfree(c.gk_count);
-  dfree(c.gk_G); c.gk_cap = 0;
+  dfree(c.gk_G); c.gk_cap = 0; dfree(c.gd_tmp);
   dfree(c.Ainv); dfree(c.Adense); dfree(c.solver_work); dfree(c.dev_info);
   dfree(c.finv); dfree(c.taps_d);
   dfree(c.w64);

@@ -200,6 +200,60 @@ __global__ void k_galerkin_fine(int nelx, int nely, int nelz,
   }
 }
 
+// One dimension of the Galerkin product: P = P_x (x) P_y (x) P_z, so
+// P^T A P = P_z^T (P_y^T (P_x^T A P_x) P_y) P_z and each factor keeps a
+// 27-point 3x3-block stencil.  Coarsening dimension D of a grid n[3]:
+//   A'(O, O+Delta) = sum_{f_D} sum_{g_D = f_D + d_D} w(f_D -> O_D)
+//                    w(g_D -> O_D + Delta_D) A(f, f + d),
+// with f = O except f_D and d = Delta except d_D: at most 7 (Delta_D = 0)
+// or 3 input blocks per output block, instead of up to 343 for the direct
+// triple product.  w is the normalised 1-D weight pw1.
+template <int D>
+__global__ void k_galerkin_dim(int nx, int ny, int nz, const double *__restrict__ Sin,
+                               double *__restrict__ Sout) {
+  const int n[3] = {nx, ny, nz};
+  int m[3] = {nx, ny, nz};
+  m[D] = (n[D] + 1) / 2;
+  const int64_t nin = (int64_t)nx * ny * nz, nout = (int64_t)m[0] * m[1] * m[2];
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 27 * nout;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int nb = (int)(t / nout);
+    const int64_t O = t - (int64_t)nb * nout;
+    int o[3] = {(int)(O % m[0]), (int)((O / m[0]) % m[1]), (int)(O / ((int64_t)m[0] * m[1]))};
+    const int dl[3] = {nb % 3 - 1, (nb / 3) % 3 - 1, nb / 9 - 1};
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    bool inside = true;
+#pragma unroll
+    for (int e = 0; e < 3; ++e) inside &= (o[e] + dl[e] >= 0 && o[e] + dl[e] < m[e]);
+    if (inside) {
+      const int I = o[D], J = o[D] + dl[D];
+      for (int fd = 2 * I - 1; fd <= 2 * I + 1; ++fd) {
+        if (fd < 0 || fd >= n[D]) continue;
+        const double wi = pw1(fd, I, n[D]);
+        if (wi == 0.0) continue;
+        int f[3] = {o[0], o[1], o[2]};
+        f[D] = fd;
+        const int64_t fi = ((int64_t)f[2] * ny + f[1]) * nx + f[0];
+        for (int dd = -1; dd <= 1; ++dd) {
+          const int gd = fd + dd;
+          if (gd < 0 || gd >= n[D]) continue;
+          const double wj = pw1(gd, J, n[D]);
+          if (wj == 0.0) continue;
+          int d3[3] = {dl[0], dl[1], dl[2]};
+          d3[D] = dd;
+          const int fnb = (d3[2] + 1) * 9 + (d3[1] + 1) * 3 + (d3[0] + 1);
+          const double w = wi * wj;
+          const double *blk = Sin + (int64_t)fnb * 9 * nin + fi;
+#pragma unroll
+          for (int q = 0; q < 9; ++q) acc[q] += w * blk[q * nin];
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) Sout[(int64_t)(nb * 9 + q) * nout + O] = acc[q];
+  }
+}
+
 // A_c(I, I+delta) = sum_f sum_g P(f,I) A_f(f,g) P(g,I+delta); one thread
 // per (coarse node, delta) block.  Fine nodes f run over the support of I
 // and g over the stencil of f intersected with the support of J, both in
@@ -609,6 +663,25 @@ int launch_galerkin_fine(Ctx &c, double *Sc, cudaStream_t s) {
   k_galerkin_fine<<<grid_for(27 * c.lev[1].nn, 128, 1 << 20), 128, 0, s>>>(
       c.nel[0], c.nel[1], c.nel[2], c.E64, c.idm, c.gk_slot, c.gk_G, c.GMi, Sc);
   return TPO_OK;
+}
+
+void launch_galerkin_dims(const Level &fine, const double *Sf, double *Sc,
+                          double *tmp, cudaStream_t s) {
+  const int fx = fine.dims[0], fy = fine.dims[1], fz = fine.dims[2];
+  const int cx = (fx + 1) / 2, cy = (fy + 1) / 2;
+  const int64_t n1 = (int64_t)cx * fy * fz, n2 = (int64_t)cx * cy * fz;
+  double *t1 = tmp, *t2 = tmp + 243 * n1;
+  count_launch(3);
+  k_galerkin_dim<0><<<grid_for(27 * n1, 128, 1 << 20), 128, 0, s>>>(fx, fy, fz, Sf, t1);
+  k_galerkin_dim<1><<<grid_for(27 * n2, 128, 1 << 20), 128, 0, s>>>(cx, fy, fz, t1, t2);
+  const int64_t n3 = n2 / fz * ((fz + 1) / 2);
+  k_galerkin_dim<2><<<grid_for(27 * n3, 128, 1 << 20), 128, 0, s>>>(cx, cy, fz, t2, Sc);
+}
+
+size_t galerkin_dims_scratch(const Level &fine) {
+  const int fx = fine.dims[0], fy = fine.dims[1], fz = fine.dims[2];
+  const int cx = (fx + 1) / 2, cy = (fy + 1) / 2;
+  return 243 * ((size_t)cx * fy * fz + (size_t)cx * cy * fz);
 }
 
 void launch_galerkin(const Level &fine, const double *Sf, const Level &coarse,

@@ -410,8 +410,9 @@ int setup_hierarchy(Ctx &c, const tpo_solve_opts &o) {
         c.err = "level-1 Galerkin product failed";
         return TPO_E_CUDA;
       }
-    } else
-      launch_galerkin(c.lev[l], c.lev[l].S64, c.lev[l + 1], c.lev[l + 1].S64, s);
+    } else {
+      launch_galerkin_dims(c.lev[l], c.lev[l].S64, c.lev[l + 1].S64, c.gd_tmp, s);
+    }
     launch_stencil_diag(c.lev[l + 1], c.lev[l + 1].S64, c.lev[l + 1].dinv64,
                         c.lev[l + 1].dinv32, s);
     if (l + 1 < c.ps)

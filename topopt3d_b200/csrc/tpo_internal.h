@@ -150,6 +150,8 @@ struct Ctx {
   unsigned int *gk_count = nullptr;
   double *gk_G = nullptr;
   size_t gk_cap = 0;
+  // scratch of the dimension-by-dimension Galerkin products (levels >= 1)
+  double *gd_tmp = nullptr;
   double *Ainv = nullptr;   // dense inverse of the coarsest operator
   int64_t nc = 0;
 
@@ -268,6 +270,11 @@ void launch_stencil_to_half(int64_t nn, const double *S, double *H64,
                             float *H32, cudaStream_t s);
 void launch_galerkin(const Level &fine, const double *Sf, const Level &coarse,
                      double *Sc, cudaStream_t s);
+// the same product one dimension at a time (three launches through tmp,
+// galerkin_dims_scratch doubles)
+void launch_galerkin_dims(const Level &fine, const double *Sf, double *Sc,
+                          double *tmp, cudaStream_t s);
+size_t galerkin_dims_scratch(const Level &fine);
 // level 1 = P^T A_0 P from the element moduli (no fine stencil); syncs
 // the stream once (the general-path element count)
 int launch_galerkin_fine(Ctx &c, double *Sc, cudaStream_t s);
