@@ -369,6 +369,56 @@ __global__ void k_stencil_to_half(int64_t nn, const double *__restrict__ S,
   }
 }
 
+// one column
+template <typename T, bool RESID>
+__global__ void k_apply_stencil_sym1(int nx, int ny, int nz,
+                                     const T *__restrict__ H,
+                                     const T *__restrict__ u,
+                                     const T *__restrict__ b, T *__restrict__ y) {
+  const int nn = nx * ny * nz;
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nn;
+       n += gridDim.x * blockDim.x) {
+    const int i = n % nx, j = (n / nx) % ny, k = n / (nx * ny);
+    T a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll
+    for (int h = 0; h < 14; ++h) {
+      const int nb = 13 + h;
+      const int di = nb % 3 - 1, dj = (nb / 3) % 3 - 1, dk = nb / 9 - 1;
+      // forward block A(n, n+d): zero when n+d is outside, index clamped
+      {
+        const int mi = min(i + di, nx - 1), mj = min(max(j + dj, 0), ny - 1),
+                  mk = min(k + dk, nz - 1);
+        const int m = (mk * ny + mj) * nx + max(mi, 0);
+        const T u0 = u[3 * m], u1 = u[3 * m + 1], u2 = u[3 * m + 2];
+        const T *s = H + (int64_t)h * 9 * nn + n;
+        a0 += s[0] * u0 + s[nn] * u1 + s[2 * (int64_t)nn] * u2;
+        a1 += s[3 * (int64_t)nn] * u0 + s[4 * (int64_t)nn] * u1 + s[5 * (int64_t)nn] * u2;
+        a2 += s[6 * (int64_t)nn] * u0 + s[7 * (int64_t)nn] * u1 + s[8 * (int64_t)nn] * u2;
+      }
+      // backward block A(n, n-d) = A(n-d, n)^T, stored by node n-d
+      if (h > 0) {
+        const int mi = i - di, mj = j - dj, mk = k - dk;
+        const bool in = mi >= 0 && mi < nx && mj >= 0 && mj < ny && mk >= 0 && mk < nz;
+        const int m = in ? (mk * ny + mj) * nx + mi : n;
+        const T w = in ? T(1) : T(0);
+        const T u0 = w * u[3 * m], u1 = w * u[3 * m + 1], u2 = w * u[3 * m + 2];
+        const T *s = H + (int64_t)h * 9 * nn + m;
+        a0 += s[0] * u0 + s[3 * (int64_t)nn] * u1 + s[6 * (int64_t)nn] * u2;
+        a1 += s[nn] * u0 + s[4 * (int64_t)nn] * u1 + s[7 * (int64_t)nn] * u2;
+        a2 += s[2 * (int64_t)nn] * u0 + s[5 * (int64_t)nn] * u1 + s[8 * (int64_t)nn] * u2;
+      }
+    }
+    if (RESID) {
+      a0 = b[3 * n] - a0;
+      a1 = b[3 * n + 1] - a1;
+      a2 = b[3 * n + 2] - a2;
+    }
+    y[3 * n] = a0;
+    y[3 * n + 1] = a1;
+    y[3 * n + 2] = a2;
+  }
+}
+
 // NB columns (stride ld) share every coefficient load
 template <typename T, bool RESID, int NB>
 __global__ void k_apply_stencil_sym(int nx, int ny, int nz,
@@ -587,12 +637,16 @@ template <typename T, bool RESID, int NB>
 void sym_launch(const Level &v, const T *H, const T *u, const T *b, T *y,
                 cudaStream_t s) {
   count_launch();
-  // one thread per node carries NB columns: a wider column block needs
-  // fewer threads in flight for the same bytes
   const int g = grid_for(v.nn, 128);
-  k_apply_stencil_sym<T, RESID, NB><<<g, 128, 0, s>>>(
-      v.dims[0], v.dims[1], v.dims[2], H, u, b, y, 3 * v.nn);
+  if (NB == 1)
+    k_apply_stencil_sym1<T, RESID><<<g, 128, 0, s>>>(v.dims[0], v.dims[1],
+                                                    v.dims[2], H, u, b, y);
+  else
+    k_apply_stencil_sym<T, RESID, NB><<<g, 128, 0, s>>>(
+        v.dims[0], v.dims[1], v.dims[2], H, u, b, y, 3 * v.nn);
 }
+
+
 
 template <typename T, bool RESID>
 void sym_dispatch(const Level &v, const T *H, const T *u, const T *b, T *y,

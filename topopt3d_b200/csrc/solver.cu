@@ -415,9 +415,10 @@ int setup_hierarchy(Ctx &c, const tpo_solve_opts &o) {
     }
     launch_stencil_diag(c.lev[l + 1], c.lev[l + 1].S64, c.lev[l + 1].dinv64,
                         c.lev[l + 1].dinv32, s);
-    if (l + 1 < c.ps)
+    if (l + 1 < c.ps) {
       launch_stencil_to_half(c.lev[l + 1].nn, c.lev[l + 1].S64, c.lev[l + 1].H64,
                              c.lev[l + 1].H32, s);
+    }
     if (l + 1 >= c.ps && l + 1 < c.L - 1)
       launch_soa_to_aos(c.lev[l + 1].nn, c.lev[l + 1].S64, c.lev[l + 1].A64,
                         c.lev[l + 1].A32, s);
