@@ -61,7 +61,7 @@ __device__ __forceinline__ void fetch_node(const ApplyArgs<T> &a,
                                            int gx, int gy, int z, int Nx, int Ny,
                                            int Nz, NodeReg<T> &r) {
   if (gx >= 0 && gx < Nx && gy >= 0 && gy < Ny && z >= 0 && z < Nz) {
-    const int64_t n = ((int64_t)z * Ny + gy) * Nx + gx;
+    const int n = (z * Ny + gy) * Nx + gx;
     r.f = __ldg(fix + n);
     r.v[0] = input_value<T, IN>(a, 3 * n);
     r.v[1] = input_value<T, IN>(a, 3 * n + 1);
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(32 * TY)
     // element layer z-1 is applied when plane z is the top plane
     const int ez = z - 1;
     nE = (exy && ez >= 0 && ez < nelz)
-             ? __ldg(E + ((int64_t)ez * nely + gy) * nelx + gx)
+             ? __ldg(E + (ez * nely + gy) * nelx + gx)
              : T(0);
   };
 
@@ -175,6 +175,7 @@ __global__ void __launch_bounds__(32 * TY)
   for (int c = 0; c < 3; ++c) les[c] = led[c] = T(0);
 
   fetch(zs - 1);
+#pragma unroll 2
   for (int p = zs - 1; p <= ze + 1; ++p) {
     // ---- plane p: take the prefetched values, prefetch plane p + 1
     T cu[3], cr[3], cq[3], crq[3];
@@ -237,7 +238,7 @@ __global__ void __launch_bounds__(32 * TY)
         val[c] = (es - ed) + left;
       }
       if (tx >= 1 && ty >= 1 && gx < Nx && gy < Ny) {
-        const int64_t n = ((int64_t)(p - 2) * Ny + gy) * Nx + gx;
+        const int n = ((p - 2) * Ny + gy) * Nx + gx;
         const unsigned f = __ldg(fix + n);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
