@@ -49,7 +49,8 @@ def parse():
     ap.add_argument("--no-multi-rhs", action="store_true")
     ap.add_argument("--no-buckling", action="store_true")
     # profiling case: set up `--config` and launch one operation `--reps`
-    # times with nothing else around it (for ncu captures; prints no line)
+    # times with nothing else around it (for ncu captures; prints no line);
+    # --config also selects the reference arm's problem (default 192x96x96)
     ap.add_argument("--kernel", default=None,
                     choices=["apply32", "apply64", "vcycle32", "vcycle64",
                              "solve_mixed", "solve_fp64"])
@@ -329,9 +330,10 @@ def run_ours(args, rank, world, local):
         "clocks": clocks,
     }
     t.set_stream(None)
-    if not args.no_multi_rhs:
+    # per-GPU figures of the other workloads: measured on one GPU only
+    if not args.no_multi_rhs and world == 1:
         line["multi_rhs"] = run_multi_rhs(args, T, P, torch, dev, stream)
-    if not args.no_buckling:
+    if not args.no_buckling and world == 1:
         line["buckling"] = run_buckling(args, T, P, torch, dev, stream)
 
     if not args.no_e2e:
@@ -457,19 +459,20 @@ def run_e2e(args, T, P, t, x, world, dev, torch):
 
 # ------------------------------------------------------------ CPU baseline
 
-def cpu_baseline(sample_its=3, steps=None, warmup=0):
+def cpu_baseline(sample_its=3, steps=None, warmup=0, cfg=CONFIG):
     """The oracle's assembled FP64 PCG + GMG (OpenMP, all host threads) on
-    the same 192x96x96 problem.  Without `steps`: one complete solve from
+    the same problem (192x96x96 unless `cfg` names another).  Without `steps`: one complete solve from
     U = 0 is timed (solves/s = 1 / its time).  With `steps` (the reference
     arm): each step runs `sample_its` PCG iterations and solves/s = 1 /
     (per-iteration time x iterations of the full solve)."""
     from oracle import oracle as O
     from topopt3d_b200 import problems as P
-    c = P.CONFIGS[CONFIG]
+    c = P.CONFIGS[cfg]
     cores = os.cpu_count()
     ref = O.Problem(c["nel"], rmin=c["rmin"], mg_levels=c["levels"])
-    P.apply_bcs(ref, P.bcs(CONFIG))
-    ref.set_design(P.design(CONFIG), 3.0, 1e-10)
+    P.apply_bcs(ref, P.bcs(cfg))
+    ref.set_design(P.design(cfg), 3.0, 1e-10)
+    mesh = "x".join(str(v) for v in c["nel"])
     t0 = time.perf_counter()
     ref.assemble(O.default_opts())
     setup_s = time.perf_counter() - t0
@@ -479,7 +482,7 @@ def cpu_baseline(sample_its=3, steps=None, warmup=0):
     if not steps:
         return {"value": round(1.0 / full_s, 6), "unit": UNIT, "cores": cores,
                 "kind": "port",
-                "sample": f"one complete FP64 PCG+GMG solve from U=0 of the 192x96x96 "
+                "sample": f"one complete FP64 PCG+GMG solve from U=0 of the {mesh} "
                           f"problem ({its_full} iterations, relres {rr:.2e}, status {st}; "
                           f"assembled BSR SpMV, Galerkin PtAP, OpenMP); set-up "
                           f"{setup_s:.1f} s untimed",
@@ -498,7 +501,7 @@ def cpu_baseline(sample_its=3, steps=None, warmup=0):
     per_it = sample()
     out = {"value": round(1.0 / (per_it * its_full), 6), "unit": UNIT,
            "cores": cores, "kind": "port",
-           "sample": f"{sample_its} PCG+GMG iterations of the 192x96x96 problem "
+           "sample": f"{sample_its} PCG+GMG iterations of the {mesh} problem "
                      f"(assembled BSR SpMV, FP64, OpenMP) x {its_full} iterations of "
                      f"the full solve; setup {setup_s:.1f} s and a full solve "
                      f"({full_s:.1f} s, status {st}) untimed",
@@ -518,13 +521,15 @@ def run_reference(args, rank, world):
     so its CPU path runs as the oracle restatement."""
     if rank != 0:
         return None
-    cb = cpu_baseline(sample_its=2, steps=args.steps, warmup=min(args.warmup, 1))
+    cb = cpu_baseline(sample_its=2, steps=args.steps, warmup=min(args.warmup, 1),
+                      cfg=args.config)
     return {"impl": "reference", "metric": METRIC, "value": cb["value"],
             "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "192x96x96 hex8 cantilever, 5,447,811 dof, FP64 "
-                                   "PCG + 5-level GMG to 1e-8 (CPU)"},
+            "config": ({"workload": "192x96x96 hex8 cantilever, 5,447,811 dof, FP64 "
+                                    "PCG + 5-level GMG to 1e-8 (CPU)"}
+                       if args.config == CONFIG else {"workload": args.config}),
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
