@@ -254,71 +254,6 @@ __global__ void k_galerkin_dim(int nx, int ny, int nz, const double *__restrict_
   }
 }
 
-// A_c(I, I+delta) = sum_f sum_g P(f,I) A_f(f,g) P(g,I+delta); one thread
-// per (coarse node, delta) block.  Fine nodes f run over the support of I
-// and g over the stencil of f intersected with the support of J, both in
-// increasing index order.
-__global__ void k_galerkin(int fx, int fy, int fz, int cx, int cy, int cz,
-                           const double *__restrict__ Sf,
-                           double *__restrict__ Sc) {
-  const int64_t nnf = (int64_t)fx * fy * fz, nnc = (int64_t)cx * cy * cz;
-  const int64_t total = nnc * 27;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int nb = (int)(t / nnc);
-    const int64_t I = t - (int64_t)nb * nnc;
-    const int ix = I % cx, iy = (I / cx) % cy, iz = I / ((int64_t)cx * cy);
-    const int jx = ix + nb % 3 - 1, jy = iy + (nb / 3) % 3 - 1, jz = iz + nb / 9 - 1;
-    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    if (jx >= 0 && jx < cx && jy >= 0 && jy < cy && jz >= 0 && jz < cz) {
-      for (int az = -1; az <= 1; ++az) {
-        const int gzf = 2 * iz + az;
-        if (gzf < 0 || gzf >= fz) continue;
-        const double wiz = pw1(gzf, iz, fz);
-        if (wiz == 0.0) continue;
-        for (int ay = -1; ay <= 1; ++ay) {
-          const int gyf = 2 * iy + ay;
-          if (gyf < 0 || gyf >= fy) continue;
-          const double wiy = pw1(gyf, iy, fy);
-          if (wiy == 0.0) continue;
-          for (int ax = -1; ax <= 1; ++ax) {
-            const int gxf = 2 * ix + ax;
-            if (gxf < 0 || gxf >= fx) continue;
-            const double wix = pw1(gxf, ix, fx);
-            if (wix == 0.0) continue;
-            const double wI = wix * wiy * wiz;
-            const int64_t f = ((int64_t)gzf * fy + gyf) * fx + gxf;
-            for (int ez = -1; ez <= 1; ++ez) {
-              const int hz = gzf + ez;
-              if (hz < 0 || hz >= fz) continue;
-              const double wjz = pw1(hz, jz, fz);
-              if (wjz == 0.0) continue;
-              for (int ey = -1; ey <= 1; ++ey) {
-                const int hy = gyf + ey;
-                if (hy < 0 || hy >= fy) continue;
-                const double wjy = pw1(hy, jy, fy);
-                if (wjy == 0.0) continue;
-                for (int ex = -1; ex <= 1; ++ex) {
-                  const int hx = gxf + ex;
-                  if (hx < 0 || hx >= fx) continue;
-                  const double wjx = pw1(hx, jx, fx);
-                  if (wjx == 0.0) continue;
-                  const double w = wI * (wjx * wjy * wjz);
-                  const int fnb = (ez + 1) * 9 + (ey + 1) * 3 + (ex + 1);
-                  const double *blk = Sf + (int64_t)fnb * 9 * nnf + f;
-#pragma unroll
-                  for (int q = 0; q < 9; ++q) acc[q] += w * blk[q * nnf];
-                }
-              }
-            }
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < 9; ++q) Sc[(int64_t)(nb * 9 + q) * nnc + I] = acc[q];
-  }
-}
 
 template <typename T, bool RESID>
 __global__ void k_apply_stencil(int nx, int ny, int nz, const T *__restrict__ S,
@@ -738,13 +673,6 @@ size_t galerkin_dims_scratch(const Level &fine) {
   return 243 * ((size_t)cx * fy * fz + (size_t)cx * cy * fz);
 }
 
-void launch_galerkin(const Level &fine, const double *Sf, const Level &coarse,
-                     double *Sc, cudaStream_t s) {
-  count_launch();
-  k_galerkin<<<grid_for(coarse.nn * 27, 128, 1 << 20), 128, 0, s>>>(
-      fine.dims[0], fine.dims[1], fine.dims[2], coarse.dims[0], coarse.dims[1],
-      coarse.dims[2], Sf, Sc);
-}
 
 void launch_stencil_diag(const Level &v, const double *S, double *dinv64,
                          float *dinv32, cudaStream_t s) {

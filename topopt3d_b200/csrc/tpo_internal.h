@@ -268,8 +268,6 @@ void launch_apply_stencil_sym(const Level &v, const T *H, const T *u,
                               const T *b, T *y, cudaStream_t s, int nb = 1);
 void launch_stencil_to_half(int64_t nn, const double *S, double *H64,
                             float *H32, cudaStream_t s);
-void launch_galerkin(const Level &fine, const double *Sf, const Level &coarse,
-                     double *Sc, cudaStream_t s);
 // the same product one dimension at a time (three launches through tmp,
 // galerkin_dims_scratch doubles)
 void launch_galerkin_dims(const Level &fine, const double *Sf, double *Sc,
