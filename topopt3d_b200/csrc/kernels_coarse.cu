@@ -123,10 +123,12 @@ __device__ __forceinline__ T pick(const T a[3], int q) {
   return q == 0 ? a[0] : (q == 1 ? a[1] : a[2]);
 }
 
-// at least 2 co-resident blocks per SM (<= 128 registers) for every width:
+// co-resident blocks per SM: 4 for one column (<= 64 registers; measured
+// best of 1..6, the small spills cost less than the missing warps), 2 (<= 128
+// registers) for wider blocks:
 // the phases are latency-bound and need the warps
 template <typename T, int NB>
-__global__ void __launch_bounds__(kCoarseThreads, NB == 1 ? 3 : 2)
+__global__ void __launch_bounds__(kCoarseThreads, NB == 1 ? 4 : 2)
     k_coarse_cycle(CoarseCycle<T> P) {
   cg::grid_group grid = cg::this_grid();
   const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
