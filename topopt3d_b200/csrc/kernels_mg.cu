@@ -304,12 +304,41 @@ __global__ void k_stencil_to_half(int64_t nn, const double *__restrict__ S,
   }
 }
 
-// one column
-template <typename T, bool RESID>
+// one column; IN / OUT select how the input is formed and what the
+// epilogue writes, as in the fine-level kernel (kernels_apply_staged.cu,
+// finish_dof): IN_U reads u, IN_CHEB forms the Chebyshev start
+// invtheta D^-1 b on the fly; OUT_Y / OUT_RESID / OUT_CHEB2 / OUT_POST0 /
+// OUT_POST1 write Au, b - Au or the fused Chebyshev(2) updates
+template <typename T, int IN>
+__device__ __forceinline__ T sym_in(const ApplyArgs<T> &a, int i) {
+  if (IN == IN_CHEB) return a.invtheta * (a.dinv[i] * a.b[i]);
+  return a.u[i];
+}
+
+template <typename T, int OUT>
+__device__ __forceinline__ void sym_out(const ApplyArgs<T> &a, int i, T Au, T u) {
+  if (OUT == OUT_Y) {
+    a.y[i] = Au;
+  } else if (OUT == OUT_RESID) {
+    a.y[i] = a.b[i] - Au;
+  } else if (OUT == OUT_CHEB2) {
+    const T di = a.dinv[i], bi = a.b[i];
+    const T r1 = di * bi - di * Au;
+    a.y[i] = u + (a.c1 * u + a.c2 * r1);
+  } else if (OUT == OUT_POST0) {
+    const T d0 = a.invtheta * (a.dinv[i] * (a.b[i] - Au));
+    a.y[i] = d0;
+    a.y2[i] = u + d0;
+  } else {   // OUT_POST1
+    const T r1 = a.theta * u - a.dinv[i] * Au;
+    a.y[i] = a.y2[i] + (a.c1 * u + a.c2 * r1);
+  }
+}
+
+template <typename T, int IN, int OUT>
 __global__ void k_apply_stencil_sym1(int nx, int ny, int nz,
                                      const T *__restrict__ H,
-                                     const T *__restrict__ u,
-                                     const T *__restrict__ b, T *__restrict__ y) {
+                                     const ApplyArgs<T> args) {
   const int nn = nx * ny * nz;
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nn;
        n += gridDim.x * blockDim.x) {
@@ -324,7 +353,8 @@ __global__ void k_apply_stencil_sym1(int nx, int ny, int nz,
         const int mi = min(i + di, nx - 1), mj = min(max(j + dj, 0), ny - 1),
                   mk = min(k + dk, nz - 1);
         const int m = (mk * ny + mj) * nx + max(mi, 0);
-        const T u0 = u[3 * m], u1 = u[3 * m + 1], u2 = u[3 * m + 2];
+        const T u0 = sym_in<T, IN>(args, 3 * m), u1 = sym_in<T, IN>(args, 3 * m + 1),
+                u2 = sym_in<T, IN>(args, 3 * m + 2);
         const T *s = H + (int64_t)h * 9 * nn + n;
         a0 += s[0] * u0 + s[nn] * u1 + s[2 * (int64_t)nn] * u2;
         a1 += s[3 * (int64_t)nn] * u0 + s[4 * (int64_t)nn] * u1 + s[5 * (int64_t)nn] * u2;
@@ -336,21 +366,19 @@ __global__ void k_apply_stencil_sym1(int nx, int ny, int nz,
         const bool in = mi >= 0 && mi < nx && mj >= 0 && mj < ny && mk >= 0 && mk < nz;
         const int m = in ? (mk * ny + mj) * nx + mi : n;
         const T w = in ? T(1) : T(0);
-        const T u0 = w * u[3 * m], u1 = w * u[3 * m + 1], u2 = w * u[3 * m + 2];
+        const T u0 = w * sym_in<T, IN>(args, 3 * m), u1 = w * sym_in<T, IN>(args, 3 * m + 1),
+                u2 = w * sym_in<T, IN>(args, 3 * m + 2);
         const T *s = H + (int64_t)h * 9 * nn + m;
         a0 += s[0] * u0 + s[3 * (int64_t)nn] * u1 + s[6 * (int64_t)nn] * u2;
         a1 += s[nn] * u0 + s[4 * (int64_t)nn] * u1 + s[7 * (int64_t)nn] * u2;
         a2 += s[2 * (int64_t)nn] * u0 + s[5 * (int64_t)nn] * u1 + s[8 * (int64_t)nn] * u2;
       }
     }
-    if (RESID) {
-      a0 = b[3 * n] - a0;
-      a1 = b[3 * n + 1] - a1;
-      a2 = b[3 * n + 2] - a2;
-    }
-    y[3 * n] = a0;
-    y[3 * n + 1] = a1;
-    y[3 * n + 2] = a2;
+    const bool need_u = OUT == OUT_CHEB2 || OUT == OUT_POST0 || OUT == OUT_POST1;
+    const T Au[3] = {a0, a1, a2};
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      sym_out<T, OUT>(args, 3 * n + c, Au[c], need_u ? sym_in<T, IN>(args, 3 * n + c) : T(0));
   }
 }
 
@@ -573,10 +601,14 @@ void sym_launch(const Level &v, const T *H, const T *u, const T *b, T *y,
                 cudaStream_t s) {
   count_launch();
   const int g = grid_for(v.nn, 128);
-  if (NB == 1)
-    k_apply_stencil_sym1<T, RESID><<<g, 128, 0, s>>>(v.dims[0], v.dims[1],
-                                                    v.dims[2], H, u, b, y);
-  else
+  if (NB == 1) {
+    ApplyArgs<T> a{};
+    a.u = u;
+    a.b = b;
+    a.y = y;
+    k_apply_stencil_sym1<T, IN_U, RESID ? OUT_RESID : OUT_Y><<<g, 128, 0, s>>>(
+        v.dims[0], v.dims[1], v.dims[2], H, a);
+  } else
     k_apply_stencil_sym<T, RESID, NB><<<g, 128, 0, s>>>(
         v.dims[0], v.dims[1], v.dims[2], H, u, b, y, 3 * v.nn);
 }
@@ -599,6 +631,28 @@ void sym_dispatch(const Level &v, const T *H, const T *u, const T *b, T *y,
     nb -= w;
   }
 }
+
+template <typename T>
+void launch_apply_sym_fused(const Level &v, const T *H, int in, int out,
+                            const ApplyArgs<T> &a, cudaStream_t s) {
+  count_launch();
+  const int g = grid_for(v.nn, 128);
+  const int nx = v.dims[0], ny = v.dims[1], nz = v.dims[2];
+  if (in == IN_CHEB && out == OUT_CHEB2)
+    k_apply_stencil_sym1<T, IN_CHEB, OUT_CHEB2><<<g, 128, 0, s>>>(nx, ny, nz, H, a);
+  else if (out == OUT_POST0)
+    k_apply_stencil_sym1<T, IN_U, OUT_POST0><<<g, 128, 0, s>>>(nx, ny, nz, H, a);
+  else if (out == OUT_POST1)
+    k_apply_stencil_sym1<T, IN_U, OUT_POST1><<<g, 128, 0, s>>>(nx, ny, nz, H, a);
+  else if (out == OUT_RESID)
+    k_apply_stencil_sym1<T, IN_U, OUT_RESID><<<g, 128, 0, s>>>(nx, ny, nz, H, a);
+  else
+    k_apply_stencil_sym1<T, IN_U, OUT_Y><<<g, 128, 0, s>>>(nx, ny, nz, H, a);
+}
+template void launch_apply_sym_fused<double>(const Level &, const double *, int, int,
+                                             const ApplyArgs<double> &, cudaStream_t);
+template void launch_apply_sym_fused<float>(const Level &, const float *, int, int,
+                                            const ApplyArgs<float> &, cudaStream_t);
 
 template <typename T>
 void launch_apply_stencil_sym(const Level &v, const T *H, const T *u,

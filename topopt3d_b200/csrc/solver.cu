@@ -140,10 +140,15 @@ void vcycle_rec(Ctx &c, int l, const T *b, T *x, const tpo_solve_opts &o,
   LV<T> w = lv(v, (T *)nullptr);
   const int64_t n = 3 * v.nn;
   const Cheb ch = cheb_of(v.lam, o);
-  if (l == 0 && o.cheb_degree == 2) {
-    // fine level, Chebyshev(2): the smoother updates run in the epilogues
-    // of the matrix-free apply (kernels_apply_staged.cu, finish_dof)
+  const bool fine_fused = (l == 0);
+  const bool sym_fused = (l >= 1 && l < c.ps && nb == 1);
+  if (o.cheb_degree == 2 && (fine_fused || sym_fused)) {
+    // Chebyshev(2): the smoother updates run in the epilogues of the
+    // operator kernel (the matrix-free apply on the fine level,
+    // kernels_apply_staged.cu; the half-stored stencil below the
+    // persistent levels, kernels_mg.cu), 4 launches per level
     const T *E = fineE(c, (T *)nullptr);
+    const T *H = halfS(v, (T *)nullptr);
     const double rn = 1.0 / (2.0 * ch.sigma - ch.rho0);
     ApplyArgs<T> a{};
     a.b = b;
@@ -152,22 +157,30 @@ void vcycle_rec(Ctx &c, int l, const T *b, T *x, const tpo_solve_opts &o,
     a.theta = static_cast<T>(ch.theta);
     a.c1 = static_cast<T>(rn * ch.rho0);
     a.c2 = static_cast<T>(2.0 * rn / ch.delta);
+    auto fused = [&](int in, int out) {
+      if (fine_fused)
+        launch_apply_fused<T>(c, E, in, out, a, s, nb);
+      else
+        launch_apply_sym_fused<T>(v, H, in, out, a, s);
+    };
     a.y = x;
-    launch_apply_fused<T>(c, E, IN_CHEB, OUT_CHEB2, a, s, nb);   // pre-smooth
-    launch_apply_fine<T>(c, E, x, b, w.a, s, nb);                 // residual
+    fused(IN_CHEB, OUT_CHEB2);                                 // pre-smooth
+    a.u = x;                                                   // residual
+    a.y = w.a;
+    fused(IN_U, OUT_RESID);
     Level &cv = c.lev[l + 1];
     LV<T> cw = lv(cv, (T *)nullptr);
     launch_restrict<T>(v, cv, w.a, cw.b, s, nb);
     vcycle_rec<T>(c, l + 1, cw.b, cw.x, o, s, nb);
     launch_prolong_add<T>(v, cv, cw.x, x, s, nb);
-    a.u = x;                                                  // post-smooth
+    a.u = x;                                                   // post-smooth
     a.y = w.d;
     a.y2 = w.r;
-    launch_apply_fused<T>(c, E, IN_U, OUT_POST0, a, s, nb);
+    fused(IN_U, OUT_POST0);
     a.u = w.d;
     a.y = x;
     a.y2 = w.r;
-    launch_apply_fused<T>(c, E, IN_U, OUT_POST1, a, s, nb);
+    fused(IN_U, OUT_POST1);
     return;
   }
   // pre-smoothing from a zero guess

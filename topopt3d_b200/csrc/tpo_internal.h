@@ -266,6 +266,11 @@ void launch_apply_stencil(const Level &v, const T *S, const T *u, const T *b,
 template <typename T>
 void launch_apply_stencil_sym(const Level &v, const T *H, const T *u,
                               const T *b, T *y, cudaStream_t s, int nb = 1);
+// the symmetric-half stencil of one column with the fused Chebyshev(2)
+// input/epilogue modes of the fine level (ApplyArgs: u, b, dinv, y, y2)
+template <typename T>
+void launch_apply_sym_fused(const Level &v, const T *H, int in, int out,
+                            const ApplyArgs<T> &a, cudaStream_t s);
 void launch_stencil_to_half(int64_t nn, const double *S, double *H64,
                             float *H32, cudaStream_t s);
 // the same product one dimension at a time (three launches through tmp,
