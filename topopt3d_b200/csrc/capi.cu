@@ -211,7 +211,7 @@ void free_all(Ctx &c) {
   c.eig_n = 0;
   if (c.cublas) cublasDestroy(static_cast<cublasHandle_t>(c.cublas));
   c.cublas = nullptr;
-  dfree(c.scal); dfree(c.part); dfree(c.ticket); dfree(c.tmpe); dfree(c.tmpe2);
+  dfree(c.scal); dfree(c.part); dfree(c.ticket); dfree(c.gbar); dfree(c.tmpe); dfree(c.tmpe2);
   dfree(c.io_a); dfree(c.io_b);
   dfree(c.oc_ws);
   if (c.scal_h) cudaFreeHost(c.scal_h);
@@ -374,6 +374,7 @@ int tpo_create(const tpo_mesh_params *p, tpo_ctx **out) {
   A(c.Es64, c.ne);
   A(c.fix, c.nn); A(c.idm, c.nn); A(c.F, 3 * c.nn); A(c.U, 3 * c.nn);
   A(c.scal, tpo::kScalCount); A(c.part, tpo::kPartCount); A(c.ticket, 2 * tpo::kMaxBatch);
+  A(c.gbar, 1);
   A(c.tmpe, c.ne); A(c.tmpe2, c.ne); A(c.dev_info, 1);
   A(c.io_a, nio); A(c.io_b, nio);
 #undef A

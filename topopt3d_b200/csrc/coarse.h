@@ -17,7 +17,7 @@ template <typename T>
 struct CoarseLevel {
   int dims[3];
   int64_t nn;
-  const T *A;      // the Galerkin stencil, node-major: A[n*243 + nb*9 + 3r+s]
+  const T *A;      // the Galerkin stencil, node-major: A[n*243 + (3r+s)*27 + nb]
   const T *dinv;   // 1 / diag
   T *b;            // right-hand side (restricted residual of the parent)
   T *xpre;         // pre-smoothed iterate, then + P x_child
@@ -39,6 +39,9 @@ struct CoarseCycle {
   int cdims[3];                      // coarsest nodes per dimension
   T *bc, *xc;                        // coarsest right-hand side / solution
                                      // (column stride nc)
+  unsigned int *bar;                 // grid-barrier counter (zero between
+                                     // launches)
+  double *fault;                     // set to 1 when a barrier wait runs out
 };
 
 template <typename T>

@@ -5,9 +5,9 @@
 // smoothing step, transfer or residual is a microseconds-long latency-bound
 // launch; a launch per phase would cost more than the work.  Here the grid
 // stays resident (one cooperative launch sized to the co-resident block
-// count) and the phases are separated by grid-wide barriers
-// (cooperative_groups grid sync, valid because the launch guarantees
-// co-residency).  Each phase is a grid-stride loop over nodes.  A block of
+// count) and the phases are separated by grid-wide barriers (grid_barrier
+// below, valid because the launch guarantees co-residency).  Each phase is
+// a grid-stride loop over nodes.  A block of
 // NB right-hand sides rides through the same barriers: the stencil of a
 // node is read once for all NB columns.
 //
@@ -20,21 +20,57 @@
 //   res = b - A x;  b_c = P^T res;  (recurse);  x += P x_c
 //   post: r = D^-1 (b - A x), d = r/theta, x' = x + d;  m-1 x [...]
 // The level math is the one of the per-level kernels in kernels_mg.cu.
-#include <cooperative_groups.h>
-
 #include "coarse.h"
 #include "transfer.cuh"
 
 namespace tpo {
 
-namespace cg = cooperative_groups;
-
 namespace {
 
+// polls of one grid-barrier wait before it gives up (a poll is an L2 round
+// trip, so this is seconds; a phase takes microseconds)
+constexpr int kBarrierPolls = 1 << 22;
+
+// Grid-wide barrier of the persistent kernel, a sense-reversing counter:
+// block 0 adds 2^31 - (blocks - 1) and every other block adds 1, so once all
+// blocks have arrived bit 31 has flipped and the low bits are back where
+// they started (zero), ready for the next barrier or launch.  The arrival
+// is an atomic with release semantics at GPU scope, made after the block
+// barrier so it covers the writes of every thread of the block; the wait
+// polls with acquire loads, and the closing block barrier passes the
+// acquire on to the other threads.  (A barrier on a counter of our own is
+// used rather than the cooperative-groups grid sync: with the latter the
+// phase after each sync ran about twice as long on B200.)  A wait that runs
+// out of polls sets *fault, read by the host with the solver scalars, and
+// returns false; the caller then returns from the kernel.
+__device__ __forceinline__ bool grid_barrier(unsigned int *bar, double *fault) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned int add = blockIdx.x == 0 ? 0x80000000u - (gridDim.x - 1) : 1u;
+    unsigned int old, cur;
+    asm volatile("atom.add.release.gpu.u32 %0, [%1], %2;"
+                 : "=r"(old) : "l"(bar), "r"(add) : "memory");
+    int polls = 0;
+    ok = 1;
+    do {
+      asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(cur) : "l"(bar) : "memory");
+      if (++polls > kBarrierPolls) {
+        ok = 0;
+        *(volatile double *)fault = 1.0;
+        break;
+      }
+    } while (((old ^ cur) & 0x80000000u) == 0u);
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
 // y_n = sum_delta A(n, n+delta) u_{n+delta} for one node by one warp, for
-// NB columns: lane `q` < 27 loads block q (9 contiguous values of the
-// node-major copy, so the warp reads 243 consecutive values) and the
-// neighbour's u of every column.  The 3 NB partial sums are then reduced
+// NB columns: lane `q` < 27 loads block q and the neighbour's u of every
+// column.  The node-major copy interleaves the 27 blocks per coefficient
+// (A[n*243 + (3r+s)*27 + q]), so each of the 9 loads of the warp reads 27
+// consecutive values.  The 3 NB partial sums are then reduced
 // across the warp by a reduce-scatter: at each of the first log2(NB)
 // butterfly steps a lane keeps half of its columns and sends the other
 // half, so that afterwards the lanes of group col = lane / (32 / NB) hold
@@ -58,10 +94,10 @@ __device__ __forceinline__ void warp_stencil(const CoarseLevel<T> &L, int n,
     const int mj = min(max(j + (lane / 3) % 3 - 1, 0), ny - 1);
     const int mk = min(max(k + lane / 9 - 1, 0), nz - 1);
     const int m = (mk * ny + mj) * nx + mi;
-    const T *s = L.A + (int64_t)n * 243 + lane * 9;
+    const T *s = L.A + (int64_t)n * 243 + lane;
     T a[9];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) a[q] = s[q];
+    for (int q = 0; q < 9; ++q) a[q] = s[q * 27];
     T di0 = T(0), di1 = T(0), di2 = T(0);
     if (FROM_B) {
       di0 = L.inv_theta * L.dinv[3 * m];
@@ -130,7 +166,6 @@ __device__ __forceinline__ T pick(const T a[3], int q) {
 template <typename T, int NB>
 __global__ void __launch_bounds__(kCoarseThreads, NB == 1 ? 4 : 2)
     k_coarse_cycle(CoarseCycle<T> P) {
-  cg::grid_group grid = cg::this_grid();
   const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
   const int lane = threadIdx.x & 31;
@@ -162,12 +197,12 @@ __global__ void __launch_bounds__(kCoarseThreads, NB == 1 ? 4 : 2)
           L.xpre[i] = d0 + d;
         }
       }
-      grid.sync();
+      if (!grid_barrier(P.bar, P.fault)) return;
       T *t = dc; dc = dn; dn = t;
     } else {
       for (int64_t i = tid; i < NB * ld; i += nthr)
         L.xpre[i] = L.inv_theta * (L.dinv[i % ld] * L.b[i]);
-      grid.sync();
+      if (!grid_barrier(P.bar, P.fault)) return;
     }
     for (int k = 2; k < L.deg; ++k) {
       for (int n = gwarp; n < nn; n += nwarps) {
@@ -183,7 +218,7 @@ __global__ void __launch_bounds__(kCoarseThreads, NB == 1 ? 4 : 2)
           L.xpre[i] += d;
         }
       }
-      grid.sync();
+      if (!grid_barrier(P.bar, P.fault)) return;
       T *t = dc; dc = dn; dn = t;
     }
     for (int n = gwarp; n < nn; n += nwarps) {
@@ -194,7 +229,7 @@ __global__ void __launch_bounds__(kCoarseThreads, NB == 1 ? 4 : 2)
         L.res[i] = L.b[i] - pick(a, lm.comp);
       }
     }
-    grid.sync();
+    if (!grid_barrier(P.bar, P.fault)) return;
     // b_child = P^T res
     const bool dense_next = (l + 1 == P.nlev);
     T *bc = dense_next ? P.bc : P.lev[l + 1].b;
@@ -215,7 +250,7 @@ __global__ void __launch_bounds__(kCoarseThreads, NB == 1 ? 4 : 2)
         o[3 * I + 2] = s[2];
       }
     }
-    grid.sync();
+    if (!grid_barrier(P.bar, P.fault)) return;
   }
 
   // ---------------- coarsest: x = Ainv b, a warp per row, FP64 accumulation
@@ -243,7 +278,7 @@ __global__ void __launch_bounds__(kCoarseThreads, NB == 1 ? 4 : 2)
     for (int c = 0; c < NB; ++c)
       if (lane == c) P.xc[c * P.nc + row] = static_cast<T>(s[c]);
   }
-  grid.sync();
+  if (!grid_barrier(P.bar, P.fault)) return;
 
   // ---------------- up-sweep: prolong-add, post-smooth
   for (int l = P.nlev - 1; l >= 0; --l) {
@@ -269,7 +304,7 @@ __global__ void __launch_bounds__(kCoarseThreads, NB == 1 ? 4 : 2)
         x[3 * f + 2] += s[2];
       }
     }
-    grid.sync();
+    if (!grid_barrier(P.bar, P.fault)) return;
     for (int n = gwarp; n < nn; n += nwarps) {
       T a[3];
       warp_stencil<T, NB>(L, n, L.xpre, lane, a);
@@ -283,7 +318,7 @@ __global__ void __launch_bounds__(kCoarseThreads, NB == 1 ? 4 : 2)
         L.xout[i] = L.xpre[i] + d;
       }
     }
-    grid.sync();
+    if (!grid_barrier(P.bar, P.fault)) return;
     T *dc = L.d0, *dn = L.d1;
     for (int k = 1; k < L.deg; ++k) {
       for (int n = gwarp; n < nn; n += nwarps) {
@@ -299,7 +334,7 @@ __global__ void __launch_bounds__(kCoarseThreads, NB == 1 ? 4 : 2)
           L.xout[i] += d;
         }
       }
-      grid.sync();
+      if (!grid_barrier(P.bar, P.fault)) return;
       T *t = dc; dc = dn; dn = t;
     }
   }

@@ -786,7 +786,8 @@ __global__ void k_soa_to_aos(int64_t nn, const double *__restrict__ S,
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nn * 243;
        t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t n = t / 243;
-    const int q = (int)(t - n * 243);
+    const int w = (int)(t - n * 243);   // (3r+s)*27 + nb
+    const int q = (w % 27) * 9 + w / 27;
     const double v = S[(int64_t)q * nn + n];
     A64[t] = v;
     A32[t] = static_cast<float>(v);

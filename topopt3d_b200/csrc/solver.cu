@@ -118,6 +118,8 @@ CoarseCycle<T> coarse_cycle_params(Ctx &c, const tpo_solve_opts &o) {
   for (int d = 0; d < 3; ++d) P.cdims[d] = cl.dims[d];
   P.bc = cw.b;
   P.xc = cw.x;
+  P.bar = c.gbar;
+  P.fault = c.scal + kSlotFault;
   return P;
 }
 
@@ -240,6 +242,15 @@ int readback(Ctx &c, int nb) {
   CK(cudaMemcpyAsync(c.scal_h, c.scal, sizeof(double) * kColScal * nb,
                      cudaMemcpyDeviceToHost, c.stream));
   CK(cudaStreamSynchronize(c.stream));
+  if (c.scal_h[kSlotFault] != 0.0) {
+    // a grid barrier of the coarse-grid kernel gave up waiting: the blocks
+    // returned and the counter may be mid-barrier, so clear both
+    c.scal_h[kSlotFault] = 0.0;
+    CK(cudaMemsetAsync(c.gbar, 0, sizeof(unsigned int), c.stream));
+    CK(cudaMemsetAsync(c.scal + kSlotFault, 0, sizeof(double), c.stream));
+    c.err = "coarse-grid kernel: a grid-barrier wait ran out";
+    return TPO_E_CUDA;
+  }
   return TPO_OK;
 }
 

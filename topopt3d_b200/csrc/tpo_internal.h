@@ -73,7 +73,7 @@ struct Level {
   // S[(nb*9 + 3r + s) * nn + node], nb = (dk+1)*9 + (dj+1)*3 + (di+1)
   double *S64 = nullptr;
   float *S32 = nullptr;
-  // node-major copies A[n*243 + nb*9 + 3r + s] for the persistent kernel
+  // node-major copies A[n*243 + (3r + s)*27 + nb] for the persistent kernel
   double *A64 = nullptr;
   float *A32 = nullptr;
   // symmetric half (centre + 13 forward blocks) for the levels between the
@@ -170,6 +170,8 @@ struct Ctx {
   double *scal_h = nullptr; // pinned host mirror
   double *part = nullptr;   // reduction partials
   unsigned int *ticket = nullptr;
+  unsigned int *gbar = nullptr;  // grid-barrier counter of the persistent
+                                 // coarse-grid kernel (kernels_coarse.cu)
   double *tmpe = nullptr, *tmpe2 = nullptr;   // element-sized scratch
   double *io_a = nullptr, *io_b = nullptr;    // staging for host buffers
   double *io_ba = nullptr, *io_bb = nullptr;  // the same for column blocks
@@ -215,13 +217,16 @@ constexpr int kRedBlocks = 592;   // 4 x 148 SMs: fixed grid for reductions
 // column has kColScal device scalars at scal + j * kColScal:
 //   0 rho = r.z, 1 rho of the previous iteration, 2 p.q, 3 r.r (current
 //   PCG), 4 b.b, 5 r.r of the FP64 residual, 6 frozen flag (non-zero: the
-//   column has converged and its CG updates are skipped), 7 spare.
+//   column has converged and its CG updates are skipped), 7 (column 0
+//   only) fault flag of the persistent coarse-grid kernel: non-zero when a
+//   grid-barrier wait ran out (read with the other scalars by readback).
 // Scalars of the design-side calls follow the column block at kScalMisc.
 constexpr int kMaxBatch = 8;
 constexpr int kColScal = 8;
 constexpr int kScalMisc = kMaxBatch * kColScal;   // 64
 constexpr int kScalCount = kScalMisc + 16;
 enum { SC_COMPLIANCE = kScalMisc, SC_VOLUME, SC_OC_DG, SC_OC_CHANGE, SC_POWER };
+constexpr int kSlotFault = 7;
 
 // fixed reduction grid (blocks per column) for a block of nb columns
 inline int red_grid(int nb) {
@@ -292,7 +297,8 @@ void launch_prolong_add(const Level &fine, const Level &coarse, const T *xc,
 void launch_to_dense(const Level &v, const double *S, double *A,
                      cudaStream_t s);
 void launch_eye(int64_t n, double *A, cudaStream_t s);
-// stencil SoA S[q*nn + n] -> node-major A[n*243 + q] (FP64 and an FP32 copy)
+// stencil SoA S[(nb*9 + 3r+s)*nn + n] -> node-major A[n*243 + (3r+s)*27 + nb]
+// (FP64 and an FP32 copy)
 void launch_soa_to_aos(int64_t nn, const double *S, double *A64, float *A32,
                        cudaStream_t s);
 template <typename T>
