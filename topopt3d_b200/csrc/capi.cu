@@ -218,15 +218,20 @@ void free_all(Ctx &c) {
   c.scal_h = nullptr;
   if (c.cusolver) cusolverDnDestroy(static_cast<cusolverDnHandle_t>(c.cusolver));
   c.cusolver = nullptr;
-  if (c.aux_stream) cudaStreamSynchronize(c.aux_stream);
+  for (cudaStream_t &q : c.aux_stream)
+    if (q) cudaStreamSynchronize(q);
   for (cudaEvent_t &e : c.lev_ev) {
     if (e) cudaEventDestroy(e);
     e = nullptr;
   }
-  if (c.aux_ev) cudaEventDestroy(c.aux_ev);
-  c.aux_ev = nullptr;
-  if (c.aux_stream) cudaStreamDestroy(c.aux_stream);
-  c.aux_stream = nullptr;
+  for (cudaEvent_t &e : c.aux_ev) {
+    if (e) cudaEventDestroy(e);
+    e = nullptr;
+  }
+  for (cudaStream_t &q : c.aux_stream) {
+    if (q) cudaStreamDestroy(q);
+    q = nullptr;
+  }
   if (c.own_stream) cudaStreamDestroy(c.own_stream);
   c.own_stream = c.stream = nullptr;
 }
@@ -355,9 +360,10 @@ int tpo_create(const tpo_mesh_params *p, tpo_ctx **out) {
     delete ctx;
     return code;
   };
-  if (cudaStreamCreateWithFlags(&c.aux_stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&c.aux_ev, cudaEventDisableTiming) != cudaSuccess)
-    return fail(TPO_E_CUDA);
+  for (int i = 0; i < tpo::kAuxStreams; ++i)
+    if (cudaStreamCreateWithFlags(&c.aux_stream[i], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c.aux_ev[i], cudaEventDisableTiming) != cudaSuccess)
+      return fail(TPO_E_CUDA);
   for (cudaEvent_t &e : c.lev_ev)
     if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
       return fail(TPO_E_CUDA);
@@ -373,7 +379,7 @@ int tpo_create(const tpo_mesh_params *p, tpo_ctx **out) {
   A(c.x, c.ne); A(c.rho, c.ne); A(c.E64, c.ne); A(c.dEdz, c.ne); A(c.E32, c.ne);
   A(c.Es64, c.ne);
   A(c.fix, c.nn); A(c.idm, c.nn); A(c.F, 3 * c.nn); A(c.U, 3 * c.nn);
-  A(c.scal, tpo::kScalCount); A(c.part, tpo::kPartCount); A(c.ticket, 2 * tpo::kMaxBatch);
+  A(c.scal, tpo::kScalCount); A(c.part, tpo::kPartCount); A(c.ticket, tpo::kMaxBatch + tpo::kAuxStreams);
   A(c.gbar, 1);
   A(c.tmpe, c.ne); A(c.tmpe2, c.ne); A(c.dev_info, 1);
   A(c.io_a, nio); A(c.io_b, nio);

@@ -778,6 +778,17 @@ __global__ void k_eye(int64_t n, double *A) {
        t += (int64_t)gridDim.x * blockDim.x)
     A[t] = (t / n == t % n) ? 1.0 : 0.0;
 }
+
+// full symmetric n x n matrix from the lower triangle of a column-major one:
+// A(r, c) = L(max(r, c), min(r, c))
+__global__ void k_sym_from_lower(int64_t n, const double *__restrict__ L,
+                                 double *__restrict__ A) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = t / n, r = t - c * n;
+    A[t] = r >= c ? L[t] : L[r * n + c];
+  }
+}
 }  // namespace
 
 namespace {
@@ -804,6 +815,11 @@ void launch_soa_to_aos(int64_t nn, const double *S, double *A64, float *A32,
 void launch_eye(int64_t n, double *A, cudaStream_t s) {
   count_launch();
   k_eye<<<grid_for(n * n, 256), 256, 0, s>>>(n, A);
+}
+
+void launch_sym_from_lower(int64_t n, const double *L, double *A, cudaStream_t s) {
+  count_launch();
+  k_sym_from_lower<<<grid_for(n * n, 256), 256, 0, s>>>(n, L, A);
 }
 
 template <typename T>

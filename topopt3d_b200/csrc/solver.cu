@@ -5,6 +5,7 @@
 // :673): KSP CG, nonzero initial guess, convergence on the unpreconditioned
 // residual ||b - K u|| <= rtol ||b||, PCMG with Galerkin coarse operators,
 // Chebyshev/Jacobi smoothing and a direct (here Cholesky) coarse solve.
+#include <cublas_v2.h>
 #include <cusolverDn.h>
 
 #include <algorithm>
@@ -403,24 +404,27 @@ int estimate_lambda(Ctx &c, int l, int its, double *lam) {
 
 int setup_hierarchy(Ctx &c, const tpo_solve_opts &o) {
   const double t0 = now_ms();
-  cudaStream_t s = c.stream, s2 = c.aux_stream;
+  cudaStream_t s = c.stream;
   invalidate_graphs(c);
-  // Chebyshev bounds (power iterations) of each smoothed level run on the
-  // side stream s2 as soon as that level's operator is built on s, with
-  // their own reduction scratch; the Galerkin chain and the coarsest
-  // factorisation proceed on s meanwhile
-  double *part2 = c.part + kAuxPart;
-  unsigned int *ticket2 = c.ticket + kMaxBatch;
+  // Chebyshev bounds (power iterations) of each smoothed level run on a
+  // side stream as soon as that level's operator is built on s, with their
+  // own reduction scratch: level l on side stream l % kAuxStreams, so the
+  // levels' latency-bound iterations overlap one another as well as the
+  // Galerkin chain and the coarsest factorisation on s
   auto level_ready = [&](int l) -> int {
     if (l + 1 >= c.L) return TPO_OK;   // the coarsest level is not smoothed
+    const int i = l % kAuxStreams;
     CK(cudaEventRecord(c.lev_ev[l], s));
-    CK(cudaStreamWaitEvent(s2, c.lev_ev[l], 0));
-    power_iteration(c, l, o.power_its, s2, part2, ticket2);
+    CK(cudaStreamWaitEvent(c.aux_stream[i], c.lev_ev[l], 0));
+    power_iteration(c, l, o.power_its, c.aux_stream[i],
+                    c.part + kAuxPart + i * kRedBlocks, c.ticket + kMaxBatch + i);
     return TPO_OK;
   };
   auto join = [&]() {
-    cudaEventRecord(c.aux_ev, s2);
-    cudaStreamWaitEvent(s, c.aux_ev, 0);
+    for (int i = 0; i < kAuxStreams; ++i) {
+      cudaEventRecord(c.aux_ev[i], c.aux_stream[i]);
+      cudaStreamWaitEvent(s, c.aux_ev[i], 0);
+    }
   };
   // fine level: Jacobi diagonal (and the assembled stencil when it is the
   // only level)
@@ -452,8 +456,11 @@ int setup_hierarchy(Ctx &c, const tpo_solve_opts &o) {
     }
   }
   CK(cudaGetLastError());
-  // coarsest level: dense Cholesky, then the explicit inverse for a
-  // bandwidth-parallel GEMV inside the V-cycle
+  // coarsest level: dense Cholesky A = L L^T, then the explicit inverse
+  // A^-1 = X^T X with X = L^-1 (one triangular solve against the identity
+  // and a symmetric rank-n product, about half the time of solving
+  // A Y = I with both factors) for a bandwidth-parallel GEMV inside the
+  // V-cycle
   Level &cl = c.lev[c.L - 1];
   const double *Sc = (c.L == 1) ? c.S0 : cl.S64;
   const int64_t nc = 3 * cl.nn;
@@ -485,13 +492,34 @@ int setup_hierarchy(Ctx &c, const tpo_solve_opts &o) {
     c.solver_work_n = lwork;
   }
   if (cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, (int)nc, c.Adense, (int)nc,
-                       c.solver_work, lwork, c.dev_info) != CUSOLVER_STATUS_SUCCESS ||
-      cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, (int)nc, (int)nc, c.Adense,
-                       (int)nc, c.Ainv, (int)nc, c.dev_info) != CUSOLVER_STATUS_SUCCESS) {
+                       c.solver_work, lwork, c.dev_info) != CUSOLVER_STATUS_SUCCESS) {
     c.err = "coarse Cholesky factorisation failed";
     join();
     return TPO_E_CUDA;
   }
+  cublasHandle_t hb = static_cast<cublasHandle_t>(c.cublas);
+  if (!hb) {
+    if (cublasCreate(&hb) != CUBLAS_STATUS_SUCCESS) {
+      c.err = "cublasCreate failed";
+      join();
+      return TPO_E_CUDA;
+    }
+    c.cublas = hb;
+  }
+  const double one = 1.0, zero = 0.0;
+  // Ainv <- L^-1 (Ainv holds the identity); Adense <- lower(X^T X)
+  if (cublasSetStream(hb, s) != CUBLAS_STATUS_SUCCESS ||
+      cublasSetPointerMode(hb, CUBLAS_POINTER_MODE_HOST) != CUBLAS_STATUS_SUCCESS ||
+      cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                  CUBLAS_DIAG_NON_UNIT, (int)nc, (int)nc, &one, c.Adense, (int)nc,
+                  c.Ainv, (int)nc) != CUBLAS_STATUS_SUCCESS ||
+      cublasDsyrk(hb, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, (int)nc, (int)nc, &one,
+                  c.Ainv, (int)nc, &zero, c.Adense, (int)nc) != CUBLAS_STATUS_SUCCESS) {
+    c.err = "coarse inverse from the Cholesky factor failed";
+    join();
+    return TPO_E_CUDA;
+  }
+  launch_sym_from_lower(nc, c.Adense, c.Ainv, s);
   int info_h = 0;
   CK(cudaMemcpyAsync(&info_h, c.dev_info, sizeof(int), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));

@@ -92,6 +92,9 @@ struct Level {
         *a32 = nullptr, *e32 = nullptr, *w32 = nullptr;
 };
 
+// side streams of the set-up (per-level power iterations)
+constexpr int kAuxStreams = 4;
+
 struct Ctx {
   tpo_mesh_params prm{};
   int nel[3] = {0, 0, 0};
@@ -105,11 +108,12 @@ struct Ctx {
   int device = 0;
   cudaStream_t stream = nullptr;      // stream all work is issued on
   cudaStream_t own_stream = nullptr;  // the context's own stream
-  // set-up side stream (Chebyshev bound estimates overlap the Galerkin
-  // chain) and its events
-  cudaStream_t aux_stream = nullptr;
+  // set-up side streams (the Chebyshev bound estimates of the levels
+  // overlap the Galerkin chain and one another; level l runs on side
+  // stream l % kAuxStreams) and their events
+  cudaStream_t aux_stream[kAuxStreams] = {};
   cudaEvent_t lev_ev[16] = {};
-  cudaEvent_t aux_ev = nullptr;
+  cudaEvent_t aux_ev[kAuxStreams] = {};
   std::string err;
 
   // element constants
@@ -232,9 +236,11 @@ constexpr int kSlotFault = 7;
 inline int red_grid(int nb) {
   return nb <= 1 ? kRedBlocks : (kRedBlocks / nb < 148 ? 148 : kRedBlocks / nb);
 }
-constexpr int kPartCount = 4096;   // >= kAuxPart + red_grid(1), and red_grid(nb) * nb <= kAuxPart
-// the set-up side stream's reductions use part + kAuxPart, ticket + kMaxBatch
+// reduction scratch: red_grid(nb) * nb <= kAuxPart partials on the main
+// stream; set-up side stream i uses part + kAuxPart + i * kRedBlocks and
+// ticket + kMaxBatch + i
 constexpr int kAuxPart = 2048;
+constexpr int kPartCount = kAuxPart + kAuxStreams * kRedBlocks;
 
 // fine matrix-free operator: y = M K M u + (1-M) u, or y = b - (that)
 template <typename T>
@@ -297,6 +303,8 @@ void launch_prolong_add(const Level &fine, const Level &coarse, const T *xc,
 void launch_to_dense(const Level &v, const double *S, double *A,
                      cudaStream_t s);
 void launch_eye(int64_t n, double *A, cudaStream_t s);
+// full symmetric matrix from the lower triangle of a column-major one
+void launch_sym_from_lower(int64_t n, const double *L, double *A, cudaStream_t s);
 // stencil SoA S[(nb*9 + 3r+s)*nn + n] -> node-major A[n*243 + (3r+s)*27 + nb]
 // (FP64 and an FP32 copy)
 void launch_soa_to_aos(int64_t nn, const double *S, double *A64, float *A32,
