@@ -44,7 +44,7 @@ extern "C" {
 #define TPO_MEM_DEVICE 1
 
 #define TPO_PREC_FP64 0     /* FP64 apply, smoother, transfers, CG */
-#define TPO_PREC_MIXED 1    /* FP32 inner PCG+GMG inside FP64 defect correction */
+#define TPO_PREC_MIXED 1    /* FP32 PCG+GMG with FP64 residual replacement */
 
 #define TPO_BC_SUPPORT 0
 #define TPO_BC_LOAD 1
@@ -68,10 +68,11 @@ typedef struct {
   double cheb_lo;     /* smoothing interval [lo, hi] * lambda_max(D^-1 A) */
   double cheb_hi;
   int32_t power_its;  /* power iterations for lambda_max at setup (15) */
-  double inner_rtol;  /* mixed form: floor of the relative drop asked of one
-                         FP32 inner solve (1e-5); each pass asks for the drop
-                         that reaches rtol with a 3x margin, if larger */
-  int32_t max_outer;  /* mixed form: defect-correction passes (10) */
+  double inner_rtol;  /* mixed form: relative drop of the FP32 residual
+                         between two FP64 residual replacements (1e-2); the
+                         last pass asks for 0.7 rtol instead when that is
+                         less of a drop */
+  int32_t max_outer;  /* mixed form: FP64 residual replacements (10) */
   int32_t use_graph;  /* capture the V-cycle/CG iteration in a CUDA graph */
   int32_t rhs_block;  /* tpo_solve: right-hand sides solved together as one
                          block (1, 2, 4 or 8); 0 = autotuned between 4 and 8
@@ -80,15 +81,15 @@ typedef struct {
 
 typedef struct {
   int32_t status;     /* as the return code */
-  int32_t iterations; /* CG iterations (sum over inner solves when mixed) */
-  int32_t outer;      /* defect-correction passes (1 in FP64 form) */
+  int32_t iterations; /* CG iterations (FP32 iterations when mixed) */
+  int32_t outer;      /* FP64 residual replacements (1 in FP64 form) */
   double relres;      /* final ||F - K U|| / ||F||, FP64 */
   double solve_ms;    /* host wall time of the solve phase */
   double setup_ms;    /* host wall time of the last FEAssemble/PCSetUp */
 } tpo_solve_info;
 
 /* fills the defaults used throughout (rtol 1e-8, maxit 500, FP64, Chebyshev
- * degree 2 on [0.1, 1.1] * lambda, 15 power iterations, inner_rtol 1e-5,
+ * degree 2 on [0.1, 1.1] * lambda, 15 power iterations, inner_rtol 1e-2,
  * max_outer 10, graphs on, autotuned right-hand-side blocks) */
 TPO_API void tpo_default_solve_opts(tpo_solve_opts *opts);
 

@@ -232,6 +232,15 @@ void free_all(Ctx &c) {
     if (q) cudaStreamDestroy(q);
     q = nullptr;
   }
+  if (c.setup_stream) {
+    cudaStreamSynchronize(c.setup_stream);
+    cudaStreamDestroy(c.setup_stream);
+  }
+  c.setup_stream = nullptr;
+  for (cudaEvent_t &e : c.setup_ev) {
+    if (e) cudaEventDestroy(e);
+    e = nullptr;
+  }
   if (c.own_stream) cudaStreamDestroy(c.own_stream);
   c.own_stream = c.stream = nullptr;
 }
@@ -275,7 +284,7 @@ void tpo_default_solve_opts(tpo_solve_opts *o) {
   o->cheb_lo = 0.1;
   o->cheb_hi = 1.1;
   o->power_its = 15;
-  o->inner_rtol = 1e-5;
+  o->inner_rtol = 1e-2;
   o->max_outer = 10;
   o->use_graph = 1;
   o->rhs_block = 0;
@@ -360,6 +369,16 @@ int tpo_create(const tpo_mesh_params *p, tpo_ctx **out) {
     delete ctx;
     return code;
   };
+  {
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&c.setup_stream, cudaStreamNonBlocking, greatest) !=
+            cudaSuccess)
+      return fail(TPO_E_CUDA);
+    for (cudaEvent_t &e : c.setup_ev)
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+        return fail(TPO_E_CUDA);
+  }
   for (int i = 0; i < tpo::kAuxStreams; ++i)
     if (cudaStreamCreateWithFlags(&c.aux_stream[i], cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c.aux_ev[i], cudaEventDisableTiming) != cudaSuccess)
@@ -384,8 +403,9 @@ int tpo_create(const tpo_mesh_params *p, tpo_ctx **out) {
   A(c.tmpe, c.ne); A(c.tmpe2, c.ne); A(c.dev_info, 1);
   A(c.io_a, nio); A(c.io_b, nio);
 #undef A
-  // scalar mirror plus a staging row for per-column uploads
-  if (cudaMallocHost(&c.scal_h, (tpo::kScalCount + tpo::kMaxBatch) * sizeof(double)) !=
+  // scalar mirror plus one staging row per column slot for per-column uploads
+  if (cudaMallocHost(&c.scal_h, (tpo::kScalCount + tpo::kColScal * tpo::kMaxBatch) *
+                                     sizeof(double)) !=
       cudaSuccess)
     return fail(TPO_E_CUDA);
   static constexpr int kLexToLocal[8] = {0, 1, 3, 2, 4, 5, 7, 6};

@@ -64,12 +64,15 @@ __device__ __forceinline__ void finish_reduction(double v, double *part,
   }
 }
 
-// a.b per column (blockIdx.y)
+// a.b per column (blockIdx.y); a column whose skip flag is set (every block
+// of it returns, so its ticket stays zero) keeps its out/shift_to slots
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads)
     k_dot(int64_t n, const T *__restrict__ a, const T *__restrict__ b,
-          double *part, unsigned int *ticket, double *out, double *shift_to) {
+          double *part, unsigned int *ticket, double *out, double *shift_to,
+          const double *skip) {
   const int j = blockIdx.y;
+  if (skip && skip[j * kColScal] != 0.0) return;
   a += j * n;
   b += j * n;
   double s = 0;
@@ -182,6 +185,16 @@ __global__ void k_axpy_f32(int64_t n, double *U, const float *d,
     U[i] += s * static_cast<double>(d[i]);
 }
 
+// v *= f per column, f in the column's scalar slot
+__global__ void k_scale_cols_f32(int64_t n, float *v, const double *scal) {
+  const int j = blockIdx.y;
+  const float f = static_cast<float>(scal[j * kColScal]);
+  v += j * n;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    v[i] *= f;
+}
+
 __global__ void k_d2f(int64_t n, const double *a, float *b) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
@@ -215,8 +228,21 @@ void launch_dot(const Ctx &c, int64_t n, const T *a, const T *b, double *out,
                 unsigned int *ticket) {
   count_launch();
   k_dot<T><<<dim3(red_grid(nb), nb), kRedThreads, 0, s>>>(
-      n, a, b, part ? part : c.part, ticket ? ticket : c.ticket, out, shift_to);
+      n, a, b, part ? part : c.part, ticket ? ticket : c.ticket, out, shift_to,
+      nullptr);
 }
+
+template <typename T>
+void launch_rho_dot(const Ctx &c, int64_t n, const T *r, const T *z, cudaStream_t s,
+                    int nb) {
+  count_launch();
+  k_dot<T><<<dim3(red_grid(nb), nb), kRedThreads, 0, s>>>(
+      n, r, z, c.part, c.ticket, c.scal + 0, c.scal + 1, c.scal + 6);
+}
+template void launch_rho_dot<double>(const Ctx &, int64_t, const double *,
+                                     const double *, cudaStream_t, int);
+template void launch_rho_dot<float>(const Ctx &, int64_t, const float *,
+                                    const float *, cudaStream_t, int);
 template void launch_dot<double>(const Ctx &, int64_t, const double *,
                                  const double *, double *, double *,
                                  cudaStream_t, int, double *, unsigned int *);
@@ -275,6 +301,12 @@ void launch_to_f32_scaled(int64_t n, const double *a, const double *scal,
                           float *b, cudaStream_t s, int nb) {
   count_launch();
   k_to_f32_scaled<<<col_grid(n, nb), 256, 0, s>>>(n, a, scal, b);
+}
+
+void launch_scale_cols_f32(int64_t n, float *v, const double *scal, cudaStream_t s,
+                           int nb) {
+  count_launch();
+  k_scale_cols_f32<<<col_grid(n, nb), 256, 0, s>>>(n, v, scal);
 }
 
 void launch_axpy_f32(int64_t n, double *U, const float *d, const double *scal,

@@ -1,5 +1,5 @@
 // Host orchestration of the FE solve: GMG set-up (PCSetUp), the V-cycle,
-// FP64 PCG and the mixed FP32/FP64 defect-correction solve.
+// FP64 PCG and the mixed FP32 PCG with FP64 residual replacement.
 //
 // Reference behaviour restated here (FEAnalysis.cpp:387-416, :541-573,
 // :673): KSP CG, nonzero initial guess, convergence on the unpreconditioned
@@ -222,7 +222,7 @@ void cg_body(Ctx &c, int64_t n, T *x, T *r, T *z, T *p, T *q,
              const tpo_solve_opts &o, bool first, cudaStream_t s, int nb) {
   double *sc = c.scal;
   vcycle_rec<T>(c, 0, r, z, o, s, nb);
-  launch_dot<T>(c, n, r, z, sc + 0, sc + 1, s, nb);
+  launch_rho_dot<T>(c, n, r, z, s, nb);
   launch_cg_p<T>(n, z, p, sc, first, s, nb);
   launch_apply_fine<T>(c, fineE(c, (T *)nullptr), p, nullptr, q, s, nb);
   launch_dot<T>(c, n, p, q, sc + 2, nullptr, s, nb);
@@ -255,10 +255,13 @@ int readback(Ctx &c, int nb) {
   return TPO_OK;
 }
 
-// device scalar slot `slot` of nb columns <- host values (through pinned
-// staging after the column block of scal_h)
+// device scalar slot `slot` of nb columns <- host values, through a pinned
+// staging row of its own after the scalar mirror: the copy is asynchronous,
+// so uploads of different slots may follow one another without a
+// synchronisation, but a slot must not be uploaded twice before the stream
+// has passed the first copy
 int upload_slot(Ctx &c, int slot, const double *v, int nb) {
-  double *st = c.scal_h + kScalCount;
+  double *st = c.scal_h + kScalCount + slot * kMaxBatch;
   for (int j = 0; j < nb; ++j) st[j] = v[j];
   CK(cudaMemcpy2DAsync(c.scal + slot, sizeof(double) * kColScal, st,
                        sizeof(double), sizeof(double), nb,
@@ -278,11 +281,13 @@ int copy_slot(Ctx &c, int dst, int src, int nb) {
 // initial guesses and r must already hold b - K x; ||r_j||^2 is in slot 3
 // of the host mirror.  Column j stops at ||r_j||^2 <= target_rr[j]; columns
 // with frozen[j] set do not iterate.  On return its[j] = iterations of
-// column j and st[j] = its status.
+// column j and st[j] = its status.  resume: continue the previous run's
+// recurrence (the first iteration forms p = z + beta p from the p and rho
+// left in place) instead of starting with p = z.
 template <typename T>
 int pcg_loop(Ctx &c, const tpo_solve_opts &o, T *x, T *r, T *z, T *p, T *q,
              const double *target_rr, int maxit, int nb, double *frozen,
-             int *its, int *st) {
+             int *its, int *st, bool resume = false) {
   cudaStream_t s = c.stream;
   const int64_t n = 3 * c.nn;
   cudaGraphExec_t &g = (sizeof(T) == 8) ? c.graph64 : c.graph32;
@@ -304,7 +309,7 @@ int pcg_loop(Ctx &c, const tpo_solve_opts &o, T *x, T *r, T *z, T *p, T *q,
   if (int rc = upload_slot(c, 6, frozen, nb)) return rc;
   int k = 0;
   while (k < maxit && active) {
-    const bool first = (k == 0);
+    const bool first = (k == 0) && !resume;
     if (!first && o.use_graph) {
       if (!g || gx != (const void *)x || gnb != nb) {
         if (g) {
@@ -402,9 +407,11 @@ int estimate_lambda(Ctx &c, int l, int its, double *lam) {
   return TPO_OK;
 }
 
-int setup_hierarchy(Ctx &c, const tpo_solve_opts &o) {
+namespace {
+
+// the hierarchy on stream s (see setup_hierarchy)
+int setup_on(Ctx &c, const tpo_solve_opts &o, cudaStream_t s) {
   const double t0 = now_ms();
-  cudaStream_t s = c.stream;
   invalidate_graphs(c);
   // Chebyshev bounds (power iterations) of each smoothed level run on a
   // side stream as soon as that level's operator is built on s, with their
@@ -541,6 +548,21 @@ int setup_hierarchy(Ctx &c, const tpo_solve_opts &o) {
   return TPO_OK;
 }
 
+}  // namespace
+
+// FEAssemble/PCSetUp: the Galerkin hierarchy, the coarsest inverse and the
+// Chebyshev bounds.  The work runs on the context's highest-priority set-up
+// stream, ordered after everything already issued on c.stream, and c.stream
+// waits for it on every return path.
+int setup_hierarchy(Ctx &c, const tpo_solve_opts &o) {
+  CK(cudaEventRecord(c.setup_ev[0], c.stream));
+  CK(cudaStreamWaitEvent(c.setup_stream, c.setup_ev[0], 0));
+  const int rc = setup_on(c, o, c.setup_stream);
+  CK(cudaEventRecord(c.setup_ev[1], c.setup_stream));
+  CK(cudaStreamWaitEvent(c.stream, c.setup_ev[1], 0));
+  return rc;
+}
+
 int vcycle_apply(Ctx &c, const tpo_solve_opts &o, int precision,
                  const double *r, double *z) {
   cudaStream_t s = c.stream;
@@ -653,57 +675,92 @@ int solve(Ctx &c, const tpo_solve_opts &o, const double *b, double *x,
       rn[j] = std::sqrt(c.scal_h[j * kColScal + 5]);
     }
   } else if (active) {
-    // mixed: FP32 PCG+GMG on K d_j = r_j/||r_j|| inside FP64 defect
-    // correction, all columns of the block together
-    int round = 0;
-    while (round < o.max_outer) {
-      double tgt_in[kMaxBatch];
-      double inner_frozen[kMaxBatch];
-      int live = 0;
+    // mixed: ONE FP32 PCG+GMG recurrence on K d_j = r_j/||r_j|| with FP64
+    // residual replacement (the "reliable updates" of Sleijpen & van der
+    // Vorst, 1996; residual replacement, van der Vorst & Ye, 2000).  When
+    // every live column's FP32 residual has dropped by inner_rtol, or to
+    // 0.7x what its target asks, x += ||r|| d in FP64, the FP64 residual
+    // b - K x replaces the FP32 one (rescaled to unit norm), and the FP32
+    // recurrence resumes with its search direction and rho rescaled by the
+    // same factor.  Restarting from p = z instead (plain defect correction)
+    // would throw away the Krylov space and cost 1-2 iterations per pass.
+    // Convergence is only ever decided on the FP64 residual.  Passes are
+    // kept short (inner_rtol 1e-2 by default): over a long FP32 pass the
+    // recursive residual drifts from the true one (K p cancels heavily in
+    // FP32 for smooth p), and the old search direction then no longer fits
+    // the replaced residual.  If the FP64 residual comes out more than 2x
+    // above what the FP32 recurrence predicted, the next pass restarts from
+    // p = z instead of resuming.
+    launch_to_f32_scaled(n, c.r64, sc + 5, c.r32, s, nb);
+    CK(cudaMemsetAsync(c.x32, 0, sizeof(float) * n * nb, s));
+    launch_dot<float>(c, n, c.r32, c.r32, sc + 3, nullptr, s, nb);
+    if (int rc = readback(c, nb)) return rc;
+    bool resume = false;
+    int passes = 0;
+    while (passes < o.max_outer) {
+      double trig[kMaxBatch], inner_frozen[kMaxBatch];
+      bool live[kMaxBatch];
+      int nlive = 0, maxit_in = 0;
       for (int j = 0; j < nb; ++j) {
-        const bool done = status[j] == TPO_OK || status[j] == TPO_E_BREAKDOWN ||
-                          rn[j] <= target[j] || its_total[j] >= o.maxit;
-        inner_frozen[j] = done ? 1.0 : 0.0;
-        if (!done) ++live;
+        live[j] = !(status[j] == TPO_OK || status[j] == TPO_E_BREAKDOWN ||
+                    rn[j] <= target[j] || its_total[j] >= o.maxit);
+        inner_frozen[j] = live[j] ? 0.0 : 1.0;
+        trig[j] = 0.0;
+        if (!live[j]) continue;
+        ++nlive;
+        const double eta = std::max(o.inner_rtol, 0.7 * target[j] / std::max(rn[j], 1e-300));
+        trig[j] = eta * eta * c.scal_h[j * kColScal + 3];
+        maxit_in = std::max(maxit_in, o.maxit - its_total[j]);
       }
-      if (!live) break;
-      launch_to_f32_scaled(n, c.r64, sc + 5, c.r32, s, nb);
-      CK(cudaMemsetAsync(c.x32, 0, sizeof(float) * n * nb, s));
-      launch_dot<float>(c, n, c.r32, c.r32, sc + 3, nullptr, s, nb);
-      if (int rc = readback(c, nb)) return rc;
-      int maxit_in = 0;
-      for (int j = 0; j < nb; ++j) {
-        // ask the FP32 solve for the reduction that reaches the target with
-        // a 3x margin, but never below the FP32-attainable floor inner_rtol
-        const double eta = std::max(o.inner_rtol, 0.3 * target[j] / std::max(rn[j], 1e-300));
-        tgt_in[j] = eta * eta * c.scal_h[j * kColScal + 3];
-        if (inner_frozen[j] == 0.0) maxit_in = std::max(maxit_in, o.maxit - its_total[j]);
-      }
-      pcg_loop<float>(c, o, c.x32, c.r32, c.z32, c.p32, c.q32, tgt_in, maxit_in,
-                      nb, inner_frozen, its, st);
-      ++round;
-      // columns that were done before this round get a zero correction
-      // (their x32 stays zero)
+      if (!nlive) break;
+      pcg_loop<float>(c, o, c.x32, c.r32, c.z32, c.p32, c.q32, trig, maxit_in, nb,
+                      inner_frozen, its, st, resume);
+      ++passes;
+      double predicted[kMaxBatch];   // ||r|| the FP32 recurrence ended at
+      for (int j = 0; j < nb; ++j)
+        predicted[j] = rn[j] * std::sqrt(std::max(c.scal_h[j * kColScal + 3], 0.0));
+      // FP64 residual replacement (columns that were done before this pass
+      // have a zero x32 and keep their x)
       launch_axpy_f32(n, x, c.x32, sc + 5, s, nb);
+      CK(cudaMemsetAsync(c.x32, 0, sizeof(float) * n * nb, s));
       launch_apply_fine<double>(c, c.E64, x, b, c.r64, s, nb);
       launch_dot<double>(c, n, c.r64, c.r64, sc + 5, nullptr, s, nb);
+      launch_to_f32_scaled(n, c.r64, sc + 5, c.r32, s, nb);
+      launch_dot<float>(c, n, c.r32, c.r32, sc + 3, nullptr, s, nb);
       if (int rc = readback(c, nb)) return rc;
+      double f[kMaxBatch], rho[kMaxBatch];
+      bool restart = false;
       for (int j = 0; j < nb; ++j) {
         const double rn_new = std::sqrt(c.scal_h[j * kColScal + 5]);
-        const bool was_live = !(status[j] == TPO_OK || status[j] == TPO_E_BREAKDOWN ||
-                                rn[j] <= target[j] || its_total[j] >= o.maxit);
-        if (!was_live) {
+        f[j] = 1.0;
+        rho[j] = c.scal_h[j * kColScal + 0];
+        if (!live[j]) {
           rn[j] = rn_new;
           continue;
         }
         its_total[j] += its[j];
         ++outer[j];
-        if (st[j] == TPO_E_BREAKDOWN && !(rn_new < rn[j])) status[j] = TPO_E_BREAKDOWN;
-        rn[j] = rn_new;
         if (!std::isfinite(rn_new)) {
           status[j] = TPO_E_BREAKDOWN;
-          c.err = "non-finite residual in defect correction";
+          c.err = "non-finite residual in the mixed-precision solve";
+        } else if (st[j] == TPO_E_BREAKDOWN) {
+          // the FP32 recurrence broke down: fatal unless it still made
+          // progress, in which case the next pass restarts from p = z
+          if (!(rn_new < rn[j])) status[j] = TPO_E_BREAKDOWN;
+          restart = true;
+        } else if (rn_new > target[j]) {
+          f[j] = rn[j] / rn_new;
+          rho[j] *= f[j] * f[j];
+          if (rn_new > 2.0 * predicted[j]) restart = true;
         }
+        rn[j] = rn_new;
+      }
+      resume = !restart;
+      if (resume) {
+        // p and rho into the units of the new unit-norm residual
+        if (int rc = upload_slot(c, 2, f, nb)) return rc;
+        if (int rc = upload_slot(c, 0, rho, nb)) return rc;
+        launch_scale_cols_f32(n, c.p32, sc + 2, s, nb);
       }
     }
     for (int j = 0; j < nb; ++j)

@@ -114,6 +114,11 @@ struct Ctx {
   cudaStream_t aux_stream[kAuxStreams] = {};
   cudaEvent_t lev_ev[16] = {};
   cudaEvent_t aux_ev[kAuxStreams] = {};
+  // the set-up's critical chain (Galerkin products, coarse factorisation
+  // and inverse) runs on a highest-priority stream forked from `stream`, so
+  // the side streams' power iterations fill in around it
+  cudaStream_t setup_stream = nullptr;
+  cudaEvent_t setup_ev[2] = {};
   std::string err;
 
   // element constants
@@ -331,6 +336,12 @@ template <typename T>
 void launch_dot(const Ctx &c, int64_t n, const T *a, const T *b, double *out,
                 double *shift_to, cudaStream_t s, int nb = 1,
                 double *part = nullptr, unsigned int *ticket = nullptr);
+// CG rho = r.z per column into slot 0, the previous rho into slot 1; a
+// frozen column (slot 6 set) keeps both, so a resumed recurrence finds the
+// rho of its last active iteration
+template <typename T>
+void launch_rho_dot(const Ctx &c, int64_t n, const T *r, const T *z, cudaStream_t s,
+                    int nb);
 template <typename T>
 void launch_cg_p(int64_t n, const T *z, T *p, const double *scal, bool first,
                  cudaStream_t s, int nb = 1);
@@ -346,6 +357,9 @@ void launch_scale_diag(int64_t n, double *w, const double *dinv,
                        cudaStream_t s);
 void launch_to_f32_scaled(int64_t n, const double *a, const double *scal,
                           float *b, cudaStream_t s, int nb = 1);
+// v_j *= scal[j * kColScal] per column (scal points at the factor's slot)
+void launch_scale_cols_f32(int64_t n, float *v, const double *scal, cudaStream_t s,
+                           int nb);
 void launch_axpy_f32(int64_t n, double *U, const float *d, const double *scal,
                      cudaStream_t s, int nb = 1);
 void launch_d2f(int64_t n, const double *a, float *b, cudaStream_t s);
