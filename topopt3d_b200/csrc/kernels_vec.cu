@@ -185,16 +185,6 @@ __global__ void k_axpy_f32(int64_t n, double *U, const float *d,
     U[i] += s * static_cast<double>(d[i]);
 }
 
-// v *= f per column, f in the column's scalar slot
-__global__ void k_scale_cols_f32(int64_t n, float *v, const double *scal) {
-  const int j = blockIdx.y;
-  const float f = static_cast<float>(scal[j * kColScal]);
-  v += j * n;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    v[i] *= f;
-}
-
 __global__ void k_d2f(int64_t n, const double *a, float *b) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
@@ -301,12 +291,6 @@ void launch_to_f32_scaled(int64_t n, const double *a, const double *scal,
                           float *b, cudaStream_t s, int nb) {
   count_launch();
   k_to_f32_scaled<<<col_grid(n, nb), 256, 0, s>>>(n, a, scal, b);
-}
-
-void launch_scale_cols_f32(int64_t n, float *v, const double *scal, cudaStream_t s,
-                           int nb) {
-  count_launch();
-  k_scale_cols_f32<<<col_grid(n, nb), 256, 0, s>>>(n, v, scal);
 }
 
 void launch_axpy_f32(int64_t n, double *U, const float *d, const double *scal,

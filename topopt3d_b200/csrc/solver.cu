@@ -681,8 +681,8 @@ int solve(Ctx &c, const tpo_solve_opts &o, const double *b, double *x,
     // every live column's FP32 residual has dropped by inner_rtol, or to
     // 0.7x what its target asks, x += ||r|| d in FP64, the FP64 residual
     // b - K x replaces the FP32 one (rescaled to unit norm), and the FP32
-    // recurrence resumes with its search direction and rho rescaled by the
-    // same factor.  Restarting from p = z instead (plain defect correction)
+    // recurrence resumes with its search direction and rho rescaled to the
+    // new units.  Restarting from p = z instead (plain defect correction)
     // would throw away the Krylov space and cost 1-2 iterations per pass.
     // Convergence is only ever decided on the FP64 residual.  Passes are
     // kept short (inner_rtol 1e-2 by default): over a long FP32 pass the
@@ -691,10 +691,11 @@ int solve(Ctx &c, const tpo_solve_opts &o, const double *b, double *x,
     // the replaced residual.  If the FP64 residual comes out more than 2x
     // above what the FP32 recurrence predicted, the next pass restarts from
     // p = z instead of resuming.
+    // the FP32 residual r/||r|| has unit norm to FP32 rounding, so its
+    // squared norm (the base of each pass's drop) is taken as 1 on the host
     launch_to_f32_scaled(n, c.r64, sc + 5, c.r32, s, nb);
     CK(cudaMemsetAsync(c.x32, 0, sizeof(float) * n * nb, s));
-    launch_dot<float>(c, n, c.r32, c.r32, sc + 3, nullptr, s, nb);
-    if (int rc = readback(c, nb)) return rc;
+    for (int j = 0; j < nb; ++j) c.scal_h[j * kColScal + 3] = rn[j] > 0.0 ? 1.0 : 0.0;
     bool resume = false;
     int passes = 0;
     while (passes < o.max_outer) {
@@ -726,7 +727,6 @@ int solve(Ctx &c, const tpo_solve_opts &o, const double *b, double *x,
       launch_apply_fine<double>(c, c.E64, x, b, c.r64, s, nb);
       launch_dot<double>(c, n, c.r64, c.r64, sc + 5, nullptr, s, nb);
       launch_to_f32_scaled(n, c.r64, sc + 5, c.r32, s, nb);
-      launch_dot<float>(c, n, c.r32, c.r32, sc + 3, nullptr, s, nb);
       if (int rc = readback(c, nb)) return rc;
       double f[kMaxBatch], rho[kMaxBatch];
       bool restart = false;
@@ -750,18 +750,19 @@ int solve(Ctx &c, const tpo_solve_opts &o, const double *b, double *x,
           restart = true;
         } else if (rn_new > target[j]) {
           f[j] = rn[j] / rn_new;
-          rho[j] *= f[j] * f[j];
+          // p and rho in the units of the new residual are f p and f^2 rho.
+          // p is only read by the next p = z + (rho_new / rho) p, so f p
+          // comes from storing f rho instead: (rho_new / (f rho)) p =
+          // (rho_new / (f^2 rho)) (f p)
+          rho[j] *= f[j];
           if (rn_new > 2.0 * predicted[j]) restart = true;
         }
         rn[j] = rn_new;
+        c.scal_h[j * kColScal + 3] = rn_new > 0.0 ? 1.0 : 0.0;
       }
       resume = !restart;
-      if (resume) {
-        // p and rho into the units of the new unit-norm residual
-        if (int rc = upload_slot(c, 2, f, nb)) return rc;
+      if (resume)
         if (int rc = upload_slot(c, 0, rho, nb)) return rc;
-        launch_scale_cols_f32(n, c.p32, sc + 2, s, nb);
-      }
     }
     for (int j = 0; j < nb; ++j)
       if (status[j] != TPO_E_BREAKDOWN) status[j] = rn[j] <= target[j] ? TPO_OK : TPO_NOT_CONVERGED;

@@ -357,9 +357,6 @@ void launch_scale_diag(int64_t n, double *w, const double *dinv,
                        cudaStream_t s);
 void launch_to_f32_scaled(int64_t n, const double *a, const double *scal,
                           float *b, cudaStream_t s, int nb = 1);
-// v_j *= scal[j * kColScal] per column (scal points at the factor's slot)
-void launch_scale_cols_f32(int64_t n, float *v, const double *scal, cudaStream_t s,
-                           int nb);
 void launch_axpy_f32(int64_t n, double *U, const float *d, const double *scal,
                      cudaStream_t s, int nb = 1);
 void launch_d2f(int64_t n, const double *a, float *b, cudaStream_t s);
