@@ -332,6 +332,10 @@ int tpo_create(const tpo_mesh_params *p, tpo_ctx **out) {
     }
   }
   c.L = (int)c.lev.size();
+  if (c.L > tpo::kMaxLevels) {
+    delete ctx;
+    return TPO_E_UNSUPPORTED;
+  }
   // the small levels and the dense coarsest solve run in one persistent
   // kernel: from the first level (>= 1) with at most kPersistentMaxNodes
   c.ps = c.L - 1;

@@ -145,19 +145,18 @@ __global__ void k_power_start(int64_t n, double *a) {
     a[i] = start_value((uint64_t)i);
 }
 
-// a = w / sqrt(nrm2)   (w may alias a)
-__global__ void k_power_normalize(int64_t n, double *a, const double *w,
-                                  const double *nrm2) {
-  const double s = sqrt(*nrm2);
+__global__ void __launch_bounds__(kRedThreads)
+    k_scale_diag_dot(int64_t n, double *__restrict__ w, const double *__restrict__ dinv,
+                     double *part, unsigned int *ticket, double *out,
+                     double *shift_to) {
+  double s = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    a[i] = w[i] / s;
-}
-
-__global__ void k_scale_diag(int64_t n, double *w, const double *dinv) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    w[i] *= dinv[i];
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double wi = w[i] * dinv[i];
+    w[i] = wi;
+    s += wi * wi;
+  }
+  finish_reduction(s, part, ticket, out, shift_to);
 }
 
 // b = float(a / sqrt(*nrm2)) per column (a zero column stays zero)
@@ -273,18 +272,12 @@ void launch_power_start(int64_t n, double *a, cudaStream_t s) {
   k_power_start<<<grid_for(n, 256), 256, 0, s>>>(n, a);
 }
 
-void launch_power_normalize(int64_t n, double *a, const double *w,
-                            const double *dinv, const double *nrm2,
-                            cudaStream_t s) {
+void launch_scale_diag_dot(const Ctx &c, int64_t n, double *w, const double *dinv,
+                           double *out, double *shift_to, cudaStream_t s,
+                           double *part, unsigned int *ticket) {
   count_launch();
-  (void)dinv;
-  k_power_normalize<<<grid_for(n, 256), 256, 0, s>>>(n, a, w, nrm2);
-}
-
-void launch_scale_diag(int64_t n, double *w, const double *dinv,
-                       cudaStream_t s) {
-  count_launch();
-  k_scale_diag<<<grid_for(n, 256), 256, 0, s>>>(n, w, dinv);
+  k_scale_diag_dot<<<red_grid(1), kRedThreads, 0, s>>>(
+      n, w, dinv, part ? part : c.part, ticket ? ticket : c.ticket, out, shift_to);
 }
 
 void launch_to_f32_scaled(int64_t n, const double *a, const double *scal,

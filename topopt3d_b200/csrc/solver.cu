@@ -376,34 +376,44 @@ void invalidate_graphs(Ctx &c) {
   c.graph64_nb = c.graph32_nb = 0;
 }
 
-// power iteration for lambda_max(D^-1 A_l) on stream s, no host sync: the
-// squared norm of the last iterate ends in scal[SC_POWER + l].  The start
-// vector is the splitmix64 sequence the oracle shares.
+// power iteration for lambda_max(D^-1 A_l) on stream s, no host sync.  The
+// start vector is the splitmix64 sequence the oracle shares.  The iterates
+// v_{k+1} = D^-1 A v_k are not normalised (lambda_max(D^-1 A) is a small
+// number, so 15 steps stay far inside the FP64 range): each step is the
+// apply and one fused pass for the diagonal scaling and the squared norm,
+// which leaves ||v_k||^2 in scal[SC_POWER + l] and ||v_{k-1}||^2 in
+// scal[SC_POWER_PREV + l].  lambda = ||v_k|| / ||v_{k-1}|| is then the
+// estimate ||D^-1 A a|| of the normalised iteration, a = v_{k-1}/||v_{k-1}||.
 void power_iteration(Ctx &c, int l, int its, cudaStream_t s, double *part,
                      unsigned int *ticket) {
   Level &v = c.lev[l];
   const int64_t n = 3 * v.nn;
   double *a = v.d64, *w = v.a64;
-  double *nrm = c.scal + SC_POWER + l;
+  double *nrm = c.scal + SC_POWER + l, *prev = c.scal + SC_POWER_PREV + l;
   launch_power_start(n, a, s);
   launch_dot<double>(c, n, a, a, nrm, nullptr, s, 1, part, ticket);
-  launch_power_normalize(n, a, a, nullptr, nrm, s);
   for (int k = 0; k < its; ++k) {
     level_apply<double>(c, l, a, nullptr, w, s);
-    launch_scale_diag(n, w, v.dinv64, s);
-    launch_dot<double>(c, n, w, w, nrm, nullptr, s, 1, part, ticket);
-    launch_power_normalize(n, a, w, nullptr, nrm, s);
+    launch_scale_diag_dot(c, n, w, v.dinv64, nrm, prev, s, part, ticket);
+    std::swap(a, w);
   }
+}
+
+// lambda of level l from the power iteration's two last squared norms in
+// the host mirror
+double power_lambda(const Ctx &c, int l) {
+  return std::sqrt(c.scal_h[SC_POWER + l] / c.scal_h[SC_POWER_PREV + l]);
 }
 
 int estimate_lambda(Ctx &c, int l, int its, double *lam) {
   cudaStream_t s = c.stream;
   power_iteration(c, l, its, s, nullptr, nullptr);
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(c.scal_h + SC_POWER + l, c.scal + SC_POWER + l, sizeof(double),
+  CK(cudaMemcpyAsync(c.scal_h + SC_POWER, c.scal + SC_POWER,
+                     sizeof(double) * (SC_POWER_PREV + kMaxLevels - SC_POWER),
                      cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
-  *lam = std::sqrt(c.scal_h[SC_POWER + l]);
+  *lam = power_lambda(c, l);
   return TPO_OK;
 }
 
@@ -538,10 +548,11 @@ int setup_on(Ctx &c, const tpo_solve_opts &o, cudaStream_t s) {
   }
   // Chebyshev bounds from the side stream
   join();
-  CK(cudaMemcpyAsync(c.scal_h + SC_POWER, c.scal + SC_POWER, sizeof(double) * c.L,
+  CK(cudaMemcpyAsync(c.scal_h + SC_POWER, c.scal + SC_POWER,
+                     sizeof(double) * (SC_POWER_PREV + kMaxLevels - SC_POWER),
                      cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
-  for (int l = 0; l + 1 < c.L; ++l) c.lev[l].lam = std::sqrt(c.scal_h[SC_POWER + l]);
+  for (int l = 0; l + 1 < c.L; ++l) c.lev[l].lam = power_lambda(c, l);
   c.setup_opts = o;
   c.assembled = true;
   c.setup_ms = now_ms() - t0;

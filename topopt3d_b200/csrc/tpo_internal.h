@@ -94,6 +94,8 @@ struct Level {
 
 // side streams of the set-up (per-level power iterations)
 constexpr int kAuxStreams = 4;
+// GMG levels of one context
+constexpr int kMaxLevels = 16;
 
 struct Ctx {
   tpo_mesh_params prm{};
@@ -112,7 +114,7 @@ struct Ctx {
   // overlap the Galerkin chain and one another; level l runs on side
   // stream l % kAuxStreams) and their events
   cudaStream_t aux_stream[kAuxStreams] = {};
-  cudaEvent_t lev_ev[16] = {};
+  cudaEvent_t lev_ev[kMaxLevels] = {};
   cudaEvent_t aux_ev[kAuxStreams] = {};
   // the set-up's critical chain (Galerkin products, coarse factorisation
   // and inverse) runs on a highest-priority stream forked from `stream`, so
@@ -229,12 +231,15 @@ constexpr int kRedBlocks = 592;   // 4 x 148 SMs: fixed grid for reductions
 //   column has converged and its CG updates are skipped), 7 (column 0
 //   only) fault flag of the persistent coarse-grid kernel: non-zero when a
 //   grid-barrier wait ran out (read with the other scalars by readback).
-// Scalars of the design-side calls follow the column block at kScalMisc.
+// Scalars of the design-side calls follow the column block at kScalMisc;
+// the power iteration of level l leaves its last two squared norms in
+// SC_POWER + l and SC_POWER_PREV + l.
 constexpr int kMaxBatch = 8;
 constexpr int kColScal = 8;
 constexpr int kScalMisc = kMaxBatch * kColScal;   // 64
-constexpr int kScalCount = kScalMisc + 16;
 enum { SC_COMPLIANCE = kScalMisc, SC_VOLUME, SC_OC_DG, SC_OC_CHANGE, SC_POWER };
+constexpr int SC_POWER_PREV = SC_POWER + kMaxLevels;
+constexpr int kScalCount = SC_POWER_PREV + kMaxLevels;
 constexpr int kSlotFault = 7;
 
 // fixed reduction grid (blocks per column) for a block of nb columns
@@ -349,12 +354,12 @@ template <typename T>
 void launch_cg_update(const Ctx &c, int64_t n, T *x, T *r, const T *p,
                       const T *q, const double *scal, double *rr,
                       cudaStream_t s, int nb = 1);
-void launch_power_normalize(int64_t n, double *a, const double *w,
-                            const double *dinv, const double *nrm2,
-                            cudaStream_t s);
 void launch_power_start(int64_t n, double *a, cudaStream_t s);
-void launch_scale_diag(int64_t n, double *w, const double *dinv,
-                       cudaStream_t s);
+// w *= dinv and its squared norm into *out (the previous *out into
+// *shift_to), one pass; reduction scratch as launch_dot's
+void launch_scale_diag_dot(const Ctx &c, int64_t n, double *w, const double *dinv,
+                           double *out, double *shift_to, cudaStream_t s,
+                           double *part, unsigned int *ticket);
 void launch_to_f32_scaled(int64_t n, const double *a, const double *scal,
                           float *b, cudaStream_t s, int nb = 1);
 void launch_axpy_f32(int64_t n, double *U, const float *d, const double *scal,
