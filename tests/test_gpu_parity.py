@@ -149,6 +149,40 @@ def test_cfg0_solve_compliance_sensitivity(T, oracle, prec):
         assert abs(info["iterations"] - its_o) <= 2
 
 
+@pytest.mark.parametrize("inner_rtol", [0.1, 1e-2, 1e-5])
+def test_mixed_residual_replacement(T, oracle, inner_rtol):
+    """The mixed solve on a high-contrast design (30% of the elements near
+    void): short FP32 passes (0.1: many FP64 residual replacements), the
+    default (1e-2), and long passes (1e-5), where the FP32 recurrence
+    drifts from the true residual and the next pass must restart instead of
+    resuming.  Every form converges in FP64 to rtol and matches the
+    oracle's solution; a three-column block converges per column."""
+    nel = P.CONFIGS["cfg0"]["nel"]
+    rng = np.random.default_rng(31)
+    x = rng.uniform(0.2, 1.0, int(np.prod(nel)))
+    x[rng.random(x.size) < 0.3] = 1e-3
+    t, ref = pair(T, oracle, nel, levels=3, spec=P.bcs("cfg0"), x=x)
+    Uo, st, its_o, _ = ref.solve()
+    assert st == 0
+    info = t.FESolve(T.default_opts(precision=T.PREC_MIXED, inner_rtol=inner_rtol,
+                                    max_outer=30))
+    assert info["status"] == 0 and info["relres"] <= 1e-8
+    assert info["outer"] >= 2
+    assert np.linalg.norm(t.U - Uo) / np.linalg.norm(Uo) < 1e-6
+    if inner_rtol == 1e-2:
+        assert info["iterations"] <= its_o + 2
+    F = P.point_loads(nel, 3, seed=5)
+    U = np.zeros_like(F)
+    info = t.solve(np.ascontiguousarray(F), U, nrhs=3,
+                   opts=T.default_opts(precision=T.PREC_MIXED, inner_rtol=inner_rtol,
+                                       max_outer=30, rhs_block=4))
+    assert info["status"] == 0 and info["relres"] <= 1e-8
+    for j in range(3):
+        Uj, st, _, _ = ref.solve(b=F[j])
+        assert st == 0
+        assert np.linalg.norm(U[j] - Uj) / np.linalg.norm(Uj) < 1e-6
+
+
 def test_odd_mesh_solve(T, oracle):
     nel = (7, 5, 3)
     t, ref = pair(T, oracle, nel, levels=2, seed=9)
