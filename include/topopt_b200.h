@@ -211,6 +211,20 @@ TPO_API int tpo_ks_apply(tpo_ctx *ctx, const double *u, double *y, int32_t nrhs,
  * tpo_ks_assemble. */
 TPO_API int tpo_buckling(tpo_ctx *ctx, const tpo_eig_opts *opts, double *lambda,
                  double *phi, int mem, tpo_eig_info *info);
+/* The gradient of Stability::Function (Buckling.cpp:87-88, 113-272) with
+ * TopOpt::Chain_Filter (Material_Interpolation.cpp:150-187): value = (sum
+ * lambda_i^p)^(1/p) over nev <= 32 eigenpairs (lambda on the host; phi
+ * 3*nNode x nev column-major and K-normalised, in `mem`, as tpo_buckling
+ * returns them) and its gradient dvdx (nElem, in `mem`) with respect to the
+ * design x; dvdrho (optional) is the gradient with respect to the filtered
+ * density before the filter chain rule.  The nev adjoint systems
+ * K v_i = d(phi_i^T Ks phi_i)/dU (:155-225) are solved as blocks of
+ * right-hand sides with opts (NULL = defaults); info (optional) aggregates
+ * them.  Needs tpo_fe_assemble, and tpo_ks_assemble from the current U. */
+TPO_API int tpo_buckling_sensitivity(tpo_ctx *ctx, int32_t nev, const double *lambda,
+                             const double *phi, double p, const tpo_solve_opts *opts,
+                             double *value, double *dvdx, double *dvdrho, int mem,
+                             tpo_solve_info *info);
 
 /* U, F, x, rho, E, dEdz accessors: which = "U","F","x","rho","E","dEdz" */
 TPO_API int tpo_get_vector(const tpo_ctx *ctx, const char *which, double *out, int mem);

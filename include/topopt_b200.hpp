@@ -21,6 +21,7 @@
 #define TOPOPT_B200_HPP
 
 #include <array>
+#include <cmath>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -94,6 +95,20 @@ class TopOpt {
     lambda.assign(eig.nev, 0.0);
     const int rc = tpo_buckling(ctx_, &eig, lambda.data(), nullptr, TPO_MEM_HOST,
                                 &eig_info);
+    return rc < 0 ? rc : 0;
+  }
+  // Stability::Function with its gradient (Buckling.cpp:15-272): the
+  // eigenpairs, value = (sum lambda^p)^(1/p) and dvalue/dx through one
+  // adjoint solve per eigenpair (solved with `opts`)
+  int BucklingGradient(std::vector<double> &lambda, double p, double *value,
+                       std::vector<double> &dvdx) {
+    lambda.assign(eig.nev, 0.0);
+    std::vector<double> phi((size_t)eig.nev * 3 * nNode);
+    int rc = tpo_buckling(ctx_, &eig, lambda.data(), phi.data(), TPO_MEM_HOST, &eig_info);
+    if (rc < 0) return rc;
+    dvdx.assign(nElem, 0.0);
+    rc = tpo_buckling_sensitivity(ctx_, eig.nev, lambda.data(), phi.data(), p, &opts, value,
+                                  dvdx.data(), nullptr, TPO_MEM_HOST, nullptr);
     return rc < 0 ? rc : 0;
   }
   std::vector<double> get(const char *which) const {
@@ -184,6 +199,28 @@ class Volume : public Function_Base {
     gradients.assign(calc_gradient ? t.nElem : 0, 0.0);
     return tpo_volume(t.handle(), &values0,
                       calc_gradient ? gradients.data() : nullptr, TPO_MEM_HOST);
+  }
+};
+
+// Stability::Function (Buckling.cpp:15-272): the buckling eigenvalues of
+// Ks phi = lambda K phi aggregated as (sum lambda^p)^(1/p), p = 8, and with
+// calc_gradient its design gradient
+class Stability : public Function_Base {
+ public:
+  using Function_Base::Function_Base;
+
+ protected:
+  int Function(TopOpt &t) override {
+    const double p = 8.0;
+    if (int rc = t.StressFnc()) return rc;
+    std::vector<double> lambda;
+    if (calc_gradient) return t.BucklingGradient(lambda, p, &values0, gradients);
+    gradients.clear();
+    if (int rc = t.Buckling(lambda)) return rc;
+    double s = 0.0;
+    for (double l : lambda) s += std::pow(l, p);
+    values0 = std::pow(s, 1.0 / p);
+    return 0;
   }
 };
 

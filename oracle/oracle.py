@@ -351,6 +351,75 @@ def buckling(pb, nev=6, ncv=None, tol=1e-12, solve_rtol=1e-13, v0_seed=0):
     return lam[order], phi[:, order].T
 
 
+def buckling_sensitivity(pb, nel, U, lam, phi, penal=3.0, p=8.0,
+                         dx=(1.0, 1.0, 1.0), E0=1.0, nu=0.3, solve_rtol=1e-13):
+    """The gradient of Stability::Function (Buckling.cpp:113-272) with the
+    filter chain rule (TopOpt::Chain_Filter, Material_Interpolation.cpp:
+    150-187, which without a max-length filter is P^T), in numpy over the
+    oracle.  pb is set up as for `buckling` (design set, assembled, Ks built
+    from U); lam (nev) and phi (nev x 3 nNode, K-normalised) the eigenpairs.
+
+    value = (sum lam^p)^(1/p) (:87-88).  The adjoint right-hand side of pair
+    i is sum_e Es_e phi_e^T dKsdu[a] phi_e at the element's dofs a, with
+    dKsdu[a] = ks_e of a unit displacement (:134-147, :155-178), zero at
+    fixed dofs (:186-190); v_i solves K v_i = rhs_i (:193-225).  Per element
+    (:229-263): sum_i lam_i^(p-1) (phi^T dKsdy phi - lam_i phi^T dKdy phi +
+    v_i^T dKdy U), dKsdy = -dEsdz ks_e(U) (StressFnc :331-332), dKdy =
+    dEdz K0, times value^(1-p) (:265).  dEsdz = p rho^(p-1)
+    (Material_Interpolation.cpp:67-70).  Returns (value, dvdx, dvdrho)."""
+    nel = tuple(int(v) for v in nel)
+    ne = int(np.prod(nel))
+    n = 3 * pb.nn
+    nodes = np.array([element_nodes(nel, e) for e in range(ne)])
+    dofs = (3 * nodes[:, :, None] + np.arange(3)).reshape(ne, 24)
+    rho, _, dEdz = pb.material()
+    Es = pb.es()
+    dEsdz = penal * rho ** (penal - 1)
+    K0 = element_stiffness(dx, E0, nu)
+    eye = np.eye(24)
+    dKsdu = np.array([stress_stiffness_element(eye[d], dx, E0, nu) for d in range(24)])
+    lam = np.asarray(lam, np.float64)
+    phi = np.asarray(phi, np.float64)
+    nev = lam.size
+    Ue = U[dofs]
+    Pe = phi[:, dofs]
+    t = np.einsum("kei,aij,kej->kea", Pe, dKsdu, Pe) * Es[None, :, None]
+    rhs = np.zeros((nev, n))
+    for k in range(nev):
+        np.add.at(rhs[k], dofs.ravel(), t[k].ravel())
+    fm, _ = pb.get_bc()
+    fixed = ((fm[:, None] >> np.arange(3)) & 1).astype(bool).ravel()
+    rhs[:, fixed] = 0.0
+    o = default_opts(rtol=solve_rtol, maxit=5000)
+    V = np.zeros_like(rhs)
+    for k in range(nev):
+        V[k], st, _, _ = pb.solve(b=np.ascontiguousarray(rhs[k]), opts=o)
+        if st != 0:
+            raise RuntimeError(f"oracle adjoint solve failed (status {st})")
+    Ve = V[:, dofs]
+    ks = np.einsum("ed,dij->eij", Ue, dKsdu)      # ks_e(U), linear in U
+    pdKsp = -dEsdz[None] * np.einsum("kei,eij,kej->ke", Pe, ks, Pe)
+    pdKp = dEdz[None] * np.einsum("kei,ij,kej->ke", Pe, K0, Pe)
+    vKu = dEdz[None] * np.einsum("kei,ij,ej->ke", Ve, K0, Ue)
+    value = float(np.sum(lam ** p) ** (1.0 / p))
+    g = np.sum(lam[:, None] ** (p - 1) * (pdKsp - lam[:, None] * pdKp + vKu), axis=0)
+    g *= value ** (1.0 - p)
+    return value, pb.filter(g, transpose=True), g
+
+
+def buckling_dense(pb, nev):
+    """The nev largest eigenpairs of Ks phi = lambda K phi by a dense
+    generalized symmetric eigensolve (small problems only): lambda
+    descending, phi as rows, K-normalised."""
+    import scipy.linalg as sla
+    n = 3 * pb.nn
+    A = dense(pb.ks_apply, n)
+    B = dense(pb.apply, n)
+    w, v = sla.eigh(0.5 * (A + A.T), 0.5 * (B + B.T))
+    order = np.argsort(w)[::-1][:nev]
+    return w[order], v[:, order].T
+
+
 def oc_update(x, dfdx, g, dgdx, move, xmin=None, xmax=None):
     """MMA::OCsub (MMA.cpp:103-180); returns (x_new, change)."""
     n = x.size

@@ -23,6 +23,10 @@ from topopt3d_b200 import problems as P
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
+def rel(a, b):
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
 def fixture(name):
     return dict(np.load(os.path.join(GOLD, name + ".npz")))
 
@@ -74,6 +78,45 @@ def test_oracle_buckling_reproduces_fixture(oracle):
     lam, _ = oracle.buckling(pb, nev=int(g["nev"]))
     np.testing.assert_allclose(lam, g["lam"], rtol=1e-9)
     assert float(g["dense_err"]) < 1e-10
+
+
+def oracle_column(oracle, nel, levels, rtol=1e-14, x=None):
+    """The cfg4 column on the oracle: design set, assembled, U solved, Ks
+    built.  Returns (problem, U)."""
+    c = P.CONFIGS["cfg4"]
+    pb = oracle.Problem(nel, rmin=c["rmin"], mg_levels=levels)
+    P.apply_bcs(pb, P.bcs("cfg4", nel))
+    pb.set_design(P.design("cfg4", nel) if x is None else x, 3.0, 1e-10)
+    o = oracle.default_opts(rtol=rtol, maxit=5000)
+    pb.assemble(o)
+    U, st, _, _ = pb.solve(opts=o)
+    assert st == 0
+    pb.ks_assemble(U)
+    return pb, U
+
+
+def test_oracle_buckling_sensitivity_matches_finite_differences(oracle):
+    """The oracle's restatement of the gradient (Buckling.cpp:113-272 with
+    the filter chain rule) against central differences of the aggregated
+    value, each evaluation a full design -> U -> Ks -> dense eigensolve."""
+    nel, nev, h = (4, 2, 6), 3, 1e-5
+    x0 = P.design("cfg4", nel)
+    pb, U = oracle_column(oracle, nel, 2, x=x0)
+    lam, phi = oracle.buckling_dense(pb, nev)
+    assert lam[-1] > 1.05 * oracle.buckling_dense(pb, nev + 1)[0][-1]  # a gap
+    value, dvdx, _ = oracle.buckling_sensitivity(pb, nel, U, lam, phi)
+    assert abs(value - np.sum(lam ** 8) ** 0.125) <= 1e-14 * value
+
+    def agg(x):
+        q, _ = oracle_column(oracle, nel, 2, x=x)
+        return np.sum(oracle.buckling_dense(q, nev)[0] ** 8) ** 0.125
+
+    for e in (0, 7, 20, 33, 47):
+        xp, xm = x0.copy(), x0.copy()
+        xp[e] += h
+        xm[e] -= h
+        fd = (agg(xp) - agg(xm)) / (2 * h)
+        assert abs(dvdx[e] - fd) <= 1e-7 * abs(fd), (e, dvdx[e], fd)
 
 
 def gpu_problem(T, g, precision_rtol=1e-12):
@@ -159,9 +202,70 @@ def test_buckling_cfg4(T):
 def test_stability_function(T):
     g = fixture("buckling_column_8x4x8")
     t = gpu_problem(T, g)
-    f = T.Stability([1.0], 0.0, 1.0, objective=True)
+    f = T.Stability([1.0], 0.0, 1.0, objective=True, calc_gradient=False)
     f.Compute(t)
     expect = np.sum(np.asarray(g["lam"]) ** 8) ** (1 / 8)
     assert abs(f.values[0] - expect) <= 1e-8 * expect
-    with pytest.raises(T.TopOptError):
-        T.Stability([1.0], 0.0, 1.0, calc_gradient=True)
+    assert f.gradient is None
+
+
+@pytest.mark.gpu
+def test_buckling_sensitivity_matches_oracle(T, oracle):
+    """The gradient through the C ABI from the same eigenpairs as the oracle
+    (the oracle's dense eigensolve of the 8x4x8 column, passed in as host
+    and as device buffers): value to round-off, dvdx and dvdrho to 1e-8."""
+    import torch
+    g = fixture("buckling_column_8x4x8")
+    nel, levels, nev = tuple(int(v) for v in g["nel"]), int(g["levels"]), 4
+    pb, U = oracle_column(oracle, nel, levels)
+    lam, phi = oracle.buckling_dense(pb, nev)
+    val_o, dvdx_o, drho_o = oracle.buckling_sensitivity(pb, nel, U, lam, phi)
+    t = gpu_problem(T, g)
+    o = T.default_opts(rtol=1e-12, maxit=5000)
+    val, dvdx, drho = t.buckling_sensitivity(lam, phi, opts=o, want_drho=True)
+    assert abs(val - val_o) <= 1e-14 * val_o
+    assert rel(dvdx, dvdx_o) < 1e-8 and rel(drho, drho_o) < 1e-8
+    assert t.last_adjoint["status"] == 0
+    dev = torch.tensor(phi, device="cuda")
+    val_d, dvdx_d = t.buckling_sensitivity(lam, dev, opts=o)
+    assert val_d == val and rel(dvdx_d.cpu().numpy(), dvdx) < 1e-12
+
+
+@pytest.mark.gpu
+def test_stability_gradient_finite_differences(T):
+    """Stability with calc_gradient on the GPU's own eigenpairs against
+    central differences of the whole GPU pipeline (MatIntFnc, FEAssemble,
+    FESolve, Ks, LOBPCG) on the 8x4x8 column."""
+    g = fixture("buckling_column_8x4x8")
+    nel, cfg = tuple(int(v) for v in g["nel"]), str(g["cfg"])
+    x0 = P.design(cfg, nel)
+    t = gpu_problem(T, g)
+    eig = dict(nev=4, block=12, tol=1e-10)
+    lam, phi = t.buckling(want_vectors=True, **eig)
+    assert t.last_eig["status"] == 0
+    value, dvdx = t.buckling_sensitivity(lam, phi, opts=T.default_opts(rtol=1e-12, maxit=5000))
+    o = T.default_opts(rtol=1e-12, maxit=5000)
+
+    def agg(x):
+        t.MatIntFnc(x)
+        t.FEAssemble(o)
+        t.set("U", np.zeros(3 * t.nNode))
+        assert t.FESolve(o)["status"] == 0
+        t.ks_assemble()
+        return np.sum(t.buckling(**eig) ** 8) ** 0.125
+
+    h = 1e-5
+    for e in (3, 100, 200):
+        xp, xm = x0.copy(), x0.copy()
+        xp[e] += h
+        xm[e] -= h
+        fd = (agg(xp) - agg(xm)) / (2 * h)
+        assert abs(dvdx[e] - fd) <= 1e-6 * abs(fd), (e, dvdx[e], fd)
+    t.MatIntFnc(x0)
+    t.FEAssemble(o)
+    t.set("U", np.zeros(3 * t.nNode))
+    t.FESolve(o)
+    f = T.Stability([1.0], 0.0, 1.0, objective=True, calc_gradient=True, nev=4)
+    f.Compute(t)
+    assert abs(f.values[0] - value) <= 1e-8 * value
+    assert rel(f.gradient, dvdx) < 1e-5

@@ -34,7 +34,7 @@ EXPORTS = (
     "tpo_set_vector", "tpo_compliance", "tpo_volume", "tpo_filter",
     "tpo_oc_update", "tpo_sync", "tpo_set_stream", "tpo_kernel_launches",
     "tpo_sensitivity_noalloc", "tpo_default_eig_opts", "tpo_ks_assemble",
-    "tpo_ks_apply", "tpo_buckling",
+    "tpo_ks_apply", "tpo_buckling", "tpo_buckling_sensitivity",
 )
 NOALLOC_MAX_ELEMS = 1 << 20
 
@@ -130,6 +130,9 @@ def load(path: str | None = None):
         "tpo_ks_apply": (C.c_int, [vp, vp, vp, i32, C.c_int]),
         "tpo_buckling": (C.c_int, [vp, C.POINTER(EigOpts), dp, vp, C.c_int,
                                    C.POINTER(EigInfo)]),
+        "tpo_buckling_sensitivity": (C.c_int, [vp, i32, dp, vp, d, C.POINTER(SolveOpts),
+                                               dp, vp, vp, C.c_int,
+                                               C.POINTER(SolveInfo)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

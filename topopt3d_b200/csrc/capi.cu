@@ -207,7 +207,7 @@ void free_all(Ctx &c) {
   dfree(c.Ainv); dfree(c.Adense); dfree(c.solver_work); dfree(c.dev_info);
   dfree(c.finv); dfree(c.taps_d);
   dfree(c.w64);
-  dfree(c.Es64); dfree(c.ks_S); dfree(c.ks_H); dfree(c.eig_buf);
+  dfree(c.Es64); dfree(c.dEsdz64); dfree(c.bk_buf); c.bk_n = 0; dfree(c.ks_S); dfree(c.ks_H); dfree(c.eig_buf);
   c.eig_n = 0;
   if (c.cublas) cublasDestroy(static_cast<cublasHandle_t>(c.cublas));
   c.cublas = nullptr;
@@ -400,7 +400,7 @@ int tpo_create(const tpo_mesh_params *p, tpo_ctx **out) {
     A(c.gk_slot, nce); A(c.gk_elem, nce); A(c.gk_count, 1);
   }
   A(c.x, c.ne); A(c.rho, c.ne); A(c.E64, c.ne); A(c.dEdz, c.ne); A(c.E32, c.ne);
-  A(c.Es64, c.ne);
+  A(c.Es64, c.ne); A(c.dEsdz64, c.ne);
   A(c.fix, c.nn); A(c.idm, c.nn); A(c.F, 3 * c.nn); A(c.U, 3 * c.nn);
   A(c.scal, tpo::kScalCount); A(c.part, tpo::kPartCount); A(c.ticket, tpo::kMaxBatch + tpo::kAuxStreams);
   A(c.gbar, 1);
@@ -568,8 +568,14 @@ int tpo_set_moduli(tpo_ctx *ctx, const double *E, const double *dEdz, int mem) {
   CK(cudaMemcpyAsync(c.E64, E, sizeof(double) * c.ne, k, c.stream));
   if (dEdz) CK(cudaMemcpyAsync(c.dEdz, dEdz, sizeof(double) * c.ne, k, c.stream));
   tpo::launch_d2f(c.ne, c.E64, c.E32, c.stream);
-  // given moduli carry no E_min split: the stress stiffness uses E itself
+  // given moduli carry no E_min split: the stress stiffness uses E itself,
+  // and its derivative dEdz (zero when none is given)
   CK(cudaMemcpyAsync(c.Es64, c.E64, sizeof(double) * c.ne, cudaMemcpyDeviceToDevice, c.stream));
+  if (dEdz)
+    CK(cudaMemcpyAsync(c.dEsdz64, c.dEdz, sizeof(double) * c.ne, cudaMemcpyDeviceToDevice,
+                       c.stream));
+  else
+    CK(cudaMemsetAsync(c.dEsdz64, 0, sizeof(double) * c.ne, c.stream));
   c.have_material = true;
   refresh_idm(c);
   CK(cudaStreamSynchronize(c.stream));
@@ -803,6 +809,49 @@ int tpo_buckling(tpo_ctx *ctx, const tpo_eig_opts *opts, double *lambda,
   const int rc = tpo::buckling(c, o, lambda, phi, mem, &one);
   if (info) *info = one;
   if (rc < 0 && rc != TPO_E_BREAKDOWN) return finish(c, rc);
+  return finish(c, rc);
+}
+
+int tpo_buckling_sensitivity(tpo_ctx *ctx, int32_t nev, const double *lambda,
+                             const double *phi, double p, const tpo_solve_opts *opts,
+                             double *value, double *dvdx, double *dvdrho, int mem,
+                             tpo_solve_info *info) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = check_mem(c, mem)) return rc;
+  REQUIRE(lambda && phi && value && dvdx, "null lambda, phi, value or dvdx");
+  REQUIRE(nev >= 1 && nev <= tpo::kMaxEigPairs, "need 1 <= nev <= 32");
+  REQUIRE(std::isfinite(p) && p >= 1.0, "the aggregation power p must be >= 1");
+  REQUIRE(c.ks_ready, "tpo_ks_assemble must be called first");
+  tpo_solve_opts o;
+  if (opts) o = *opts; else tpo_default_solve_opts(&o);
+  if (int rc = validate_solve(c, o)) return rc;
+  const size_t n = 3 * c.nn, ne = c.ne;
+  const size_t need = 2 * nev * n + 24 * ne + 2 * ne + (mem == TPO_MEM_DEVICE ? 0 : nev * n);
+  if (c.bk_n < need) {
+    dfree(c.bk_buf);
+    c.bk_n = 0;
+    CK(cudaMalloc(&c.bk_buf, sizeof(double) * need));
+    c.bk_n = need;
+  }
+  double *rhs = c.bk_buf, *v = rhs + nev * n, *W = v + nev * n, *g = W + 24 * ne,
+         *dx = g + ne;
+  const double *ph = phi;
+  if (mem != TPO_MEM_DEVICE) {
+    double *st = dx + ne;
+    CK(cudaMemcpyAsync(st, phi, sizeof(double) * nev * n, cudaMemcpyHostToDevice, c.stream));
+    ph = st;
+  }
+  tpo_solve_info one{};
+  const int rc = tpo::buckling_sensitivity(c, nev, lambda, ph, p, o, rhs, v, W, g,
+                                           mem == TPO_MEM_DEVICE ? dvdx : dx, value, &one);
+  if (info) *info = one;
+  if (rc < 0 && rc != TPO_E_BREAKDOWN) return finish(c, rc);
+  if (mem != TPO_MEM_DEVICE)
+    if (int rc2 = copy_out(c, dvdx, dx, ne, mem)) return rc2;
+  if (dvdrho)
+    if (int rc2 = copy_out(c, dvdrho, g, ne, mem)) return rc2;
+  CK(cudaStreamSynchronize(c.stream));
   return finish(c, rc);
 }
 

@@ -456,4 +456,57 @@ int buckling(Ctx &c, const tpo_eig_opts &o, double *lambda, double *phi,
   return status;
 }
 
+// The gradient of the aggregated buckling value (Stability::Function,
+// Buckling.cpp:87-88 and 113-272) and its filter chain rule (P^T,
+// Material_Interpolation.cpp:150-187 without a max-length filter), for nev
+// K-normalised eigenpairs (lam on the host, phi nev device columns of 3 nn).
+// Scratch: rhs and v (nev columns each), W (24 x nElem).  g receives the
+// gradient with respect to the filtered density, dvdx the one with respect
+// to the design; info aggregates the adjoint solves.
+int buckling_sensitivity(Ctx &c, int nev, const double *lam, const double *phi, double p,
+                         const tpo_solve_opts &o, double *rhs, double *v, double *W,
+                         double *g, double *dvdx, double *value, tpo_solve_info *info) {
+  cudaStream_t s = c.stream;
+  const int64_t n = 3 * c.nn;
+  double sum = 0.0;
+  for (int k = 0; k < nev; ++k) sum += std::pow(lam[k], p);
+  *value = std::pow(sum, 1.0 / p);
+  // adjoint right-hand sides (:155-190)
+  for (int k = 0; k < nev; ++k) launch_bk_adj_rhs(c, phi + k * n, W, rhs + k * n, s);
+  CK(cudaGetLastError());
+  // K v_k = rhs_k (:193-225), in blocks of right-hand sides
+  CK(cudaMemsetAsync(v, 0, sizeof(double) * n * nev, s));
+  tpo_solve_info acc{};
+  int worst = TPO_OK;
+  for (int j0 = 0; j0 < nev;) {
+    int nb = 1;
+    while (2 * nb <= nev - j0 && 2 * nb <= kMaxBatch) nb *= 2;
+    if (int rc = ensure_columns(c, nb)) return rc;
+    tpo_solve_info one{};
+    const int rc = solve(c, o, rhs + j0 * n, v + j0 * n, &one, nb);
+    if (rc < 0 && rc != TPO_E_BREAKDOWN) return rc;
+    if (rc < 0 ? rc < worst : (worst == TPO_OK && rc != TPO_OK)) worst = rc;
+    acc.iterations += one.iterations;
+    acc.outer += one.outer;
+    acc.relres = std::max(acc.relres, one.relres);
+    acc.solve_ms += one.solve_ms;
+    j0 += nb;
+  }
+  // element gradient (:229-265) and the filter chain rule (:267-274)
+  BkCoef coef{};
+  for (int k = 0; k < nev; ++k) {
+    coef.a[k] = std::pow(lam[k], p - 1.0);
+    coef.lam[k] = lam[k];
+  }
+  coef.scale = std::pow(*value, 1.0 - p);
+  launch_bk_gradient(c, phi, v, n, nev, coef, g, s);
+  launch_filter(c, g, dvdx, true, s);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s));
+  acc.status = worst;
+  acc.setup_ms = c.setup_ms;
+  if (info) *info = acc;
+  return worst;
+}
+
 }  // namespace tpo

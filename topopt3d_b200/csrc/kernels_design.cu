@@ -95,13 +95,14 @@ __device__ __forceinline__ double vecpow(double v, double p) {
 // Material_Interpolation.cpp:40-75 with vdMin <= 0 (y = 1, z = rho)
 __global__ void k_simp(int64_t ne, const double *__restrict__ rho, double penal,
                        double eps, double *E, double *dEdz, float *E32,
-                       double *Es) {
+                       double *Es, double *dEsdz) {
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne;
        e += (int64_t)gridDim.x * blockDim.x) {
     const double z = rho[e];
     double d = vecpow(z, penal - 1);
     const double es = d * z;
     d = d * penal;
+    dEsdz[e] = d;
     dEdz[e] = d * (1 - eps);
     const double Ee = eps + (1 - eps) * es;
     E[e] = Ee;
@@ -237,7 +238,7 @@ void launch_filter_adj_uniform(const Ctx &c, double value, double *out,
 void launch_simp(const Ctx &c, double penal, double eps, cudaStream_t s) {
   count_launch();
   k_simp<<<grid_for(c.ne, 256), 256, 0, s>>>(c.ne, c.rho, penal, eps, c.E64,
-                                              c.dEdz, c.E32, c.Es64);
+                                              c.dEdz, c.E32, c.Es64, c.dEsdz64);
 }
 
 void launch_sensitivity(const Ctx &c, const double *U, double *dc,

@@ -175,6 +175,218 @@ __global__ void k_ks_apply(int nx, int ny, int nz, const double *__restrict__ S,
   }
 }
 
+// ---- buckling sensitivities (Buckling.cpp:113-272)
+//
+// With ks_e = H_e (x) I_3, phi^T ks_e(u) phi = detJ sum_q sigma_q(u) : M_q
+// where M_q = sum_c grad(phi_c) grad(phi_c)^T at Gauss point q.  This is
+// linear in u, so its gradient with respect to u_e (the reference's
+// phi^T dKsdu phi, :134-147 and :168-173) is detJ sum_q B_q^T D m_q, m_q the
+// Voigt form of M_q with doubled shears.
+
+// M_q of one element for phi (phi[l][c], lexicographic corners) as the
+// Voigt vector (Mxx, Myy, Mzz, 2Mxy, 2Myz, 2Mxz)
+__device__ __forceinline__ void phi_moment(const KsConst &kc, int q, const double phi[8][3],
+                                           double m[6]) {
+  double G[3][3];   // G[c][a] = d phi_c / d x_a
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      double s = 0.0;
+#pragma unroll
+      for (int l = 0; l < 8; ++l) s += kc.g[q][a][l] * phi[l][c];
+      G[c][a] = s;
+    }
+  double M[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) M[a][b] = G[0][a] * G[0][b] + G[1][a] * G[1][b] + G[2][a] * G[2][b];
+  m[0] = M[0][0];
+  m[1] = M[1][1];
+  m[2] = M[2][2];
+  m[3] = 2.0 * M[0][1];
+  m[4] = 2.0 * M[1][2];
+  m[5] = 2.0 * M[0][2];
+}
+
+// Voigt stress D eps of an engineering-strain Voigt vector
+__device__ __forceinline__ void voigt_stress(const KsConst &kc, const double e[6], double s[6]) {
+  s[0] = kc.t1 * e[0] + kc.t3 * (e[1] + e[2]);
+  s[1] = kc.t1 * e[1] + kc.t3 * (e[0] + e[2]);
+  s[2] = kc.t1 * e[2] + kc.t3 * (e[0] + e[1]);
+  s[3] = kc.t2 * e[3];
+  s[4] = kc.t2 * e[4];
+  s[5] = kc.t2 * e[5];
+}
+
+// W[(3l + c) * ne + e] = Es_e d(phi^T ks_e phi)/du_{l,c} for one eigenvector
+__global__ void k_bk_adj_element(int nelx, int nely, int nelz,
+                                 const double *__restrict__ phi,
+                                 const double *__restrict__ Es, KsConst kc,
+                                 double *__restrict__ W) {
+  const int Nx = nelx + 1, Ny = nely + 1;
+  const int64_t ne = (int64_t)nelx * nely * nelz;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e % nelx), j = (int)((e / nelx) % nely),
+              k = (int)(e / ((int64_t)nelx * nely));
+    const int64_t n0 = ((int64_t)k * Ny + j) * Nx + i;
+    double p[8][3], w[8][3];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+      const int64_t n = n0 + (l & 1) + ((l >> 1) & 1) * Nx + ((l >> 2) & 1) * (int64_t)Nx * Ny;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        p[l][c] = phi[3 * n + c];
+        w[l][c] = 0.0;
+      }
+    }
+#pragma unroll 1
+    for (int q = 0; q < 8; ++q) {
+      double m[6], s[6];
+      phi_moment(kc, q, p, m);
+      voigt_stress(kc, m, s);
+      // B_q^T s
+#pragma unroll
+      for (int l = 0; l < 8; ++l) {
+        const double gx = kc.g[q][0][l], gy = kc.g[q][1][l], gz = kc.g[q][2][l];
+        w[l][0] += gx * s[0] + gy * s[3] + gz * s[5];
+        w[l][1] += gy * s[1] + gx * s[3] + gz * s[4];
+        w[l][2] += gz * s[2] + gy * s[4] + gx * s[5];
+      }
+    }
+    const double sc = Es[e] * kc.detJ;
+#pragma unroll
+    for (int l = 0; l < 8; ++l)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) W[(int64_t)(3 * l + c) * ne + e] = sc * w[l][c];
+  }
+}
+
+// rhs[3n + c] = sum over the (up to 8) elements around node n of their
+// W entry for n, in a fixed order; zero at fixed dofs (:186-190)
+__global__ void k_bk_adj_gather(int nelx, int nely, int nelz,
+                                const double *__restrict__ W,
+                                const uint8_t *__restrict__ fix,
+                                double *__restrict__ rhs) {
+  const int Nx = nelx + 1, Ny = nely + 1, Nz = nelz + 1;
+  const int64_t nn = (int64_t)Nx * Ny * Nz, ne = (int64_t)nelx * nely * nelz;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
+       n += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(n % Nx), j = (int)((n / Nx) % Ny), k = (int)(n / ((int64_t)Nx * Ny));
+    double acc[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int cz = 0; cz < 2; ++cz)
+#pragma unroll
+      for (int cy = 0; cy < 2; ++cy)
+#pragma unroll
+        for (int cx = 0; cx < 2; ++cx) {
+          const int ei = i - 1 + cx, ej = j - 1 + cy, ek = k - 1 + cz;
+          if (ei < 0 || ej < 0 || ek < 0 || ei >= nelx || ej >= nely || ek >= nelz)
+            continue;
+          const int64_t e = ((int64_t)ek * nely + ej) * nelx + ei;
+          const int ln = (1 - cx) + 2 * (1 - cy) + 4 * (1 - cz);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) acc[c] += W[(int64_t)(3 * ln + c) * ne + e];
+        }
+    const unsigned f = fix[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) rhs[3 * n + c] = ((f >> c) & 1u) ? 0.0 : acc[c];
+  }
+}
+
+// per element, over the nev eigenpairs (phi_k, v_k columns of stride ld):
+// g_e = scale sum_k a_k (-dEsdz_e phi^T ks_e(U) phi - lam_k dEdz_e phi^T K0 phi
+//                        + dEdz_e v^T K0 U)          (:229-265)
+__global__ void k_bk_gradient(int nelx, int nely, int nelz,
+                              const double *__restrict__ U,
+                              const double *__restrict__ phi,
+                              const double *__restrict__ v, int64_t ld, int nev,
+                              const double *__restrict__ dEdz,
+                              const double *__restrict__ dEsdz, KsConst kc,
+                              const double *__restrict__ K0, BkCoef coef,
+                              double *__restrict__ g) {
+  const int Nx = nelx + 1, Ny = nely + 1;
+  const int64_t ne = (int64_t)nelx * nely * nelz;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e % nelx), j = (int)((e / nelx) % nely),
+              k = (int)(e / ((int64_t)nelx * nely));
+    const int64_t n0 = ((int64_t)k * Ny + j) * Nx + i;
+    int64_t node[8];
+    double u[8][3];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+      node[l] = n0 + (l & 1) + ((l >> 1) & 1) * Nx + ((l >> 2) & 1) * (int64_t)Nx * Ny;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) u[l][c] = U[3 * node[l] + c];
+    }
+    // K0 U_e
+    double ku[24];
+#pragma unroll
+    for (int r = 0; r < 24; ++r) {
+      double s = 0.0;
+#pragma unroll
+      for (int l = 0; l < 8; ++l)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) s += __ldg(K0 + r * 24 + 3 * l + c) * u[l][c];
+      ku[r] = s;
+    }
+    const double de = dEdz[e], dse = dEsdz[e];
+    double acc = 0.0;
+#pragma unroll 1
+    for (int kk = 0; kk < nev; ++kk) {
+      const double *pk = phi + kk * ld, *vk = v + kk * ld;
+      double p[8][3];
+      double vku = 0.0;
+#pragma unroll
+      for (int l = 0; l < 8; ++l)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          p[l][c] = pk[3 * node[l] + c];
+          vku += vk[3 * node[l] + c] * ku[3 * l + c];
+        }
+      // phi^T ks_e(U) phi = detJ sum_q sigma_q(U) : M_q(phi)
+      double pksp = 0.0;
+#pragma unroll 1
+      for (int q = 0; q < 8; ++q) {
+        double F[3][3];   // F[c][a] = d u_c / d x_a
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            double s = 0.0;
+#pragma unroll
+            for (int l = 0; l < 8; ++l) s += kc.g[q][a][l] * u[l][c];
+            F[c][a] = s;
+          }
+        const double eps[6] = {F[0][0], F[1][1], F[2][2], F[0][1] + F[1][0],
+                               F[1][2] + F[2][1], F[0][2] + F[2][0]};
+        double sig[6], m[6];
+        voigt_stress(kc, eps, sig);
+        phi_moment(kc, q, p, m);
+        pksp += sig[0] * m[0] + sig[1] * m[1] + sig[2] * m[2] + sig[3] * m[3] +
+                sig[4] * m[4] + sig[5] * m[5];
+      }
+      pksp *= kc.detJ;
+      // phi^T K0 phi
+      double pkp = 0.0;
+#pragma unroll
+      for (int r = 0; r < 24; ++r) {
+        double s = 0.0;
+#pragma unroll
+        for (int l = 0; l < 8; ++l)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) s += __ldg(K0 + r * 24 + 3 * l + c) * p[l][c];
+        pkp += p[r / 3][r % 3] * s;
+      }
+      acc += coef.a[kk] * (-dse * pksp - coef.lam[kk] * de * pkp + de * vku);
+    }
+    g[e] = coef.scale * acc;
+  }
+}
+
 template <int NB>
 void ks_launch(const Ctx &c, const double *u, double *y) {
   count_launch();
@@ -190,6 +402,23 @@ void launch_ks_assemble(const Ctx &c, cudaStream_t s) {
                                                     c.U, c.Es64, c.ksc, c.ks_H);
   k_ks_gather<<<grid_for(c.nn, 128), 128, 0, s>>>(c.nel[0], c.nel[1], c.nel[2],
                                                    c.ks_H, c.ks_S);
+}
+
+void launch_bk_adj_rhs(const Ctx &c, const double *phi, double *W, double *rhs,
+                       cudaStream_t s) {
+  count_launch(2);
+  k_bk_adj_element<<<grid_for(c.ne, 128), 128, 0, s>>>(c.nel[0], c.nel[1], c.nel[2], phi,
+                                                        c.Es64, c.ksc, W);
+  k_bk_adj_gather<<<grid_for(c.nn, 128), 128, 0, s>>>(c.nel[0], c.nel[1], c.nel[2], W,
+                                                       c.fix, rhs);
+}
+
+void launch_bk_gradient(const Ctx &c, const double *phi, const double *v, int64_t ld,
+                        int nev, const BkCoef &coef, double *g, cudaStream_t s) {
+  count_launch();
+  k_bk_gradient<<<grid_for(c.ne, 128), 128, 0, s>>>(c.nel[0], c.nel[1], c.nel[2], c.U,
+                                                     phi, v, ld, nev, c.dEdz, c.dEsdz64,
+                                                     c.ksc, c.K0lex, coef, g);
 }
 
 void launch_ks_apply(const Ctx &c, const double *u, double *y, int nb) {

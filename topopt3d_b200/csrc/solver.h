@@ -19,6 +19,10 @@ int ensure_columns(Ctx &c, int nb);
 // the nev largest eigenvalues of Ks phi = lambda K phi (eigen.cu)
 int buckling(Ctx &c, const tpo_eig_opts &o, double *lambda, double *phi,
              int phi_mem, tpo_eig_info *info);
+// gradient of the aggregated buckling value (eigen.cu)
+int buckling_sensitivity(Ctx &c, int nev, const double *lam, const double *phi, double p,
+                         const tpo_solve_opts &o, double *rhs, double *v, double *W,
+                         double *g, double *dvdx, double *value, tpo_solve_info *info);
 int solve(Ctx &c, const tpo_solve_opts &o, const double *b, double *x,
           tpo_solve_info *info, int nb = 1, tpo_solve_info *col = nullptr);
 

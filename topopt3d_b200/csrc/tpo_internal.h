@@ -146,6 +146,7 @@ struct Ctx {
   double *F = nullptr, *U = nullptr;
   double *x = nullptr, *rho = nullptr, *E64 = nullptr, *dEdz = nullptr;
   double *Es64 = nullptr;   // rho^p without E_min (stress stiffness)
+  double *dEsdz64 = nullptr;   // d Es / d rho (Material_Interpolation.cpp:67-70)
   float *E32 = nullptr;
   double *S0 = nullptr;     // fine-level assembled stencil (setup only)
   double *K0lex = nullptr;  // K0 in lexicographic corner order (576)
@@ -205,6 +206,8 @@ struct Ctx {
   void *cublas = nullptr;
   double *eig_buf = nullptr;
   size_t eig_n = 0;
+  double *bk_buf = nullptr;   // buckling-sensitivity workspace
+  size_t bk_n = 0;
 
   // CUDA graphs of the CG iteration bodies, keyed on (x, columns)
   cudaGraphExec_t graph64 = nullptr, graph32 = nullptr;
@@ -378,6 +381,22 @@ void launch_filter_adj_uniform(const Ctx &c, double value, double *out,
 void launch_simp(const Ctx &c, double penal, double eps, cudaStream_t s);
 // stress stiffness from c.U and c.Es64 (kernels_ks.cu)
 void launch_ks_assemble(const Ctx &c, cudaStream_t s);
+// buckling sensitivities (kernels_ks.cu): per eigenpair k, a_k = lam_k^(p-1);
+// scale = value^(1-p)
+constexpr int kMaxEigPairs = 32;
+struct BkCoef {
+  double a[kMaxEigPairs];
+  double lam[kMaxEigPairs];
+  double scale;
+};
+// adjoint right-hand side of one eigenvector phi: rhs = sum_e Es_e
+// d(phi^T ks_e phi)/du_e (W: 24 x nElem scratch), zero at fixed dofs
+void launch_bk_adj_rhs(const Ctx &c, const double *phi, double *W, double *rhs,
+                       cudaStream_t s);
+// g_e, the gradient before the filter chain rule, from c.U and nev columns
+// of phi and the adjoint solutions v (stride ld)
+void launch_bk_gradient(const Ctx &c, const double *phi, const double *v, int64_t ld,
+                        int nev, const BkCoef &coef, double *g, cudaStream_t s);
 // y = Ks u for nb columns (stride 3 nn), on c.stream
 void launch_ks_apply(const Ctx &c, const double *u, double *y, int nb);
 void launch_sensitivity(const Ctx &c, const double *U, double *dc,

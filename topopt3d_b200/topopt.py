@@ -297,6 +297,34 @@ class TopOpt:
         self.last_eig["rc"] = rc
         return (lam, phi) if want_vectors else lam
 
+    def buckling_sensitivity(self, lam, phi, p=8.0, opts=None, want_drho=False):
+        """The aggregated buckling value (sum lam^p)^(1/p) and its gradient
+        with respect to the design (Buckling.cpp:87-88, 113-272 with the
+        filter chain rule) from the eigenpairs `buckling(want_vectors=True)`
+        returned (phi as rows, K-normalised); with want_drho also the
+        gradient with respect to the filtered density.  The adjoint solves
+        use opts (default: FP64, rtol 1e-8); their record is kept in
+        last_adjoint."""
+        lam = np.ascontiguousarray(lam, np.float64)
+        nev = lam.size
+        ph, mem, keep = _buf(phi, 3 * self.nNode * nev)
+        if _is_torch(phi):
+            dvdx = phi.new_zeros(self.nElem)
+            drho = phi.new_zeros(self.nElem) if want_drho else None
+        else:
+            dvdx = np.zeros(self.nElem)
+            drho = np.zeros(self.nElem) if want_drho else None
+        dp_ = lambda a: None if a is None else C.c_void_p(
+            a.data_ptr() if _is_torch(a) else a.ctypes.data)
+        value = C.c_double(0.0)
+        info = L.SolveInfo()
+        self._check(self._lib.tpo_buckling_sensitivity(
+            self._h, nev, lam.ctypes.data_as(C.POINTER(C.c_double)), ph, float(p),
+            None if opts is None else C.byref(opts), C.byref(value), dp_(dvdx),
+            dp_(drho), mem, C.byref(info)), "buckling_sensitivity")
+        self.last_adjoint = info.as_dict()
+        return (value.value, dvdx, drho) if want_drho else (value.value, dvdx)
+
     def volume(self, gradient=True):
         v = C.c_double()
         dv = np.zeros(self.nElem) if gradient else None
@@ -378,25 +406,28 @@ class Volume(Function_Base):
 
 
 class Stability(Function_Base):
-    """Stability::Function (Buckling.cpp:15-88): the buckling eigenvalues
+    """Stability::Function (Buckling.cpp:15-272): the buckling eigenvalues
     of Ks phi = lambda K phi aggregated as (sum lambda^p)^(1/p), p = 8
-    (:87-88).  The eigenvalue sensitivities (:113-272) are not computed:
-    only calc_gradient = False is supported."""
+    (:87-88), and with calc_gradient its design gradient through one
+    adjoint solve per eigenpair (:113-272)."""
 
     def __init__(self, values, min_val, max_val, objective=True,
                  calc_gradient=False, nev=6, block=12):
-        if calc_gradient:
-            raise TopOptError(-4, "buckling sensitivities are not implemented")
-        super().__init__(values, min_val, max_val, objective, False)
+        super().__init__(values, min_val, max_val, objective, calc_gradient)
         self.nev, self.block = nev, block
         self.lam = None
 
     def Function(self, topOpt):
         topOpt.ks_assemble()
-        self.lam = topOpt.buckling(nev=self.nev, block=self.block)
         p = 8.0
-        self.values[0] = float(np.sum(self.lam ** p) ** (1.0 / p))
-        self.gradients = None
+        if self.calc_gradient:
+            self.lam, phi = topOpt.buckling(nev=self.nev, block=self.block,
+                                            want_vectors=True)
+            self.values[0], self.gradients = topOpt.buckling_sensitivity(self.lam, phi, p)
+        else:
+            self.lam = topOpt.buckling(nev=self.nev, block=self.block)
+            self.values[0] = float(np.sum(self.lam ** p) ** (1.0 / p))
+            self.gradients = None
 
 
 @dataclass
