@@ -1015,21 +1015,38 @@ int tpo_oc_update(tpo_ctx *ctx, double *x, const double *xmin, const double *xma
   CK(cudaMemcpyAsync(ddf, dfdx, sizeof(double) * n, k, c.stream));
   CK(cudaMemcpyAsync(ddg, dgdx, sizeof(double) * n, k, c.stream));
   tpo::launch_oc_clip(n, ddf, c.stream);
-  // bisection on the Lagrange multiplier (MMA.cpp:136-161)
-  double l1 = 0, l2 = 1e6;
-  while (l2 - l1 > 1e-4) {
-    const double lmid = 0.5 * (l1 + l2);
-    tpo::launch_oc_step(c, n, dx, dxold, dmin, dmax, ddf, ddg, move, lmid, c.scal + tpo::SC_OC_DG, c.stream);
-    CK(cudaMemcpyAsync(c.scal_h + tpo::SC_OC_DG, c.scal + tpo::SC_OC_DG, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-    CK(cudaStreamSynchronize(c.stream));
-    if (g + c.scal_h[tpo::SC_OC_DG] > 0) l1 = lmid; else l2 = lmid;
+  // bisection on the Lagrange multiplier (MMA.cpp:136-161): on the device in
+  // one persistent launch; where the device cannot hold its grid, one
+  // launch per trial with the branch taken on the host
+  cudaError_t lerr = cudaSuccess;
+  if (tpo::launch_oc_bisect(c, n, dx, dxold, dmin, dmax, ddf, ddg, move, g, c.stream, &lerr)) {
+    CK(lerr);
+  } else {
+    double l1 = 0, l2 = 1e6;
+    while (l2 - l1 > 1e-4) {
+      const double lmid = 0.5 * (l1 + l2);
+      tpo::launch_oc_step(c, n, dx, dxold, dmin, dmax, ddf, ddg, move, lmid, c.scal + tpo::SC_OC_DG, c.stream);
+      CK(cudaMemcpyAsync(c.scal_h + tpo::SC_OC_DG, c.scal + tpo::SC_OC_DG, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+      CK(cudaStreamSynchronize(c.stream));
+      if (g + c.scal_h[tpo::SC_OC_DG] > 0) l1 = lmid; else l2 = lmid;
+    }
   }
   tpo::launch_oc_finish(c, n, dx, dxold, dmin, dmax, c.scal + tpo::SC_OC_CHANGE, c.stream);
   CK(cudaMemcpyAsync(c.scal_h + tpo::SC_OC_CHANGE, c.scal + tpo::SC_OC_CHANGE, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaMemcpyAsync(c.scal_h + tpo::kSlotFault, c.scal + tpo::kSlotFault, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
   const cudaMemcpyKind ko = mem == TPO_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   CK(cudaMemcpyAsync(x, dx, sizeof(double) * n, ko, c.stream));
   CK(cudaMemcpyAsync(dfdx, ddf, sizeof(double) * n, ko, c.stream));
   CK(cudaStreamSynchronize(c.stream));
+  if (c.scal_h[tpo::kSlotFault] != 0.0) {
+    // a grid-barrier wait of the bisection gave up: reset and report
+    c.scal_h[tpo::kSlotFault] = 0.0;
+    CK(cudaMemsetAsync(c.gbar, 0, sizeof(unsigned int), c.stream));
+    CK(cudaMemsetAsync(c.scal + tpo::kSlotFault, 0, sizeof(double), c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    c.err = "OC bisection: a grid-barrier wait ran out";
+    return TPO_E_CUDA;
+  }
   if (change) *change = c.scal_h[tpo::SC_OC_CHANGE];
   return finish(c, TPO_OK);
 }

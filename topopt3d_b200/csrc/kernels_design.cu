@@ -2,6 +2,7 @@
 // free), SIMP interpolation, the compliance sensitivity and the OC update.
 #include <math_constants.h>
 
+#include "grid_barrier.cuh"
 #include "modal.cuh"
 
 namespace tpo {
@@ -190,6 +191,67 @@ __global__ void k_sum_parts(int nparts, const double *part, double *out) {
   }
 }
 
+// The whole bisection of MMA::OCsub (MMA.cpp:136-161) in one cooperative
+// launch of kRedBlocks x 256 threads, with no host round trip per trial.
+// Each trial forms the candidate x and the block's partial of
+// dgdx . (x - xold) exactly as k_oc_step does on the same grid; after a grid
+// barrier every block sums the kRedBlocks partials in k_sum_parts' order,
+// so all blocks hold the same total and take the same branch.  The
+// partials are double-buffered by trial parity: a block writes the next
+// trial's partials only after the next barrier, which every block reaches
+// after reading the current ones.
+__global__ void __launch_bounds__(256)
+    k_oc_bisect(int64_t n, double *x, const double *xold, const double *xmin,
+                const double *xmax, const double *dfdx, const double *dgdx,
+                double move, double g, double *part, unsigned int *bar,
+                double *fault) {
+  __shared__ double sh[32];
+  __shared__ double total;
+  double l1 = 0, l2 = 1e6;
+  int trial = 0;
+  while (l2 - l1 > 1e-4) {
+    const double lmid = 0.5 * (l1 + l2);
+    double *pp = part + (trial & 1) * gridDim.x;
+    double s = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+      const double B = pow(-dfdx[i] / dgdx[i] / lmid, 0.5);
+      const double xo = xold[i], lo = xmin[i], hi = xmax[i];
+      const double step = move * (hi - lo);
+      double v = lo + (xo - lo) * B;
+      v = fmin(v, xo + step);
+      v = fmin(v, hi);
+      v = fmax(v, xo - step);
+      v = fmax(v, lo);
+      x[i] = v;
+      s += dgdx[i] * (v - xo);
+    }
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      s = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+      s = warp_sum(s);
+      if (threadIdx.x == 0) pp[blockIdx.x] = s;
+    }
+    if (!grid_barrier(bar, fault)) return;
+    double t = 0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) t += pp[i];
+    t = warp_sum(t);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      t = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+      t = warp_sum(t);
+      if (threadIdx.x == 0) total = t;
+    }
+    __syncthreads();
+    if (g + total > 0) l1 = lmid; else l2 = lmid;
+    ++trial;
+    __syncthreads();
+  }
+}
+
 // x < 1e-6 -> 0 (MMA.cpp:166-173), then Change = max |x - xold| / (xmax - xmin)
 __global__ void k_oc_finish(int64_t n, double *x, const double *xold,
                             const double *xmin, const double *xmax,
@@ -262,6 +324,30 @@ void launch_oc_step(const Ctx &c, int64_t n, double *x, const double *xold,
   k_oc_step<<<kRedBlocks, 256, 0, s>>>(n, x, xold, xmin, xmax, dfdx, dgdx, move,
                                        lmid, c.part);
   k_sum_parts<<<1, 256, 0, s>>>(kRedBlocks, c.part, out);
+}
+
+bool launch_oc_bisect(const Ctx &c, int64_t n, double *x, const double *xold,
+                      const double *xmin, const double *xmax, const double *dfdx,
+                      const double *dgdx, double move, double g, cudaStream_t s,
+                      cudaError_t *err) {
+  static int fits[64] = {0};   // 1: kRedBlocks co-resident CTAs fit, -1: not
+  int dev = 0;
+  cudaGetDevice(&dev);
+  dev &= 63;
+  if (!fits[dev]) {
+    int per_sm = 0, sms = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_oc_bisect, 256, 0);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    fits[dev] = per_sm * sms >= kRedBlocks ? 1 : -1;
+  }
+  if (fits[dev] < 0) return false;
+  count_launch();
+  double *part = c.part;   // 2 x kRedBlocks <= kPartCount
+  unsigned int *bar = c.gbar;
+  double *fault = c.scal + kSlotFault;
+  void *args[] = {&n, &x, &xold, &xmin, &xmax, &dfdx, &dgdx, &move, &g, &part, &bar, &fault};
+  *err = cudaLaunchCooperativeKernel((const void *)k_oc_bisect, kRedBlocks, 256, args, 0, s);
+  return true;
 }
 
 void launch_oc_finish(const Ctx &c, int64_t n, double *x, const double *xold,

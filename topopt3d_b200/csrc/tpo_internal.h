@@ -406,6 +406,13 @@ void launch_oc_step(const Ctx &c, int64_t n, double *x, const double *xold,
                     const double *dgdx, double move, double lmid, double *out,
                     cudaStream_t s);
 void launch_oc_clip(int64_t n, double *dfdx, cudaStream_t s);
+// the whole OC bisection in one cooperative launch of kRedBlocks CTAs (uses
+// c.part, c.gbar and the fault slot); false when the device cannot hold
+// them all at once, and the caller runs the per-trial launches instead
+bool launch_oc_bisect(const Ctx &c, int64_t n, double *x, const double *xold,
+                      const double *xmin, const double *xmax, const double *dfdx,
+                      const double *dgdx, double move, double g, cudaStream_t s,
+                      cudaError_t *err);
 void launch_oc_finish(const Ctx &c, int64_t n, double *x, const double *xold,
                       const double *xmin, const double *xmax, double *out,
                       cudaStream_t s);
