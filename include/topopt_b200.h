@@ -226,6 +226,23 @@ TPO_API int tpo_buckling_sensitivity(tpo_ctx *ctx, int32_t nev, const double *la
                              double *value, double *dvdx, double *dvdrho, int mem,
                              tpo_solve_info *info);
 
+/* Frequency::Function (Dynamic.cpp:18-171) with DiagMassFnc (:181-235):
+ * the lumped mass M (element volume x density / 24 per node component
+ * from the filtered density, plus mlump, optional per-dof point masses in
+ * `mem`; 1e-8 at fixed dofs), then the largest eigenvalues of
+ * M phi = lambda K phi (lambda = 1/omega^2, the lowest frequencies) until
+ * more than nvals have converged and the last is separated from the one
+ * before it by a relative 1e-5 (UNIQUE_LAST_NEV), by the block eigensolver
+ * of tpo_buckling with opts (NULL = defaults; nev and block are set here).
+ * lambda (host, room for 32) receives them descending and *nconv their
+ * count; *value = (sum lambda^p)^(1/p) over all of them; dvdx (nElem in
+ * `mem`, optional) its design gradient, summed over the first nvals - 1
+ * eigenpairs as the reference does (:127-160), with the filter chain rule.
+ * Needs tpo_fe_assemble; 1 <= nvals <= 29. */
+TPO_API int tpo_frequency(tpo_ctx *ctx, int32_t nvals, double density, const double *mlump,
+                  const tpo_eig_opts *opts, double p, double *lambda, int32_t *nconv,
+                  double *value, double *dvdx, int mem, tpo_eig_info *info);
+
 /* U, F, x, rho, E, dEdz accessors: which = "U","F","x","rho","E","dEdz" */
 TPO_API int tpo_get_vector(const tpo_ctx *ctx, const char *which, double *out, int mem);
 TPO_API int tpo_set_vector(tpo_ctx *ctx, const char *which, const double *in, int mem);

@@ -24,6 +24,7 @@
 #include <cmath>
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "topopt_b200.h"
@@ -221,6 +222,34 @@ class Stability : public Function_Base {
     for (double l : lambda) s += std::pow(l, p);
     values0 = std::pow(s, 1.0 / p);
     return 0;
+  }
+};
+
+// Frequency::Function (Dynamic.cpp:18-171): the largest eigenvalues of
+// M phi = lambda K phi (the lowest natural frequencies) with the lumped
+// mass of DiagMassFnc, aggregated as (sum lambda^p)^(1/p), p = 8, and with
+// calc_gradient its design gradient
+class Frequency : public Function_Base {
+ public:
+  Frequency(std::vector<double> values, double min_val, double max_val, bool objective,
+            bool calc_gradient, int nvals, double density)
+      : Function_Base(std::move(values), min_val, max_val, objective, calc_gradient),
+        nvals(nvals), density(density) {}
+  int nvals;
+  double density;
+  std::vector<double> lambda;
+
+ protected:
+  int Function(TopOpt &t) override {
+    lambda.assign(32, 0.0);
+    int32_t nconv = 0;
+    gradients.assign(calc_gradient ? t.nElem : 0, 0.0);
+    const int rc = tpo_frequency(t.handle(), nvals, density, nullptr, &t.eig, 8.0,
+                                 lambda.data(), &nconv, &values0,
+                                 calc_gradient ? gradients.data() : nullptr, TPO_MEM_HOST,
+                                 &t.eig_info);
+    lambda.resize(nconv);
+    return rc < 0 ? rc : 0;
   }
 };
 

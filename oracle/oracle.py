@@ -420,6 +420,66 @@ def buckling_dense(pb, nev):
     return w[order], v[:, order].T
 
 
+def lumped_mass(pb, nel, density, dx=(1.0, 1.0, 1.0), mlump=None):
+    """Frequency::DiagMassFnc (Dynamic.cpp:181-235) with the fixed-dof
+    zeroing (:42-44): each element adds V_e * elemSize * density / (2^3 * 3)
+    to the three dofs of each of its nodes (V = rho,
+    Material_Interpolation.cpp:63-64), then the point masses; 1e-8 on fixed
+    dofs."""
+    nel = tuple(int(v) for v in nel)
+    ne = int(np.prod(nel))
+    rho, _, _ = pb.material()
+    scale = float(np.prod(dx)) * density / 8.0 / 3.0
+    m = np.zeros(3 * pb.nn)
+    for e in range(ne):
+        for nd in element_nodes(nel, e):
+            m[3 * nd:3 * nd + 3] += rho[e] * scale
+    if mlump is not None:
+        m += mlump
+    fm, _ = pb.get_bc()
+    fixed = ((fm[:, None] >> np.arange(3)) & 1).astype(bool).ravel()
+    m[fixed] = 1e-8
+    return m, scale
+
+
+def frequency_dense(pb, nel, nvals, density, p=8.0, dx=(1.0, 1.0, 1.0),
+                    E0=1.0, nu=0.3, mlump=None):
+    """Frequency::Function (Dynamic.cpp:18-171) by a dense generalized
+    eigensolve (small problems only): the largest eigenvalues of
+    M phi = lambda K phi, more than nvals of them until the last is
+    separated from the one before it by a relative 1e-5 (UNIQUE_LAST_NEV,
+    EigenPeetz.cpp:310-312); value = (sum lambda^p)^(1/p) over all of them;
+    the gradient sums the first nvals - 1 pairs (:127-160),
+    lambda_j^(p-1) phi_j^T (dMdy - lambda_j dKdy) phi_j per element (dMdy =
+    dVdrho * the element mass, dKdy = dEdz K0), times value^(1-p), then
+    P^T.  Returns (lambda, value, dvdx, dlam) with dlam[j] = d lambda_j /
+    d rho (before the filter) for every pair."""
+    import scipy.linalg as sla
+    nel = tuple(int(v) for v in nel)
+    ne = int(np.prod(nel))
+    m, scale = lumped_mass(pb, nel, density, dx, mlump)
+    K = dense(pb.apply, 3 * pb.nn)
+    w, v = sla.eigh(np.diag(m), 0.5 * (K + K.T))
+    order = np.argsort(w)[::-1]
+    nev = nvals + 1
+    while abs(1.0 - w[order[nev - 2]] / w[order[nev - 1]]) <= 1e-5:
+        nev += 1
+    lam = w[order[:nev]]
+    phi = v[:, order[:nev]].T
+    nodes = np.array([element_nodes(nel, e) for e in range(ne)])
+    dofs = (3 * nodes[:, :, None] + np.arange(3)).reshape(ne, 24)
+    _, _, dEdz = pb.material()
+    K0 = element_stiffness(dx, E0, nu)
+    Pe = phi[:, dofs]
+    pmp = scale * np.sum(Pe * Pe, axis=2)
+    pkp = dEdz[None] * np.einsum("kei,ij,kej->ke", Pe, K0, Pe)
+    dlam = pmp - lam[:, None] * pkp
+    value = float(np.sum(lam ** p) ** (1.0 / p))
+    nt = max(0, nvals - 1)
+    g = np.sum(lam[:nt, None] ** (p - 1) * dlam[:nt], axis=0) * value ** (1.0 - p)
+    return lam, value, pb.filter(g, transpose=True), dlam
+
+
 def oc_update(x, dfdx, g, dgdx, move, xmin=None, xmax=None):
     """MMA::OCsub (MMA.cpp:103-180); returns (x_new, change)."""
     n = x.size

@@ -34,7 +34,7 @@ EXPORTS = (
     "tpo_set_vector", "tpo_compliance", "tpo_volume", "tpo_filter",
     "tpo_oc_update", "tpo_sync", "tpo_set_stream", "tpo_kernel_launches",
     "tpo_sensitivity_noalloc", "tpo_default_eig_opts", "tpo_ks_assemble",
-    "tpo_ks_apply", "tpo_buckling", "tpo_buckling_sensitivity",
+    "tpo_ks_apply", "tpo_buckling", "tpo_buckling_sensitivity", "tpo_frequency",
 )
 NOALLOC_MAX_ELEMS = 1 << 20
 
@@ -133,6 +133,8 @@ def load(path: str | None = None):
         "tpo_buckling_sensitivity": (C.c_int, [vp, i32, dp, vp, d, C.POINTER(SolveOpts),
                                                dp, vp, vp, C.c_int,
                                                C.POINTER(SolveInfo)]),
+        "tpo_frequency": (C.c_int, [vp, i32, d, vp, C.POINTER(EigOpts), d, dp,
+                                    C.POINTER(i32), dp, vp, C.c_int, C.POINTER(EigInfo)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -207,7 +207,7 @@ void free_all(Ctx &c) {
   dfree(c.Ainv); dfree(c.Adense); dfree(c.solver_work); dfree(c.dev_info);
   dfree(c.finv); dfree(c.taps_d);
   dfree(c.w64);
-  dfree(c.Es64); dfree(c.dEsdz64); dfree(c.bk_buf); c.bk_n = 0; dfree(c.ks_S); dfree(c.ks_H); dfree(c.eig_buf);
+  dfree(c.Es64); dfree(c.dEsdz64); dfree(c.bk_buf); c.bk_n = 0; dfree(c.fq_buf); c.fq_n = 0; dfree(c.ks_S); dfree(c.ks_H); dfree(c.eig_buf);
   c.eig_n = 0;
   if (c.cublas) cublasDestroy(static_cast<cublasHandle_t>(c.cublas));
   c.cublas = nullptr;
@@ -852,6 +852,53 @@ int tpo_buckling_sensitivity(tpo_ctx *ctx, int32_t nev, const double *lambda,
   if (dvdrho)
     if (int rc2 = copy_out(c, dvdrho, g, ne, mem)) return rc2;
   CK(cudaStreamSynchronize(c.stream));
+  return finish(c, rc);
+}
+
+int tpo_frequency(tpo_ctx *ctx, int32_t nvals, double density, const double *mlump,
+                  const tpo_eig_opts *opts, double p, double *lambda, int32_t *nconv,
+                  double *value, double *dvdx, int mem, tpo_eig_info *info) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = check_mem(c, mem)) return rc;
+  tpo_eig_opts o;
+  if (opts) o = *opts; else tpo_default_eig_opts(&o);
+  REQUIRE(lambda && nconv && value, "null lambda, nconv or value");
+  REQUIRE(c.assembled, "tpo_fe_assemble must be called first (K and preconditioner)");
+  REQUIRE(nvals >= 1 && nvals + 3 <= tpo::kMaxEigPairs, "need 1 <= nvals <= 29");
+  REQUIRE(std::isfinite(density) && density > 0.0, "density must be positive");
+  REQUIRE(std::isfinite(p) && p >= 1.0, "the aggregation power p must be >= 1");
+  REQUIRE(o.tol > 0 && o.maxit >= 0, "invalid tol/maxit");
+  REQUIRE(o.precond == TPO_PREC_FP64 || o.precond == TPO_PREC_MIXED, "invalid precond");
+  const size_t n = 3 * c.nn, ne = c.ne;
+  const size_t need = n + tpo::kMaxEigPairs * n + 2 * ne + n;
+  if (c.fq_n < need) {
+    dfree(c.fq_buf);
+    c.fq_n = 0;
+    CK(cudaMalloc(&c.fq_buf, sizeof(double) * need));
+    c.fq_n = need;
+  }
+  double *mdiag = c.fq_buf, *phi = mdiag + n, *g = phi + tpo::kMaxEigPairs * n,
+         *dx = g + ne, *ml = dx + ne;
+  const double *mld = mlump;
+  if (mlump && mem != TPO_MEM_DEVICE) {
+    CK(cudaMemcpyAsync(ml, mlump, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream));
+    mld = ml;
+  }
+  double lam[tpo::kMaxEigPairs] = {0.0};
+  int nc = 0;
+  tpo_eig_info one{};
+  double *dout = dvdx ? (mem == TPO_MEM_DEVICE ? dvdx : dx) : nullptr;
+  const int rc = tpo::frequency(c, nvals, density, mld, o, p, lam, &nc, mdiag, phi, g,
+                                dout, value, &one);
+  if (info) *info = one;
+  if (rc < 0 && rc != TPO_E_BREAKDOWN) return finish(c, rc);
+  *nconv = nc;
+  for (int k = 0; k < nc; ++k) lambda[k] = lam[k];
+  if (dvdx && mem != TPO_MEM_DEVICE) {
+    if (int rc2 = copy_out(c, dvdx, dx, ne, mem)) return rc2;
+    CK(cudaStreamSynchronize(c.stream));
+  }
   return finish(c, rc);
 }
 

@@ -64,6 +64,14 @@ __global__ void k_eig_start(int64_t n, int m, const uint8_t *__restrict__ fix,
   }
 }
 
+// AV = diag(d) V on m columns (the lumped mass of the frequency problem)
+__global__ void k_diag_apply(int64_t n, int m, const double *__restrict__ d,
+                             const double *__restrict__ V, double *__restrict__ AV) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * m;
+       t += (int64_t)gridDim.x * blockDim.x)
+    AV[t] = d[t % n] * V[t];
+}
+
 // zero the fixed dofs of m columns
 __global__ void k_mask(int64_t n, int m, const uint8_t *__restrict__ fix,
                        double *X) {
@@ -242,7 +250,7 @@ static int precondition(Ctx &c, const tpo_solve_opts &so, int precision,
 }
 
 int buckling(Ctx &c, const tpo_eig_opts &o, double *lambda, double *phi,
-             int phi_mem, tpo_eig_info *info) {
+             int phi_mem, tpo_eig_info *info, const double *adiag) {
   const double t0 = now_ms();
   const int64_t n = 3 * c.nn;
   const int m = o.block, nev = o.nev;
@@ -279,7 +287,12 @@ int buckling(Ctx &c, const tpo_eig_opts &o, double *lambda, double *phi,
   tpo_solve_opts so = c.setup_opts;
 
   auto applyAB = [&](const double *V, double *AV, double *BV) {
-    launch_ks_apply(c, V, AV, m);
+    if (adiag) {
+      count_launch();
+      k_diag_apply<<<grid_for(n * m, 256), 256, 0, s>>>(n, m, adiag, V, AV);
+    } else {
+      launch_ks_apply(c, V, AV, m);
+    }
     for (int j0 = 0; j0 < m;) {
       const int nb = std::min(m - j0, kMaxBatch);
       launch_apply_fine<double>(c, c.E64, V + j0 * n, nullptr, BV + j0 * n, s, nb);
@@ -507,6 +520,55 @@ int buckling_sensitivity(Ctx &c, int nev, const double *lam, const double *phi, 
   acc.setup_ms = c.setup_ms;
   if (info) *info = acc;
   return worst;
+}
+
+// Frequency::Function (Dynamic.cpp:18-171) with DiagMassFnc (:181-235):
+// the lumped mass diagonal (into mdiag), the largest eigenvalues of
+// M phi = lambda K phi until more than nvals have converged and the last is
+// separated from the one before it by a relative 1e-5 (UNIQUE_LAST_NEV,
+// EigenPeetz.cpp:310-312), value = (sum over all of them lambda^p)^(1/p)
+// and, when dvdx is given, its gradient over the first nvals - 1 pairs, as
+// the reference sums them (:127-160), then the filter chain rule.  phi:
+// device scratch of 32 columns of 3 nn.
+int frequency(Ctx &c, int nvals, double density, const double *mlump,
+              const tpo_eig_opts &o_in, double p, double *lambda, int *nconv,
+              double *mdiag, double *phi, double *g, double *dvdx, double *value,
+              tpo_eig_info *info) {
+  cudaStream_t s = c.stream;
+  const double mscale = c.prm.dx[0] * c.prm.dx[1] * c.prm.dx[2] * density / 8.0 / 3.0;
+  launch_lumped_mass(c, mscale, mlump, mdiag, s);
+  CK(cudaGetLastError());
+  tpo_eig_opts o = o_in;
+  int nev = nvals + 1, rc = TPO_OK;
+  tpo_eig_info one{};
+  for (;;) {
+    o.nev = nev;
+    o.block = std::min(kMaxEigPairs, std::max(o_in.block, nev + 2));
+    rc = buckling(c, o, lambda, phi, TPO_MEM_DEVICE, &one, mdiag);
+    if (rc < 0 && rc != TPO_E_BREAKDOWN) return rc;
+    const bool separated = std::fabs(1.0 - lambda[nev - 2] / lambda[nev - 1]) > 1e-5;
+    if (separated || rc != TPO_OK || nev + 2 > kMaxEigPairs) break;
+    ++nev;
+  }
+  *nconv = nev;
+  double sum = 0.0;
+  for (int k = 0; k < nev; ++k) sum += std::pow(lambda[k], p);
+  *value = std::pow(sum, 1.0 / p);
+  if (dvdx) {
+    BkCoef coef{};
+    const int nterms = std::max(0, nvals - 1);
+    for (int k = 0; k < nterms; ++k) {
+      coef.a[k] = std::pow(lambda[k], p - 1.0);
+      coef.lam[k] = lambda[k];
+    }
+    coef.scale = std::pow(*value, 1.0 - p);
+    launch_freq_gradient(c, phi, 3 * c.nn, nterms, mscale, coef, g, s);
+    launch_filter(c, g, dvdx, true, s);
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(s));
+  if (info) *info = one;
+  return rc;
 }
 
 }  // namespace tpo

@@ -387,6 +387,90 @@ __global__ void k_bk_gradient(int nelx, int nely, int nelz,
   }
 }
 
+// ---- frequency (Dynamic.cpp:18-235)
+
+// Frequency::DiagMassFnc (:181-235) with the fixed-dof zeroing (:42-44):
+// m[3n + c] = sum over the elements around n of V_e * scale, scale =
+// elemSize * density / (2^3 * 3), plus the point masses mlump; 1e-8 at
+// fixed dofs (MatZeroRowsColumns with diagonal 1e-8 after the assembly)
+__global__ void k_lumped_mass(int nelx, int nely, int nelz,
+                              const double *__restrict__ V, double scale,
+                              const uint8_t *__restrict__ fix,
+                              const double *__restrict__ mlump,
+                              double *__restrict__ m) {
+  const int Nx = nelx + 1, Ny = nely + 1, Nz = nelz + 1;
+  const int64_t nn = (int64_t)Nx * Ny * Nz;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
+       n += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(n % Nx), j = (int)((n / Nx) % Ny), k = (int)(n / ((int64_t)Nx * Ny));
+    double acc = 0.0;
+#pragma unroll
+    for (int cz = 0; cz < 2; ++cz)
+#pragma unroll
+      for (int cy = 0; cy < 2; ++cy)
+#pragma unroll
+        for (int cx = 0; cx < 2; ++cx) {
+          const int ei = i - 1 + cx, ej = j - 1 + cy, ek = k - 1 + cz;
+          if (ei < 0 || ej < 0 || ek < 0 || ei >= nelx || ej >= nely || ek >= nelz)
+            continue;
+          acc += V[((int64_t)ek * nely + ej) * nelx + ei] * scale;
+        }
+    const unsigned f = fix[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      m[3 * n + c] = ((f >> c) & 1u) ? 1e-8 : acc + (mlump ? mlump[3 * n + c] : 0.0);
+  }
+}
+
+// g_e = scale sum_{k < nterms} a_k (dVdrho_e mscale |phi_e|^2
+//                                   - lam_k dEdz_e phi^T K0 phi)   (:127-160)
+// with dVdrho = 1 (V = rho, Material_Interpolation.cpp:63-64)
+__global__ void k_freq_gradient(int nelx, int nely, int nelz,
+                                const double *__restrict__ phi, int64_t ld, int nterms,
+                                const double *__restrict__ dEdz,
+                                const double *__restrict__ K0, double mscale,
+                                BkCoef coef, double *__restrict__ g) {
+  const int Nx = nelx + 1, Ny = nely + 1;
+  const int64_t ne = (int64_t)nelx * nely * nelz;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e % nelx), j = (int)((e / nelx) % nely),
+              k = (int)(e / ((int64_t)nelx * nely));
+    const int64_t n0 = ((int64_t)k * Ny + j) * Nx + i;
+    int64_t node[8];
+#pragma unroll
+    for (int l = 0; l < 8; ++l)
+      node[l] = n0 + (l & 1) + ((l >> 1) & 1) * Nx + ((l >> 2) & 1) * (int64_t)Nx * Ny;
+    const double de = dEdz[e];
+    double acc = 0.0;
+#pragma unroll 1
+    for (int kk = 0; kk < nterms; ++kk) {
+      const double *pk = phi + kk * ld;
+      double p[8][3];
+      double pp = 0.0;
+#pragma unroll
+      for (int l = 0; l < 8; ++l)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          p[l][c] = pk[3 * node[l] + c];
+          pp += p[l][c] * p[l][c];
+        }
+      double pkp = 0.0;
+#pragma unroll
+      for (int r = 0; r < 24; ++r) {
+        double s = 0.0;
+#pragma unroll
+        for (int l = 0; l < 8; ++l)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) s += __ldg(K0 + r * 24 + 3 * l + c) * p[l][c];
+        pkp += p[r / 3][r % 3] * s;
+      }
+      acc += coef.a[kk] * (mscale * pp - coef.lam[kk] * de * pkp);
+    }
+    g[e] = coef.scale * acc;
+  }
+}
+
 template <int NB>
 void ks_launch(const Ctx &c, const double *u, double *y) {
   count_launch();
@@ -419,6 +503,21 @@ void launch_bk_gradient(const Ctx &c, const double *phi, const double *v, int64_
   k_bk_gradient<<<grid_for(c.ne, 128), 128, 0, s>>>(c.nel[0], c.nel[1], c.nel[2], c.U,
                                                      phi, v, ld, nev, c.dEdz, c.dEsdz64,
                                                      c.ksc, c.K0lex, coef, g);
+}
+
+void launch_lumped_mass(const Ctx &c, double scale, const double *mlump, double *m,
+                        cudaStream_t s) {
+  count_launch();
+  k_lumped_mass<<<grid_for(c.nn, 128), 128, 0, s>>>(c.nel[0], c.nel[1], c.nel[2], c.rho,
+                                                     scale, c.fix, mlump, m);
+}
+
+void launch_freq_gradient(const Ctx &c, const double *phi, int64_t ld, int nterms,
+                          double mscale, const BkCoef &coef, double *g, cudaStream_t s) {
+  count_launch();
+  k_freq_gradient<<<grid_for(c.ne, 128), 128, 0, s>>>(c.nel[0], c.nel[1], c.nel[2], phi, ld,
+                                                       nterms, c.dEdz, c.K0lex, mscale,
+                                                       coef, g);
 }
 
 void launch_ks_apply(const Ctx &c, const double *u, double *y, int nb) {

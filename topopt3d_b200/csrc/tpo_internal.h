@@ -208,6 +208,8 @@ struct Ctx {
   size_t eig_n = 0;
   double *bk_buf = nullptr;   // buckling-sensitivity workspace
   size_t bk_n = 0;
+  double *fq_buf = nullptr;   // frequency workspace
+  size_t fq_n = 0;
 
   // CUDA graphs of the CG iteration bodies, keyed on (x, columns)
   cudaGraphExec_t graph64 = nullptr, graph32 = nullptr;
@@ -393,6 +395,12 @@ struct BkCoef {
 // d(phi^T ks_e phi)/du_e (W: 24 x nElem scratch), zero at fixed dofs
 void launch_bk_adj_rhs(const Ctx &c, const double *phi, double *W, double *rhs,
                        cudaStream_t s);
+// frequency (kernels_ks.cu): the lumped mass diagonal m (3 nn) from c.rho,
+// and the gradient g_e from nterms eigenvector columns (stride ld)
+void launch_lumped_mass(const Ctx &c, double scale, const double *mlump, double *m,
+                        cudaStream_t s);
+void launch_freq_gradient(const Ctx &c, const double *phi, int64_t ld, int nterms,
+                          double mscale, const BkCoef &coef, double *g, cudaStream_t s);
 // g_e, the gradient before the filter chain rule, from c.U and nev columns
 // of phi and the adjoint solutions v (stride ld)
 void launch_bk_gradient(const Ctx &c, const double *phi, const double *v, int64_t ld,

@@ -325,6 +325,35 @@ class TopOpt:
         self.last_adjoint = info.as_dict()
         return (value.value, dvdx, drho) if want_drho else (value.value, dvdx)
 
+    def frequency(self, nvals, density, mlump=None, p=8.0, gradient=False, opts=None,
+                  **kw):
+        """Frequency::Function (Dynamic.cpp:18-171): the largest eigenvalues
+        of M phi = lambda K phi with the lumped mass of DiagMassFnc (lambda =
+        1/omega^2), more than nvals of them until the last is separated
+        (UNIQUE_LAST_NEV); returns (lambda descending, value) or, with
+        gradient, (lambda, value, dvalue/dx).  The solver record is kept in
+        last_eig."""
+        o = opts or L.default_eig_opts(**kw)
+        lam = np.zeros(32)
+        ncv = C.c_int32(0)
+        value = C.c_double(0.0)
+        ml, mem, keep = _buf(mlump, 3 * self.nNode)
+        if gradient:
+            dvdx = (mlump.new_zeros(self.nElem) if _is_torch(mlump) and mem == L.MEM_DEVICE
+                    else np.zeros(self.nElem))
+            dp_ = C.c_void_p(dvdx.data_ptr() if _is_torch(dvdx) else dvdx.ctypes.data)
+        else:
+            dvdx, dp_ = None, None
+        info = L.EigInfo()
+        rc = self._check(self._lib.tpo_frequency(
+            self._h, int(nvals), float(density), ml, C.byref(o), float(p),
+            lam.ctypes.data_as(C.POINTER(C.c_double)), C.byref(ncv), C.byref(value),
+            dp_, mem, C.byref(info)), "frequency")
+        self.last_eig = info.as_dict()
+        self.last_eig["rc"] = rc
+        lam = lam[:ncv.value].copy()
+        return (lam, value.value, dvdx) if gradient else (lam, value.value)
+
     def volume(self, gradient=True):
         v = C.c_double()
         dv = np.zeros(self.nElem) if gradient else None
@@ -428,6 +457,26 @@ class Stability(Function_Base):
             self.lam = topOpt.buckling(nev=self.nev, block=self.block)
             self.values[0] = float(np.sum(self.lam ** p) ** (1.0 / p))
             self.gradients = None
+
+
+class Frequency(Function_Base):
+    """Frequency::Function (Dynamic.cpp:18-171): the largest eigenvalues of
+    M phi = lambda K phi (the lowest natural frequencies, lambda =
+    1/omega^2) with the lumped mass of DiagMassFnc, aggregated as
+    (sum lambda^p)^(1/p), p = 8, and with calc_gradient its design gradient
+    (no adjoint solve: K and M do not depend on U)."""
+
+    def __init__(self, values, min_val, max_val, objective=True,
+                 calc_gradient=True, nvals=4, density=1.0, block=12):
+        super().__init__(values, min_val, max_val, objective, calc_gradient)
+        self.nvals, self.density, self.block = nvals, density, block
+        self.lam = None
+
+    def Function(self, topOpt):
+        r = topOpt.frequency(self.nvals, self.density, gradient=self.calc_gradient,
+                             block=self.block)
+        self.lam, self.values[0] = r[0], r[1]
+        self.gradients = r[2] if self.calc_gradient else None
 
 
 @dataclass
