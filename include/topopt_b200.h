@@ -243,6 +243,37 @@ TPO_API int tpo_frequency(tpo_ctx *ctx, int32_t nvals, double density, const dou
                   const tpo_eig_opts *opts, double p, double *lambda, int32_t *nconv,
                   double *value, double *dvdx, int mem, tpo_eig_info *info);
 
+/* ---- MMA for two or more constraints (MMA.cpp:185-595) ----------------- */
+
+typedef struct {
+  double move;        /* step limit (0.5) */
+  double asyinit;     /* asymptote parameters (0.5, 1.2, 0.7) */
+  double asyincr;
+  double asydecr;
+  double albefa;      /* move-limit factor towards the asymptotes (0.1) */
+  double raa0;        /* objective regularisation (1e-5) */
+  double epsimin;     /* smallest epsilon of the dual Newton loop (1e-7) */
+} tpo_mma_opts;
+
+/* the defaults of MMA::Set_Defaults (MMA.h:21-23) */
+TPO_API void tpo_default_mma_opts(tpo_mma_opts *opts);
+/* MMA::MMAsub (MMA.cpp:185-343) with MMA::DualSolve (:353-595), the branch
+ * MMA::Update takes for m >= 2 constraints, over nElem design variables:
+ * asymptotes from x, xold1, xold2 (fresh while *fresh_start and iter < 3;
+ * *fresh_start is cleared once not), the convex approximation, the dual
+ * Newton iteration on the m multipliers (the element passes on the GPU, the
+ * m x m steps on the host), then xold2 <- xold1 <- x, x <- the subproblem
+ * solution, *change = max |x - xold1| / (xmax - xmin).  x, xold1, xold2,
+ * low and upp are the caller's state, updated in place; xmin, xmax, dfdx
+ * (nElem) and dgdx (nElem x m, column-major) are read, all in `mem`; g (m)
+ * on the host.  The constants are Set_m's (a0 = b0 = 1, a = 0, c = 1000,
+ * d = 1); 1 <= m <= 8. */
+TPO_API int tpo_mma_update(tpo_ctx *ctx, const tpo_mma_opts *opts, int32_t iter,
+                   int32_t *fresh_start, int32_t m, double *x, double *xold1,
+                   double *xold2, double *low, double *upp, const double *xmin,
+                   const double *xmax, const double *dfdx, const double *g,
+                   const double *dgdx, double *change, int mem);
+
 /* U, F, x, rho, E, dEdz accessors: which = "U","F","x","rho","E","dEdz" */
 TPO_API int tpo_get_vector(const tpo_ctx *ctx, const char *which, double *out, int mem);
 TPO_API int tpo_set_vector(tpo_ctx *ctx, const char *which, const double *in, int mem);

@@ -480,6 +480,105 @@ def frequency_dense(pb, nel, nvals, density, p=8.0, dx=(1.0, 1.0, 1.0),
     return lam, value, pb.filter(g, transpose=True), dlam
 
 
+MMA_DEFAULTS = dict(move=0.5, asyinit=0.5, asyincr=1.2, asydecr=0.7, albefa=0.1,
+                    raa0=1e-5, epsimin=1e-7)   # MMA.h:21-23
+
+
+def mma_update(st, dfdx, g, dgdx, iter_, **opts):
+    """MMA::MMAsub (MMA.cpp:185-343) with MMA::DualSolve (:353-595) for
+    m = len(g) constraints, in numpy.  st holds x, xold1, xold2, low, upp,
+    xmin, xmax (n-vectors) and fresh_start; it is updated in place.  The
+    constants are Set_m's (:40-52): a0 = b0 = 1, a = 0, c = 1000, d = 1.
+    Returns Change."""
+    o = dict(MMA_DEFAULTS, **opts)
+    x, x1, x2 = st["x"], st["xold1"], st["xold2"]
+    xmin, xmax = st["xmin"], st["xmax"]
+    dgdx = np.asarray(dgdx, np.float64).reshape(x.size, -1)
+    g = np.asarray(g, np.float64).ravel()
+    m = g.size
+    a0, b0, a, c, d = 1.0, 1.0, np.zeros(m), 1000.0 * np.ones(m), np.ones(m)
+    span = xmax - xmin
+    if st["fresh_start"] and iter_ < 3:
+        low = x - o["asyinit"] * span
+        upp = x + o["asyinit"] * span
+    else:
+        st["fresh_start"] = False
+        zzz = (x - x1) * (x1 - x2)
+        factor = np.where(zzz > 0, o["asyincr"], np.where(zzz < 0, o["asydecr"], 1.0))
+        low = x - factor * (x1 - st["low"])
+        upp = x + factor * (st["upp"] - x1)
+        low = np.minimum(np.maximum(low, x - 10 * span), x - 0.01 * span)
+        upp = np.maximum(np.minimum(upp, x + 10 * span), x + 0.01 * span)
+    alfa = np.maximum(np.maximum(low + o["albefa"] * (x - low), x - o["move"] * span), xmin)
+    beta = np.minimum(np.minimum(upp - o["albefa"] * (upp - x), x + o["move"] * span), xmax)
+    xmami = np.maximum(upp - low, 1e-5)
+    ux1, xl1 = upp - x, x - low
+    ux2, xl2 = ux1 * ux1, xl1 * xl1
+    p0 = np.maximum(dfdx, 0.0)
+    q0 = np.maximum(-dfdx, 0.0)
+    pq0 = 0.001 * (p0 + q0) + 0.5 * o["raa0"] / xmami
+    p0 = (p0 + pq0) * ux2
+    q0 = (q0 + pq0) * xl2
+    P = np.maximum(dgdx, 0.0) * ux2[:, None]
+    Q = np.maximum(-dgdx, 0.0) * xl2[:, None]
+    b = np.sum(P / ux1[:, None] + Q / xl1[:, None], axis=0) - g
+    st["xold2"] = x1.copy()
+    st["xold1"] = x.copy()
+    st["low"], st["upp"] = low, upp
+
+    def xyz(lam):
+        plam, qlam = p0 + P @ lam, q0 + Q @ lam
+        pr, qr = np.sqrt(plam), np.sqrt(qlam)
+        xx = np.minimum(np.maximum((pr * low + qr * upp) / (pr + qr), alfa), beta)
+        y = np.maximum((lam - c) / d, 0.0)
+        z = 10 * max((lam @ a - a0) / b0, 0.0)
+        return xx, y, z, plam, qlam
+
+    def grad(xx, y, z):
+        return np.sum(P / (upp - xx)[:, None] + Q / (xx - low)[:, None], axis=0) - (b + a * z + y)
+
+    def hess(xx, lam, plam, qlam):
+        u1, l1 = upp - xx, xx - low
+        dhdx = (P / (u1 * u1)[:, None] - Q / (l1 * l1)[:, None]).T
+        inside = ((xx > alfa) & (xx < beta)).astype(np.float64)
+        dLdxx = inside / (2 * plam / u1 ** 3 + 2 * qlam / l1 ** 3)
+        H = -(dhdx * dLdxx) @ dhdx.T
+        H -= np.diag((lam > c).astype(np.float64))
+        if lam @ a > 0:
+            H -= 10 * np.outer(a, a)
+        return H
+
+    epsi = 1.0
+    eta = np.ones(m)
+    lam = 500 * eta
+    xx, y, z, plam, qlam = xyz(lam)
+    G = grad(xx, y, z)
+    while epsi > o["epsimin"]:
+        epsvec = np.full(m, epsi)
+        resmax = np.max(np.abs(np.concatenate([G + eta, eta * lam - epsvec])))
+        it = 0
+        while resmax > 0.9 * epsi and it < 100:
+            it += 1
+            H = hess(xx, lam, plam, qlam)
+            A = H - np.diag(eta / lam)
+            A += min(1e-4 * np.trace(A) / m, -1e-7) * np.eye(m)
+            dl = np.linalg.solve(A, -G - epsvec / lam)
+            de = -eta + epsvec / lam - dl * (eta / lam)
+            theta = 1.0
+            for r in (-0.99 * lam / dl, -0.99 * eta / de):
+                for v in r:
+                    if v >= 0:
+                        theta = min(theta, v)
+            lam = lam + theta * dl
+            eta = eta + theta * de
+            xx, y, z, plam, qlam = xyz(lam)
+            G = grad(xx, y, z)
+            resmax = np.max(np.abs(np.concatenate([G + eta, eta * lam - epsvec])))
+        epsi *= 0.1
+    st["x"] = xx
+    return float(np.max(np.abs((xx - st["xold1"]) / span)))
+
+
 def oc_update(x, dfdx, g, dgdx, move, xmin=None, xmax=None):
     """MMA::OCsub (MMA.cpp:103-180); returns (x_new, change)."""
     n = x.size

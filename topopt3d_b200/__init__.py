@@ -8,10 +8,10 @@ filter.  ``TopOpt`` mirrors the reference's call surface.
 from ._lib import (BC_LOAD, BC_SUPPORT, MEM_DEVICE, MEM_HOST, PREC_FP64,
                    PREC_MIXED, EigInfo, EigOpts, SolveInfo, SolveOpts,
                    default_eig_opts, default_opts, load)
-from .topopt import (OC, Compliance, Frequency, Function_Base, Stability, TopOpt,
+from .topopt import (MMA, OC, Compliance, Frequency, Function_Base, Stability, TopOpt,
                      TopOptError, Volume, optimize)
 
-__all__ = ["TopOpt", "TopOptError", "Compliance", "Volume", "Frequency", "Function_Base",
+__all__ = ["TopOpt", "TopOptError", "MMA", "Compliance", "Volume", "Frequency", "Function_Base",
            "OC", "optimize", "Stability", "EigOpts", "EigInfo",
            "default_eig_opts", "SolveOpts", "SolveInfo", "default_opts", "load",
            "PREC_FP64", "PREC_MIXED", "MEM_HOST", "MEM_DEVICE", "BC_SUPPORT",

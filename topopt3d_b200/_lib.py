@@ -35,6 +35,7 @@ EXPORTS = (
     "tpo_oc_update", "tpo_sync", "tpo_set_stream", "tpo_kernel_launches",
     "tpo_sensitivity_noalloc", "tpo_default_eig_opts", "tpo_ks_assemble",
     "tpo_ks_apply", "tpo_buckling", "tpo_buckling_sensitivity", "tpo_frequency",
+    "tpo_default_mma_opts", "tpo_mma_update",
 )
 NOALLOC_MAX_ELEMS = 1 << 20
 
@@ -66,6 +67,12 @@ class SolveInfo(C.Structure):
 class EigOpts(C.Structure):
     _fields_ = [("nev", C.c_int32), ("block", C.c_int32), ("maxit", C.c_int32),
                 ("tol", C.c_double), ("precond", C.c_int32), ("seed", C.c_uint64)]
+
+
+class MmaOpts(C.Structure):
+    _fields_ = [("move", C.c_double), ("asyinit", C.c_double), ("asyincr", C.c_double),
+                ("asydecr", C.c_double), ("albefa", C.c_double), ("raa0", C.c_double),
+                ("epsimin", C.c_double)]
 
 
 class EigInfo(C.Structure):
@@ -135,6 +142,9 @@ def load(path: str | None = None):
                                                C.POINTER(SolveInfo)]),
         "tpo_frequency": (C.c_int, [vp, i32, d, vp, C.POINTER(EigOpts), d, dp,
                                     C.POINTER(i32), dp, vp, C.c_int, C.POINTER(EigInfo)]),
+        "tpo_default_mma_opts": (None, [C.POINTER(MmaOpts)]),
+        "tpo_mma_update": (C.c_int, [vp, C.POINTER(MmaOpts), i32, C.POINTER(i32), i32,
+                                     vp, vp, vp, vp, vp, vp, vp, vp, dp, vp, dp, C.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -147,6 +157,16 @@ def load(path: str | None = None):
 def default_opts(**kw) -> SolveOpts:
     o = SolveOpts()
     load().tpo_default_solve_opts(C.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise AttributeError(k)
+        setattr(o, k, v)
+    return o
+
+
+def default_mma_opts(**kw) -> MmaOpts:
+    o = MmaOpts()
+    load().tpo_default_mma_opts(C.byref(o))
     for k, v in kw.items():
         if not hasattr(o, k):
             raise AttributeError(k)

@@ -252,6 +252,137 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// ---- MMA for m >= 2 constraints (MMA::MMAsub, MMA.cpp:185-343, and
+// MMA::DualSolve, :353-595).  Every element-wise pass reduces into
+// per-block partials over the fixed kRedBlocks grid (m values per block for
+// b, m + m(m+1)/2 for the dual gradient and Hessian); the host sums them in
+// a fixed order, so the result does not depend on scheduling.
+
+// sum of v over the block into out (thread 0), v a per-thread value
+__device__ __forceinline__ double block_total(double v, double *sh) {
+  v = warp_sum(v);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x < 32) {
+    t = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+    t = warp_sum(t);
+  }
+  return t;
+}
+
+// asymptotes (:219-247), move limits alfa/beta (:250-262), p0, q0, P, Q
+// (:265-300) and the partials of b (:303-305); then xold2 <- xold1 <- x
+// (:307).  P and Q are n x m column-major.
+__global__ void __launch_bounds__(256)
+    k_mma_prepare(int64_t n, int m, bool fresh, MmaConst k, double *x, double *x1,
+                  double *x2, double *low, double *upp, const double *xmin,
+                  const double *xmax, const double *dfdx, const double *dgdx,
+                  double *alfa, double *beta, double *p0, double *q0, double *P,
+                  double *Q, double *part) {
+  __shared__ double sh[32];
+  double bs[kMmaMaxM];
+  for (int j = 0; j < m; ++j) bs[j] = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double xi = x[i], span = xmax[i] - xmin[i];
+    double lo, up;
+    if (fresh) {
+      lo = xi - k.asyinit * span;
+      up = xi + k.asyinit * span;
+    } else {
+      const double xa = x1[i], xb = x2[i];
+      const double zz = (xi - xa) * (xa - xb);
+      const double f = zz > 0 ? k.asyincr : (zz < 0 ? k.asydecr : 1.0);
+      lo = xi - f * (xa - low[i]);
+      up = xi + f * (upp[i] - xa);
+      lo = fmin(fmax(lo, xi - 10 * span), xi - 0.01 * span);
+      up = fmax(fmin(up, xi + 10 * span), xi + 0.01 * span);
+    }
+    alfa[i] = fmax(fmax(lo + k.albefa * (xi - lo), xi - k.move * span), xmin[i]);
+    beta[i] = fmin(fmin(up - k.albefa * (up - xi), xi + k.move * span), xmax[i]);
+    const double xmami = fmax(up - lo, 1e-5);
+    const double ux1 = up - xi, xl1 = xi - lo, ux2 = ux1 * ux1, xl2 = xl1 * xl1;
+    const double df = dfdx[i];
+    double pp = fmax(df, 0.0), qq = fmax(-df, 0.0);
+    const double pq0 = 0.001 * (pp + qq) + 0.5 * k.raa0 / xmami;
+    p0[i] = (pp + pq0) * ux2;
+    q0[i] = (qq + pq0) * xl2;
+    for (int j = 0; j < m; ++j) {
+      const double dg = dgdx[j * n + i];
+      const double Pj = fmax(dg, 0.0) * ux2, Qj = fmax(-dg, 0.0) * xl2;
+      P[j * n + i] = Pj;
+      Q[j * n + i] = Qj;
+      bs[j] += Pj / ux1 + Qj / xl1;
+    }
+    low[i] = lo;
+    upp[i] = up;
+    x2[i] = x1[i];
+    x1[i] = xi;
+  }
+  for (int j = 0; j < m; ++j) {
+    const double t = block_total(bs[j], sh);
+    if (threadIdx.x == 0) part[blockIdx.x * m + j] = t;
+  }
+}
+
+// x(lambda) (XYZofLam, :432-447) and the partials of the dual gradient sums
+// sum_n P_j/ux1 + Q_j/xl1 (DualGrad, :461-474) and of the Hessian sums
+// sum_n dhdx_j dLdxx dhdx_k, k >= j (DualHess, :489-515), at lambda
+__global__ void __launch_bounds__(256)
+    k_mma_dual(int64_t n, int m, MmaLambda lam, const double *alfa, const double *beta,
+               const double *low, const double *upp, const double *p0,
+               const double *q0, const double *P, const double *Q, double *x,
+               double *part) {
+  __shared__ double sh[32];
+  const int nh = m * (m + 1) / 2, nv = m + nh;
+  double acc[kMmaMaxM + kMmaMaxM * (kMmaMaxM + 1) / 2];
+  for (int j = 0; j < nv; ++j) acc[j] = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double plam = p0[i], qlam = q0[i];
+    for (int j = 0; j < m; ++j) {
+      plam += P[j * n + i] * lam.v[j];
+      qlam += Q[j * n + i] * lam.v[j];
+    }
+    const double lo = low[i], up = upp[i], al = alfa[i], be = beta[i];
+    const double pr = sqrt(plam), qr = sqrt(qlam);
+    const double xi = fmax(fmin((pr * lo + qr * up) / (pr + qr), be), al);
+    x[i] = xi;
+    const double ux1 = up - xi, xl1 = xi - lo;
+    const double ux2 = ux1 * ux1, xl2 = xl1 * xl1;
+    const double inside = (xi > al && xi < be) ? 1.0 : 0.0;
+    const double dL = inside / (2 * plam / (ux2 * ux1) + 2 * qlam / (xl2 * xl1));
+    double dh[kMmaMaxM];
+    for (int j = 0; j < m; ++j) {
+      const double Pj = P[j * n + i], Qj = Q[j * n + i];
+      acc[j] += Pj / ux1 + Qj / xl1;
+      dh[j] = Pj / ux2 - Qj / xl2;
+    }
+    int t = m;
+    for (int j = 0; j < m; ++j)
+      for (int kk = j; kk < m; ++kk) acc[t++] += dh[j] * dL * dh[kk];
+  }
+  for (int j = 0; j < nv; ++j) {
+    const double s = block_total(acc[j], sh);
+    if (threadIdx.x == 0) part[blockIdx.x * nv + j] = s;
+  }
+}
+
+// Change = max |x - xold| / (xmax - xmin) (:309-310)
+__global__ void k_max_change(int64_t n, const double *x, const double *xold,
+                             const double *xmin, const double *xmax,
+                             unsigned long long *out) {
+  double mx = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    mx = fmax(mx, fabs((x[i] - xold[i]) / (xmax[i] - xmin[i])));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(mx));
+}
+
 // x < 1e-6 -> 0 (MMA.cpp:166-173), then Change = max |x - xold| / (xmax - xmin)
 __global__ void k_oc_finish(int64_t n, double *x, const double *xold,
                             const double *xmin, const double *xmax,
@@ -348,6 +479,33 @@ bool launch_oc_bisect(const Ctx &c, int64_t n, double *x, const double *xold,
   void *args[] = {&n, &x, &xold, &xmin, &xmax, &dfdx, &dgdx, &move, &g, &part, &bar, &fault};
   *err = cudaLaunchCooperativeKernel((const void *)k_oc_bisect, kRedBlocks, 256, args, 0, s);
   return true;
+}
+
+void launch_mma_prepare(int64_t n, int m, bool fresh, const MmaConst &k, double *x,
+                        double *x1, double *x2, double *low, double *upp,
+                        const double *xmin, const double *xmax, const double *dfdx,
+                        const double *dgdx, double *alfa, double *beta, double *p0,
+                        double *q0, double *P, double *Q, double *part, cudaStream_t s) {
+  count_launch();
+  k_mma_prepare<<<kRedBlocks, 256, 0, s>>>(n, m, fresh, k, x, x1, x2, low, upp, xmin, xmax,
+                                           dfdx, dgdx, alfa, beta, p0, q0, P, Q, part);
+}
+
+void launch_mma_dual(int64_t n, int m, const MmaLambda &lam, const double *alfa,
+                     const double *beta, const double *low, const double *upp,
+                     const double *p0, const double *q0, const double *P, const double *Q,
+                     double *x, double *part, cudaStream_t s) {
+  count_launch();
+  k_mma_dual<<<kRedBlocks, 256, 0, s>>>(n, m, lam, alfa, beta, low, upp, p0, q0, P, Q, x,
+                                        part);
+}
+
+void launch_max_change(int64_t n, const double *x, const double *xold, const double *xmin,
+                       const double *xmax, double *out, cudaStream_t s) {
+  count_launch();
+  cudaMemsetAsync(out, 0, sizeof(double), s);
+  k_max_change<<<grid_for(n, 256), 256, 0, s>>>(n, x, xold, xmin, xmax,
+                                                reinterpret_cast<unsigned long long *>(out));
 }
 
 void launch_oc_finish(const Ctx &c, int64_t n, double *x, const double *xold,

@@ -210,6 +210,9 @@ struct Ctx {
   size_t bk_n = 0;
   double *fq_buf = nullptr;   // frequency workspace
   size_t fq_n = 0;
+  double *mma_buf = nullptr;  // MMA workspace (device) and partials mirror
+  size_t mma_n = 0;
+  double *mma_h = nullptr;
 
   // CUDA graphs of the CG iteration bodies, keyed on (x, columns)
   cudaGraphExec_t graph64 = nullptr, graph32 = nullptr;
@@ -414,6 +417,26 @@ void launch_oc_step(const Ctx &c, int64_t n, double *x, const double *xold,
                     const double *dgdx, double move, double lmid, double *out,
                     cudaStream_t s);
 void launch_oc_clip(int64_t n, double *dfdx, cudaStream_t s);
+// MMA for m >= 2 constraints (kernels_design.cu): per-block partials over
+// kRedBlocks blocks (m for b; m + m(m+1)/2 for the dual gradient/Hessian)
+constexpr int kMmaMaxM = 8;
+struct MmaConst {
+  double move, asyinit, asyincr, asydecr, albefa, raa0;
+};
+struct MmaLambda {
+  double v[kMmaMaxM];
+};
+void launch_mma_prepare(int64_t n, int m, bool fresh, const MmaConst &k, double *x,
+                        double *x1, double *x2, double *low, double *upp,
+                        const double *xmin, const double *xmax, const double *dfdx,
+                        const double *dgdx, double *alfa, double *beta, double *p0,
+                        double *q0, double *P, double *Q, double *part, cudaStream_t s);
+void launch_mma_dual(int64_t n, int m, const MmaLambda &lam, const double *alfa,
+                     const double *beta, const double *low, const double *upp,
+                     const double *p0, const double *q0, const double *P, const double *Q,
+                     double *x, double *part, cudaStream_t s);
+void launch_max_change(int64_t n, const double *x, const double *xold, const double *xmin,
+                       const double *xmax, double *out, cudaStream_t s);
 // the whole OC bisection in one cooperative launch of kRedBlocks CTAs (uses
 // c.part, c.gbar and the fault slot); false when the device cannot hold
 // them all at once, and the caller runs the per-trial launches instead

@@ -526,6 +526,50 @@ class OC:
         return self.iter >= self.maxiter
 
 
+@dataclass
+class MMA(OC):
+    """MMA::Update (MMA.cpp:62-100): the OC branch for fewer than two
+    constraints (as OC), otherwise MMA::MMAsub with MMA::DualSolve
+    (:185-595) -- the element passes on the GPU, the dual Newton steps on
+    the host.  xold1, xold2, low and upp are the method's state; they start
+    from xval as MMA::Set_Values does.  opts: tpo_mma_opts fields (move is
+    taken from the dataclass field)."""
+    xold1: np.ndarray = None
+    xold2: np.ndarray = None
+    low: np.ndarray = None
+    upp: np.ndarray = None
+    fresh_start: bool = True
+    mma_opts: dict = field(default_factory=dict)
+
+    def Update(self, topOpt, dfdx, g, dgdx):
+        g = np.atleast_1d(np.asarray(g, np.float64))
+        if g.size < 2:
+            return super().Update(topOpt, dfdx, g, dgdx)
+        n = self.n
+        x = np.ascontiguousarray(self.xval, np.float64).copy()
+        if self.xold1 is None:
+            self.xold1, self.xold2 = x.copy(), x.copy()
+            self.low, self.upp = np.zeros(n), np.ones(n)
+        st = [np.ascontiguousarray(a, np.float64) for a in
+              (self.xold1, self.xold2, self.low, self.upp)]
+        df = np.ascontiguousarray(dfdx, np.float64)
+        dg = np.asfortranarray(np.asarray(dgdx, np.float64).reshape(n, g.size))
+        o = L.default_mma_opts(move=float(self.move), **self.mma_opts)
+        fresh = C.c_int32(1 if self.fresh_start else 0)
+        ch = C.c_double()
+        ptr = lambda a: a.ctypes.data_as(C.c_void_p)
+        topOpt._check(topOpt._lib.tpo_mma_update(
+            topOpt._h, C.byref(o), int(self.iter), C.byref(fresh), int(g.size), ptr(x),
+            ptr(st[0]), ptr(st[1]), ptr(st[2]), ptr(st[3]), ptr(self.xmin), ptr(self.xmax),
+            ptr(df), g.ctypes.data_as(C.POINTER(C.c_double)), ptr(dg), C.byref(ch),
+            L.MEM_HOST), "MMA update")
+        self.xold1, self.xold2, self.low, self.upp = st
+        self.fresh_start = bool(fresh.value)
+        self.xval = x
+        self.Change = ch.value
+        return x
+
+
 def optimize(topOpt, optmma, penalties=None, opts=None, callback=None):
     """The optimisation loop of Main.cpp:130-170: per penalty, MatIntFnc ->
     FEAssemble -> FESolve -> Function_Call, then Update + re-evaluate until
