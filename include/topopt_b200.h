@@ -261,8 +261,8 @@ TPO_API void tpo_default_mma_opts(tpo_mma_opts *opts);
  * MMA::Update takes for m >= 2 constraints, over nElem design variables:
  * asymptotes from x, xold1, xold2 (fresh while *fresh_start and iter < 3;
  * *fresh_start is cleared once not), the convex approximation, the dual
- * Newton iteration on the m multipliers (the element passes on the GPU, the
- * m x m steps on the host), then xold2 <- xold1 <- x, x <- the subproblem
+ * Newton iteration on the m multipliers (the whole update in one persistent
+ * GPU launch), then xold2 <- xold1 <- x, x <- the subproblem
  * solution, *change = max |x - xold1| / (xmax - xmin).  x, xold1, xold2,
  * low and upp are the caller's state, updated in place; xmin, xmax, dfdx
  * (nElem) and dgdx (nElem x m, column-major) are read, all in `mem`; g (m)
@@ -273,6 +273,9 @@ TPO_API int tpo_mma_update(tpo_ctx *ctx, const tpo_mma_opts *opts, int32_t iter,
                    double *xold2, double *low, double *upp, const double *xmin,
                    const double *xmax, const double *dfdx, const double *g,
                    const double *dgdx, double *change, int mem);
+/* the number of dual Newton steps (SearchDir solves) the last successful
+ * tpo_mma_update took */
+TPO_API int tpo_mma_last_info(const tpo_ctx *ctx, int32_t *newton_steps);
 
 /* U, F, x, rho, E, dEdz accessors: which = "U","F","x","rho","E","dEdz" */
 TPO_API int tpo_get_vector(const tpo_ctx *ctx, const char *which, double *out, int mem);

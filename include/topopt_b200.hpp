@@ -253,6 +253,66 @@ class Frequency : public Function_Base {
   }
 };
 
+// MMA (MMA.h:14-100): the optimiser object of the reference, on the GPU of
+// `t`.  Update (MMA.cpp:62-100) takes OCsub (OCeta = 0.5) for fewer than
+// two constraints and MMAsub with DualSolve otherwise, with Set_m's
+// constants a0 = b0 = 1, a = 0, c = 1000, d = 1.  dgdx is n x m
+// column-major, as an Eigen::MatrixXd stores it.
+class MMA {
+ private:
+  TopOpt &t_;
+  int m_ = 0;
+
+ public:
+  explicit MMA(TopOpt &t)
+      : t_(t), xval(t.nElem, 0.0), xold1(t.nElem, 0.0), xold2(t.nElem, 0.0),
+        low(t.nElem, 0.0), upp(t.nElem, 1.0), xmin(t.nElem, 0.0), xmax(t.nElem, 1.0) {
+    tpo_default_mma_opts(&opts);   // Set_Defaults (MMA.h:21-23)
+  }
+  void Set_Lower_Bound(std::vector<double> v) { xmin = std::move(v); }
+  void Set_Upper_Bound(std::vector<double> v) { xmax = std::move(v); }
+  void Set_Iter_Limit_Min(unsigned v) { miniter = v; }
+  void Set_Iter_Limit_Max(unsigned v) { maxiter = v; }
+  void Set_Change_Limit(double v) { minchange = v; }
+  void Set_Step_Limit(double v) { opts.move = v; }
+  void Set_Values(const std::vector<double> &x) { xval = xold1 = xold2 = x; }
+  void Set_It(unsigned it) { iter = it; }
+  void Restart() { fresh_start = true; }
+  std::vector<double> &Get_x() { return xval; }
+  unsigned &Get_It() { return iter; }
+  int64_t Get_n() const { return t_.nElem; }
+  int Get_m() const { return m_; }
+  bool Check() { return Check_Conv() || Check_It(); }
+  bool Check_Conv() const { return iter > miniter && Change < minchange; }
+  bool Check_It() { return ++iter >= maxiter; }
+
+  int Update(std::vector<double> dfdx, const std::vector<double> &g,
+             const std::vector<double> &dgdx) {
+    m_ = (int)g.size();
+    const int64_t n = t_.nElem;
+    if (m_ < 1 || (int64_t)dfdx.size() != n || (int64_t)dgdx.size() != n * m_ ||
+        (int64_t)xval.size() != n)
+      return TPO_E_ARG;
+    if (m_ < 2)
+      return tpo_oc_update(t_.handle(), xval.data(), xmin.data(), xmax.data(), dfdx.data(),
+                           g[0], dgdx.data(), opts.move, &Change, TPO_MEM_HOST);
+    int32_t fresh = fresh_start ? 1 : 0;
+    const int rc = tpo_mma_update(t_.handle(), &opts, (int32_t)iter, &fresh, m_, xval.data(),
+                                  xold1.data(), xold2.data(), low.data(), upp.data(),
+                                  xmin.data(), xmax.data(), dfdx.data(), g.data(),
+                                  dgdx.data(), &Change, TPO_MEM_HOST);
+    fresh_start = fresh != 0;
+    return rc;
+  }
+
+  tpo_mma_opts opts{};
+  std::vector<double> xval, xold1, xold2, low, upp, xmin, xmax;
+  double Change = 1.0;
+  unsigned iter = 0, miniter = 0, maxiter = 50;
+  double minchange = 0.0;
+  bool fresh_start = true;
+};
+
 }  // namespace tpo
 
 #endif  // TOPOPT_B200_HPP

@@ -487,7 +487,8 @@ MMA_DEFAULTS = dict(move=0.5, asyinit=0.5, asyincr=1.2, asydecr=0.7, albefa=0.1,
 def mma_update(st, dfdx, g, dgdx, iter_, **opts):
     """MMA::MMAsub (MMA.cpp:185-343) with MMA::DualSolve (:353-595) for
     m = len(g) constraints, in numpy.  st holds x, xold1, xold2, low, upp,
-    xmin, xmax (n-vectors) and fresh_start; it is updated in place.  The
+    xmin, xmax (n-vectors) and fresh_start; it is updated in place (and
+    newton_steps set to the number of dual Newton steps taken).  The
     constants are Set_m's (:40-52): a0 = b0 = 1, a = 0, c = 1000, d = 1.
     Returns Change."""
     o = dict(MMA_DEFAULTS, **opts)
@@ -553,12 +554,14 @@ def mma_update(st, dfdx, g, dgdx, iter_, **opts):
     lam = 500 * eta
     xx, y, z, plam, qlam = xyz(lam)
     G = grad(xx, y, z)
+    steps = 0
     while epsi > o["epsimin"]:
         epsvec = np.full(m, epsi)
         resmax = np.max(np.abs(np.concatenate([G + eta, eta * lam - epsvec])))
         it = 0
         while resmax > 0.9 * epsi and it < 100:
             it += 1
+            steps += 1
             H = hess(xx, lam, plam, qlam)
             A = H - np.diag(eta / lam)
             A += min(1e-4 * np.trace(A) / m, -1e-7) * np.eye(m)
@@ -576,6 +579,7 @@ def mma_update(st, dfdx, g, dgdx, iter_, **opts):
             resmax = np.max(np.abs(np.concatenate([G + eta, eta * lam - epsvec])))
         epsi *= 0.1
     st["x"] = xx
+    st["newton_steps"] = steps
     return float(np.max(np.abs((xx - st["xold1"]) / span)))
 
 

@@ -30,7 +30,26 @@ int main() {
   double sc = 0, sv = 0;
   for (double g : c.gradient) sc += g;
   for (double g : v.gradient) sv += g;
-  std::printf("%d %d %.15g %.15g %.15g %.15g\n", t.KUF_reason, t.info.iterations,
-              c.values0, v.values0, sc, sv);
+  // MMA::Update both ways: OCsub with the volume constraint alone, MMAsub
+  // with it and mean(x) <= 0.35 over the first half of the elements
+  const int64_t n = t.nElem, h = n / 2;
+  tpo::MMA oc(t);
+  oc.Set_Values(x);
+  if (oc.Update(c.gradient, {v.value}, v.gradient)) return 6;
+  double xh = 0, s_oc = 0, s_mma = 0;
+  for (int64_t e = 0; e < h; ++e) xh += x[e] / h;
+  std::vector<double> dg(2 * n, 0.0);
+  for (int64_t e = 0; e < n; ++e) dg[e] = v.gradient[e];
+  for (int64_t e = 0; e < h; ++e) dg[n + e] = 1.0 / h;
+  tpo::MMA mma(t);
+  mma.Set_Values(x);
+  if (mma.Update(c.gradient, {v.value, xh - 0.35}, dg) || mma.Get_m() != 2) return 7;
+  for (int64_t e = 0; e < n; ++e) {
+    s_oc += oc.Get_x()[e];
+    s_mma += mma.Get_x()[e];
+  }
+  std::printf("%d %d %.15g %.15g %.15g %.15g %.15g %.15g %.15g %.15g\n", t.KUF_reason,
+              t.info.iterations, c.values0, v.values0, sc, sv, oc.Change, s_oc, mma.Change,
+              s_mma);
   return t.KUF_reason == 0 ? 0 : 1;
 }

@@ -1,5 +1,6 @@
 """The C++ host mirror (include/topopt_b200.hpp) compiles against the C ABI
-and, on a GPU, reproduces the oracle's compliance and volume."""
+and, on a GPU, reproduces the oracle's compliance and volume, and its MMA
+object's update (the OCsub branch with one constraint, MMAsub with two)."""
 import os
 import subprocess
 
@@ -31,7 +32,7 @@ def test_cpp_mirror_compiles(tmp_path):
 def test_cpp_mirror_matches_oracle(tmp_path, oracle):
     exe = build_mirror(tmp_path)
     out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout
-    st, its, C, V, sc, sv = out.split()
+    st, its, C, V, sc, sv, ch_oc, s_oc, ch_mma, s_mma = out.split()
     nel = (12, 6, 6)
     ref = oracle.Problem(nel, rmin=1.5, mg_levels=2)
     P.apply_bcs(ref, P.cantilever_bcs(nel))
@@ -47,3 +48,17 @@ def test_cpp_mirror_matches_oracle(tmp_path, oracle):
     assert abs(float(sc) - dco.sum()) < 1e-7 * abs(dco.sum())
     # constraint gradient = dV/dx / (max - min)
     assert abs(float(sv) - dvo.sum()) < 1e-12
+    x = 0.1 + 0.9 * ((e * 7919) % 101) / 100.0
+    x_oc, c_oc = oracle.oc_update(x, dco, Vo - 0.3, dvo, 0.5)
+    assert abs(float(ch_oc) - c_oc) < 1e-9
+    assert abs(float(s_oc) - x_oc.sum()) < 1e-7
+    n = x.size
+    h = n // 2
+    d2 = np.zeros(n)
+    d2[:h] = 1.0 / h
+    st_o = {"x": x.copy(), "xold1": x.copy(), "xold2": x.copy(), "low": np.zeros(n),
+            "upp": np.ones(n), "xmin": np.zeros(n), "xmax": np.ones(n), "fresh_start": True}
+    c_mma = oracle.mma_update(st_o, dco, np.array([Vo - 0.3, x[:h].mean() - 0.35]),
+                              np.stack([dvo, d2], axis=1), 0)
+    assert abs(float(ch_mma) - c_mma) < 1e-9
+    assert abs(float(s_mma) - st_o["x"].sum()) < 1e-7

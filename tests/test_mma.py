@@ -7,7 +7,8 @@ finds.
 
 GPU: tpo_mma_update against the oracle for consecutive updates on the same
 random data (the fresh asymptotes of the first iterations and the adaptive
-ones after), and a compliance problem with two volume constraints through
+ones after), with the same number of dual Newton steps, and a compliance
+problem with two volume constraints through
 `optimize` against the same loop over the oracle.
 """
 import numpy as np
@@ -84,6 +85,7 @@ def test_mma_update_matches_oracle(T, oracle, m):
         np.testing.assert_allclose(mm.xold1, st_o["xold1"], rtol=0, atol=1e-9)
         assert abs(mm.Change - ch_o) <= 1e-9
         assert mm.fresh_start == st_o["fresh_start"]
+        assert mm.newton_steps == st_o["newton_steps"] > 0
 
 
 @pytest.mark.gpu

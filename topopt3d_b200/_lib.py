@@ -35,7 +35,7 @@ EXPORTS = (
     "tpo_oc_update", "tpo_sync", "tpo_set_stream", "tpo_kernel_launches",
     "tpo_sensitivity_noalloc", "tpo_default_eig_opts", "tpo_ks_assemble",
     "tpo_ks_apply", "tpo_buckling", "tpo_buckling_sensitivity", "tpo_frequency",
-    "tpo_default_mma_opts", "tpo_mma_update",
+    "tpo_default_mma_opts", "tpo_mma_update", "tpo_mma_last_info",
 )
 NOALLOC_MAX_ELEMS = 1 << 20
 
@@ -145,6 +145,7 @@ def load(path: str | None = None):
         "tpo_default_mma_opts": (None, [C.POINTER(MmaOpts)]),
         "tpo_mma_update": (C.c_int, [vp, C.POINTER(MmaOpts), i32, C.POINTER(i32), i32,
                                      vp, vp, vp, vp, vp, vp, vp, vp, dp, vp, dp, C.c_int]),
+        "tpo_mma_last_info": (C.c_int, [vp, C.POINTER(i32)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

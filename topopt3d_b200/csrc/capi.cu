@@ -915,33 +915,6 @@ void tpo_default_mma_opts(tpo_mma_opts *o) {
   o->epsimin = 1e-7;
 }
 
-namespace {
-// x = A^-1 b for a small dense m x m system (row-major A, partial pivoting)
-bool solve_small(std::vector<double> A, std::vector<double> b, int m, double *x) {
-  for (int k = 0; k < m; ++k) {
-    int p = k;
-    for (int r = k + 1; r < m; ++r)
-      if (std::fabs(A[r * m + k]) > std::fabs(A[p * m + k])) p = r;
-    if (A[p * m + k] == 0.0) return false;
-    if (p != k) {
-      for (int cc = 0; cc < m; ++cc) std::swap(A[k * m + cc], A[p * m + cc]);
-      std::swap(b[k], b[p]);
-    }
-    for (int r = k + 1; r < m; ++r) {
-      const double f = A[r * m + k] / A[k * m + k];
-      for (int cc = k; cc < m; ++cc) A[r * m + cc] -= f * A[k * m + cc];
-      b[r] -= f * b[k];
-    }
-  }
-  for (int k = m - 1; k >= 0; --k) {
-    double s = b[k];
-    for (int cc = k + 1; cc < m; ++cc) s -= A[k * m + cc] * x[cc];
-    x[k] = s / A[k * m + k];
-  }
-  return true;
-}
-}  // namespace
-
 int tpo_mma_update(tpo_ctx *ctx, const tpo_mma_opts *opts, int32_t iter,
                    int32_t *fresh_start, int32_t m, double *x, double *xold1,
                    double *xold2, double *low, double *upp, const double *xmin,
@@ -959,8 +932,8 @@ int tpo_mma_update(tpo_ctx *ctx, const tpo_mma_opts *opts, int32_t iter,
   REQUIRE(o.epsimin > 0 && o.epsimin < 1, "epsimin must lie in (0, 1)");
   const int64_t n = c.ne;
   const int nv = m + m * (m + 1) / 2;
-  const size_t npart = (size_t)tpo::kRedBlocks * nv;
-  const size_t need = 4 * n + 2 * n * m + 8 * n + n * m + npart + 1;
+  const size_t npart = 2 * (size_t)tpo::kRedBlocks * nv;
+  const size_t need = 4 * n + 2 * n * m + 8 * n + n * m + npart + 4;
   cudaStream_t s = c.stream;
   if (c.mma_n < need) {
     dfree(c.mma_buf);
@@ -968,11 +941,9 @@ int tpo_mma_update(tpo_ctx *ctx, const tpo_mma_opts *opts, int32_t iter,
     CK(cudaMalloc(&c.mma_buf, sizeof(double) * need));
     c.mma_n = need;
   }
-  if (!c.mma_h)
-    CK(cudaMallocHost(&c.mma_h, sizeof(double) * tpo::kRedBlocks *
-                                    (tpo::kMmaMaxM + tpo::kMmaMaxM * (tpo::kMmaMaxM + 1) / 2)));
+  if (!c.mma_h) CK(cudaMallocHost(&c.mma_h, sizeof(double) * 4));
   double *alfa = c.mma_buf, *beta = alfa + n, *p0 = beta + n, *q0 = p0 + n, *P = q0 + n,
-         *Q = P + n * m, *st = Q + n * m, *part = st + 8 * n + n * m, *chg = part + npart;
+         *Q = P + n * m, *st = Q + n * m, *part = st + 8 * n + n * m, *out = part + npart;
   // device views of the caller's arrays (staged through st for host memory)
   double *dx = x, *d1 = xold1, *d2 = xold2, *dlo = low, *dup = upp;
   const double *dmin = xmin, *dmax = xmax, *ddf = dfdx, *ddg = dgdx;
@@ -986,102 +957,30 @@ int tpo_mma_update(tpo_ctx *ctx, const tpo_mma_opts *opts, int32_t iter,
     dx = v[0]; d1 = v[1]; d2 = v[2]; dlo = v[3]; dup = v[4];
     dmin = v[5]; dmax = v[6]; ddf = v[7]; ddg = st + 8 * n;
   }
-  // MMAsub (MMA.cpp:185-307); Set_m's constants (:40-52)
-  const double a0 = 1.0, b0 = 1.0;
-  std::vector<double> a(m, 0.0), cc(m, 1000.0), d(m, 1.0);
+  // MMAsub (MMA.cpp:185-343) with DualSolve (:353-595) in one cooperative
+  // launch; Set_m's constants a0 = b0 = 1, a = 0, c = 1000, d = 1 (:40-52)
   const bool fresh = *fresh_start && iter < 3;
   if (!fresh) *fresh_start = 0;
-  tpo::MmaConst k{o.move, o.asyinit, o.asyincr, o.asydecr, o.albefa, o.raa0};
-  tpo::launch_mma_prepare(n, m, fresh, k, dx, d1, d2, dlo, dup, dmin, dmax, ddf, ddg, alfa,
-                          beta, p0, q0, P, Q, part, s);
-  auto reduce = [&](int nvals, std::vector<double> &out) -> int {
-    CK(cudaMemcpyAsync(c.mma_h, part, sizeof(double) * tpo::kRedBlocks * nvals,
-                       cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    out.assign(nvals, 0.0);
-    for (int bI = 0; bI < tpo::kRedBlocks; ++bI)
-      for (int j = 0; j < nvals; ++j) out[j] += c.mma_h[bI * nvals + j];
-    return TPO_OK;
-  };
-  std::vector<double> b;
-  if (int rc = reduce(m, b)) return rc;
-  for (int j = 0; j < m; ++j) b[j] -= g[j];
-  // DualSolve (:353-405)
-  std::vector<double> lam(m, 500.0), eta(m, 1.0), G(m), S, y(m);
-  double z = 0.0;
-  auto evaluate = [&]() -> int {   // XYZofLam + DualGrad + the DualHess sums
-    tpo::MmaLambda L{};
-    for (int j = 0; j < m; ++j) L.v[j] = lam[j];
-    tpo::launch_mma_dual(n, m, L, alfa, beta, dlo, dup, p0, q0, P, Q, dx, part, s);
-    if (int rc = reduce(nv, S)) return rc;
-    double la = 0.0;
-    for (int j = 0; j < m; ++j) {
-      y[j] = std::max((lam[j] - cc[j]) / d[j], 0.0);
-      la += lam[j] * a[j];
-    }
-    z = 10 * std::max((la - a0) / b0, 0.0);
-    for (int j = 0; j < m; ++j) G[j] = S[j] - (b[j] + a[j] * z + y[j]);
-    return TPO_OK;
-  };
-  auto resmax = [&](double epsi) {
-    double r = 0.0;
-    for (int j = 0; j < m; ++j) {
-      r = std::max(r, std::fabs(G[j] + eta[j]));
-      r = std::max(r, std::fabs(eta[j] * lam[j] - epsi));
-    }
-    return r;
-  };
-  if (int rc = evaluate()) return rc;
-  for (double epsi = 1.0; epsi > o.epsimin; epsi *= 0.1) {
-    double rmax = resmax(epsi);
-    for (int it = 0; rmax > 0.9 * epsi && it < 100; ++it) {
-      // Hess (:507-515) from the sums at the current lambda; SearchDir (:532-544)
-      std::vector<double> A(m * m, 0.0), rhs(m), dl(m), de(m);
-      int t = m;
-      for (int j = 0; j < m; ++j)
-        for (int kk = j; kk < m; ++kk) {
-          A[j * m + kk] = A[kk * m + j] = -S[t];
-          ++t;
-        }
-      double la = 0.0;
-      for (int j = 0; j < m; ++j) la += lam[j] * a[j];
-      for (int j = 0; j < m; ++j) {
-        if (lam[j] > cc[j]) A[j * m + j] -= 1.0;
-        if (la > 0)
-          for (int kk = 0; kk < m; ++kk) A[j * m + kk] -= 10 * a[j] * a[kk];
-      }
-      double tr = 0.0;
-      for (int j = 0; j < m; ++j) {
-        A[j * m + j] -= eta[j] / lam[j];
-        tr += A[j * m + j];
-      }
-      const double shift = std::min(1e-4 * tr / m, -1e-7);
-      for (int j = 0; j < m; ++j) {
-        A[j * m + j] += shift;
-        rhs[j] = -G[j] - epsi / lam[j];
-      }
-      if (!solve_small(A, rhs, m, dl.data())) {
-        c.err = "MMA dual Newton step: singular system";
-        return TPO_E_BREAKDOWN;
-      }
-      // SearchDis (:559-575)
-      double theta = 1.0;
-      for (int j = 0; j < m; ++j) {
-        de[j] = -eta[j] + epsi / lam[j] - dl[j] * (eta[j] / lam[j]);
-        const double r1 = -0.99 * lam[j] / dl[j], r2 = -0.99 * eta[j] / de[j];
-        if (r1 >= 0) theta = std::min(theta, r1);
-        if (r2 >= 0) theta = std::min(theta, r2);
-      }
-      for (int j = 0; j < m; ++j) {
-        lam[j] += theta * dl[j];
-        eta[j] += theta * de[j];
-      }
-      if (int rc = evaluate()) return rc;
-      rmax = resmax(epsi);
-    }
+  tpo::MmaSolveArgs A{};
+  A.n = n;
+  A.m = m;
+  A.fresh = fresh ? 1 : 0;
+  A.k = tpo::MmaConst{o.move, o.asyinit, o.asyincr, o.asydecr, o.albefa, o.raa0};
+  A.epsimin = o.epsimin;
+  for (int j = 0; j < m; ++j) A.g[j] = g[j];
+  A.x = dx; A.x1 = d1; A.x2 = d2; A.low = dlo; A.upp = dup;
+  A.xmin = dmin; A.xmax = dmax; A.dfdx = ddf; A.dgdx = ddg;
+  A.alfa = alfa; A.beta = beta; A.p0 = p0; A.q0 = q0; A.P = P; A.Q = Q;
+  A.part = part; A.out = out; A.bar = c.gbar; A.fault = c.scal + tpo::kSlotFault;
+  cudaError_t lerr = cudaSuccess;
+  if (!tpo::launch_mma_solve(A, s, &lerr)) {
+    c.err = "MMA update: the persistent kernel does not fit on this device";
+    return TPO_E_CUDA;
   }
-  tpo::launch_max_change(n, dx, d1, dmin, dmax, chg, s);
-  CK(cudaMemcpyAsync(change, chg, sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(lerr);
+  CK(cudaMemcpyAsync(c.mma_h, out, sizeof(double) * 3, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(c.scal_h + tpo::kSlotFault, c.scal + tpo::kSlotFault, sizeof(double),
+                     cudaMemcpyDeviceToHost, s));
   if (mem != TPO_MEM_DEVICE) {
     double *hv[5] = {x, xold1, xold2, low, upp};
     const double *dv[5] = {dx, d1, d2, dlo, dup};
@@ -1089,7 +988,28 @@ int tpo_mma_update(tpo_ctx *ctx, const tpo_mma_opts *opts, int32_t iter,
       CK(cudaMemcpyAsync(hv[i], dv[i], sizeof(double) * n, cudaMemcpyDeviceToHost, s));
   }
   CK(cudaStreamSynchronize(s));
+  if (c.scal_h[tpo::kSlotFault] != 0.0) {
+    // a grid-barrier wait of the persistent kernel gave up: reset and report
+    c.scal_h[tpo::kSlotFault] = 0.0;
+    CK(cudaMemsetAsync(c.gbar, 0, sizeof(unsigned int), s));
+    CK(cudaMemsetAsync(c.scal + tpo::kSlotFault, 0, sizeof(double), s));
+    CK(cudaStreamSynchronize(s));
+    c.err = "MMA update: a grid-barrier wait ran out";
+    return TPO_E_CUDA;
+  }
+  if (c.mma_h[2] != 0.0) {
+    c.err = "MMA dual Newton step: singular system";
+    return TPO_E_BREAKDOWN;
+  }
+  *change = c.mma_h[0];
+  c.mma_steps = (int)c.mma_h[1];
   return finish(c, TPO_OK);
+}
+
+int tpo_mma_last_info(const tpo_ctx *ctx, int32_t *newton_steps) {
+  if (!ctx || !newton_steps) return TPO_E_ARG;
+  *newton_steps = ctx->c.mma_steps;
+  return TPO_OK;
 }
 
 int tpo_apply_f32(tpo_ctx *ctx, const float *u, float *y) {

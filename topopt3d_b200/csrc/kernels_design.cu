@@ -1,5 +1,7 @@
 // Design-side kernels: the density filter (forward and transpose, matrix
-// free), SIMP interpolation, the compliance sensitivity and the OC update.
+// free), SIMP interpolation, the compliance sensitivity, the OC update and
+// the MMA update.
+#include <algorithm>
 #include <math_constants.h>
 
 #include "grid_barrier.cuh"
@@ -146,6 +148,12 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
 // one bisection trial of MMA::OCsub (MMA.cpp:139-160): candidate x and
 // per-block partial sums of dgdx . (x - xold)
 __global__ void k_oc_step(int64_t n, double *x, const double *xold,
@@ -252,135 +260,311 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// ---- MMA for m >= 2 constraints (MMA::MMAsub, MMA.cpp:185-343, and
-// MMA::DualSolve, :353-595).  Every element-wise pass reduces into
-// per-block partials over the fixed kRedBlocks grid (m values per block for
-// b, m + m(m+1)/2 for the dual gradient and Hessian); the host sums them in
-// a fixed order, so the result does not depend on scheduling.
+// ---- MMA for m >= 2 constraints (MMA::MMAsub, MMA.cpp:185-343, with
+// MMA::DualSolve, :353-595), the whole update in one cooperative launch.
+//
+// Phase 0 (MMAsub, :219-307) forms the asymptotes, the move limits
+// alfa/beta, p0, q0, P, Q and the partials of b, and shifts xold2 <- xold1
+// <- x.  Each later phase evaluates x(lambda) (XYZofLam, :432-447) with the
+// partials of the dual gradient sums sum_n P_j/ux1 + Q_j/xl1 (DualGrad,
+// :461-474) and of the Hessian sums sum_n dhdx_j dLdxx dhdx_k, k >= j
+// (DualHess, :489-515).  After the grid barrier that closes a phase every
+// block sums the partials in the same fixed order, and thread 0 of every
+// block runs the same scalar Newton logic on the same numbers (residual,
+// SearchDir with partial pivoting, SearchDis, the epsilon schedule), so all
+// blocks agree on the next lambda without a second barrier.  The partials
+// are double-buffered by phase parity (a block writes phase p + 1's only
+// after the barrier that every block passes once it has read phase p's).
+// Element i is handled by the same thread in every phase, so x, xold1 and
+// the scratch need no exchange between threads.  Change (:309-310) is a
+// max over blocks by an atomic on the order-preserving bit pattern of
+// non-negative doubles.
+template <int M>
+struct MmaDims {
+  static constexpr int NH = M * (M + 1) / 2, NV = M + NH;
+};
 
-// sum of v over the block into out (thread 0), v a per-thread value
-__device__ __forceinline__ double block_total(double v, double *sh) {
-  v = warp_sum(v);
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
-  __syncthreads();
-  double t = 0.0;
-  if (threadIdx.x < 32) {
-    t = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
-    t = warp_sum(t);
-  }
-  return t;
-}
-
-// asymptotes (:219-247), move limits alfa/beta (:250-262), p0, q0, P, Q
-// (:265-300) and the partials of b (:303-305); then xold2 <- xold1 <- x
-// (:307).  P and Q are n x m column-major.
-__global__ void __launch_bounds__(256)
-    k_mma_prepare(int64_t n, int m, bool fresh, MmaConst k, double *x, double *x1,
-                  double *x2, double *low, double *upp, const double *xmin,
-                  const double *xmax, const double *dfdx, const double *dgdx,
-                  double *alfa, double *beta, double *p0, double *q0, double *P,
-                  double *Q, double *part) {
-  __shared__ double sh[32];
-  double bs[kMmaMaxM];
-  for (int j = 0; j < m; ++j) bs[j] = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const double xi = x[i], span = xmax[i] - xmin[i];
-    double lo, up;
-    if (fresh) {
-      lo = xi - k.asyinit * span;
-      up = xi + k.asyinit * span;
-    } else {
-      const double xa = x1[i], xb = x2[i];
-      const double zz = (xi - xa) * (xa - xb);
-      const double f = zz > 0 ? k.asyincr : (zz < 0 ? k.asydecr : 1.0);
-      lo = xi - f * (xa - low[i]);
-      up = xi + f * (upp[i] - xa);
-      lo = fmin(fmax(lo, xi - 10 * span), xi - 0.01 * span);
-      up = fmax(fmin(up, xi + 10 * span), xi + 0.01 * span);
-    }
-    alfa[i] = fmax(fmax(lo + k.albefa * (xi - lo), xi - k.move * span), xmin[i]);
-    beta[i] = fmin(fmin(up - k.albefa * (up - xi), xi + k.move * span), xmax[i]);
-    const double xmami = fmax(up - lo, 1e-5);
-    const double ux1 = up - xi, xl1 = xi - lo, ux2 = ux1 * ux1, xl2 = xl1 * xl1;
-    const double df = dfdx[i];
-    double pp = fmax(df, 0.0), qq = fmax(-df, 0.0);
-    const double pq0 = 0.001 * (pp + qq) + 0.5 * k.raa0 / xmami;
-    p0[i] = (pp + pq0) * ux2;
-    q0[i] = (qq + pq0) * xl2;
-    for (int j = 0; j < m; ++j) {
-      const double dg = dgdx[j * n + i];
-      const double Pj = fmax(dg, 0.0) * ux2, Qj = fmax(-dg, 0.0) * xl2;
-      P[j * n + i] = Pj;
-      Q[j * n + i] = Qj;
-      bs[j] += Pj / ux1 + Qj / xl1;
-    }
-    low[i] = lo;
-    upp[i] = up;
-    x2[i] = x1[i];
-    x1[i] = xi;
-  }
-  for (int j = 0; j < m; ++j) {
-    const double t = block_total(bs[j], sh);
-    if (threadIdx.x == 0) part[blockIdx.x * m + j] = t;
-  }
-}
-
-// x(lambda) (XYZofLam, :432-447) and the partials of the dual gradient sums
-// sum_n P_j/ux1 + Q_j/xl1 (DualGrad, :461-474) and of the Hessian sums
-// sum_n dhdx_j dLdxx dhdx_k, k >= j (DualHess, :489-515), at lambda
-__global__ void __launch_bounds__(256)
-    k_mma_dual(int64_t n, int m, MmaLambda lam, const double *alfa, const double *beta,
-               const double *low, const double *upp, const double *p0,
-               const double *q0, const double *P, const double *Q, double *x,
-               double *part) {
-  __shared__ double sh[32];
-  const int nh = m * (m + 1) / 2, nv = m + nh;
-  double acc[kMmaMaxM + kMmaMaxM * (kMmaMaxM + 1) / 2];
-  for (int j = 0; j < nv; ++j) acc[j] = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    double plam = p0[i], qlam = q0[i];
-    for (int j = 0; j < m; ++j) {
-      plam += P[j * n + i] * lam.v[j];
-      qlam += Q[j * n + i] * lam.v[j];
-    }
-    const double lo = low[i], up = upp[i], al = alfa[i], be = beta[i];
-    const double pr = sqrt(plam), qr = sqrt(qlam);
-    const double xi = fmax(fmin((pr * lo + qr * up) / (pr + qr), be), al);
-    x[i] = xi;
-    const double ux1 = up - xi, xl1 = xi - lo;
-    const double ux2 = ux1 * ux1, xl2 = xl1 * xl1;
-    const double inside = (xi > al && xi < be) ? 1.0 : 0.0;
-    const double dL = inside / (2 * plam / (ux2 * ux1) + 2 * qlam / (xl2 * xl1));
-    double dh[kMmaMaxM];
-    for (int j = 0; j < m; ++j) {
-      const double Pj = P[j * n + i], Qj = Q[j * n + i];
-      acc[j] += Pj / ux1 + Qj / xl1;
-      dh[j] = Pj / ux2 - Qj / xl2;
-    }
-    int t = m;
-    for (int j = 0; j < m; ++j)
-      for (int kk = j; kk < m; ++kk) acc[t++] += dh[j] * dL * dh[kk];
-  }
-  for (int j = 0; j < nv; ++j) {
-    const double s = block_total(acc[j], sh);
-    if (threadIdx.x == 0) part[blockIdx.x * nv + j] = s;
-  }
-}
-
-// Change = max |x - xold| / (xmax - xmin) (:309-310)
-__global__ void k_max_change(int64_t n, const double *x, const double *xold,
-                             const double *xmin, const double *xmax,
-                             unsigned long long *out) {
-  double mx = 0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    mx = fmax(mx, fabs((x[i] - xold[i]) / (xmax[i] - xmin[i])));
+// all threads: s_tot[j] = sum_b buf[j * G + b], j < CNT, in a fixed order
+// (thread t sums b = t, t + 256, ...; then the block reduction of
+// mma_store_parts), read past L1 since other blocks wrote buf
+template <int CNT>
+__device__ __forceinline__ void mma_sum_parts(const double *buf, int G, double *s_tot,
+                                              double *sh) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double v[CNT];
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(mx));
+  for (int j = 0; j < CNT; ++j) v[j] = 0.0;
+  for (int b = threadIdx.x; b < G; b += blockDim.x)
+#pragma unroll
+    for (int j = 0; j < CNT; ++j) v[j] += __ldcg(buf + (size_t)j * G + b);
+#pragma unroll
+  for (int j = 0; j < CNT; ++j) {
+    const double t = warp_sum(v[j]);
+    if (lane == 0) sh[j * 32 + w] = t;
+  }
+  __syncthreads();
+  for (int j = w; j < CNT; j += nw) {
+    double t = lane < nw ? sh[j * 32 + lane] : 0.0;
+    t = warp_sum(t);
+    if (lane == 0) s_tot[j] = t;
+  }
+  __syncthreads();
+}
+
+// all threads: buf[j * G + blockIdx.x] = block sum of v[j], j < cnt
+template <int CNT>
+__device__ __forceinline__ void mma_store_parts(const double *v, double *buf, double *sh) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int j = 0; j < CNT; ++j) {
+    const double t = warp_sum(v[j]);
+    if (lane == 0) sh[j * 32 + w] = t;
+  }
+  __syncthreads();
+  for (int j = w; j < CNT; j += nw) {
+    double t = lane < nw ? sh[j * 32 + lane] : 0.0;
+    t = warp_sum(t);
+    if (lane == 0) buf[(size_t)j * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+// x = A^-1 r for the m x m row-major A by Gaussian elimination with
+// partial pivoting; false on a zero pivot
+template <int M>
+__device__ bool mma_solve_small(double (&A)[M * M], double (&r)[M], double (&x)[M]) {
+  for (int k = 0; k < M; ++k) {
+    int p = k;
+    for (int i = k + 1; i < M; ++i)
+      if (fabs(A[i * M + k]) > fabs(A[p * M + k])) p = i;
+    if (A[p * M + k] == 0.0) return false;
+    if (p != k) {
+      for (int c = 0; c < M; ++c) {
+        const double t = A[k * M + c];
+        A[k * M + c] = A[p * M + c];
+        A[p * M + c] = t;
+      }
+      const double t = r[k];
+      r[k] = r[p];
+      r[p] = t;
+    }
+    for (int i = k + 1; i < M; ++i) {
+      const double f = A[i * M + k] / A[k * M + k];
+      for (int c = k; c < M; ++c) A[i * M + c] -= f * A[k * M + c];
+      r[i] -= f * r[k];
+    }
+  }
+  for (int k = M - 1; k >= 0; --k) {
+    double s = r[k];
+    for (int c = k + 1; c < M; ++c) s -= A[k * M + c] * x[c];
+    x[k] = s / A[k * M + k];
+  }
+  return true;
+}
+
+template <int M>
+__global__ void __launch_bounds__(256) k_mma_solve(MmaSolveArgs a) {
+  constexpr int NV = MmaDims<M>::NV;
+  __shared__ double sh[NV * 32];
+  __shared__ double s_tot[NV];
+  __shared__ double s_lam[M];
+  __shared__ int s_done;
+  const int G = gridDim.x;
+  const int64_t n = a.n;
+  const int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t di = (int64_t)G * blockDim.x;
+  int phase = 0;
+
+  // ---- phase 0: MMAsub's element pass (:219-307)
+  {
+    double bs[M];
+#pragma unroll
+    for (int j = 0; j < M; ++j) bs[j] = 0.0;
+    for (int64_t i = i0; i < n; i += di) {
+      const double xi = a.x[i], span = a.xmax[i] - a.xmin[i];
+      double lo, up;
+      if (a.fresh) {
+        lo = xi - a.k.asyinit * span;
+        up = xi + a.k.asyinit * span;
+      } else {
+        const double xa = a.x1[i], xb = a.x2[i];
+        const double zz = (xi - xa) * (xa - xb);
+        const double f = zz > 0 ? a.k.asyincr : (zz < 0 ? a.k.asydecr : 1.0);
+        lo = xi - f * (xa - a.low[i]);
+        up = xi + f * (a.upp[i] - xa);
+        lo = fmin(fmax(lo, xi - 10 * span), xi - 0.01 * span);
+        up = fmax(fmin(up, xi + 10 * span), xi + 0.01 * span);
+      }
+      a.alfa[i] = fmax(fmax(lo + a.k.albefa * (xi - lo), xi - a.k.move * span), a.xmin[i]);
+      a.beta[i] = fmin(fmin(up - a.k.albefa * (up - xi), xi + a.k.move * span), a.xmax[i]);
+      const double xmami = fmax(up - lo, 1e-5);
+      const double ux1 = up - xi, xl1 = xi - lo, ux2 = ux1 * ux1, xl2 = xl1 * xl1;
+      const double df = a.dfdx[i];
+      const double pp = fmax(df, 0.0), qq = fmax(-df, 0.0);
+      const double pq0 = 0.001 * (pp + qq) + 0.5 * a.k.raa0 / xmami;
+      a.p0[i] = (pp + pq0) * ux2;
+      a.q0[i] = (qq + pq0) * xl2;
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        const double dg = a.dgdx[j * n + i];
+        const double Pj = fmax(dg, 0.0) * ux2, Qj = fmax(-dg, 0.0) * xl2;
+        a.P[j * n + i] = Pj;
+        a.Q[j * n + i] = Qj;
+        bs[j] += Pj / ux1 + Qj / xl1;
+      }
+      a.low[i] = lo;
+      a.upp[i] = up;
+      a.x2[i] = a.x1[i];
+      a.x1[i] = xi;
+    }
+    double *buf = a.part + (size_t)(phase & 1) * NV * G;
+    mma_store_parts<M>(bs, buf, sh);
+    if (!grid_barrier(a.bar, a.fault)) return;
+    mma_sum_parts<M>(buf, G, s_tot, sh);
+    ++phase;
+  }
+
+  // ---- DualSolve (:353-405); the scalar state lives in thread 0
+  double lam[M], eta[M], b[M];
+  double epsi = 1.0;
+  int it = 0, steps = 0, status = 0;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      b[j] = s_tot[j] - a.g[j];
+      lam[j] = 500.0;
+      eta[j] = 1.0;
+      s_lam[j] = lam[j];
+    }
+  }
+  __syncthreads();
+  for (;;) {
+    double lr[M], acc[NV];
+#pragma unroll
+    for (int j = 0; j < M; ++j) lr[j] = s_lam[j];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) acc[j] = 0.0;
+    for (int64_t i = i0; i < n; i += di) {
+      double plam = a.p0[i], qlam = a.q0[i];
+      double Pj[M], Qj[M];
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        Pj[j] = a.P[j * n + i];
+        Qj[j] = a.Q[j * n + i];
+        plam += Pj[j] * lr[j];
+        qlam += Qj[j] * lr[j];
+      }
+      const double lo = a.low[i], up = a.upp[i], al = a.alfa[i], be = a.beta[i];
+      const double pr = sqrt(plam), qr = sqrt(qlam);
+      const double xi = fmax(fmin((pr * lo + qr * up) / (pr + qr), be), al);
+      a.x[i] = xi;
+      const double ux1 = up - xi, xl1 = xi - lo;
+      const double ux2 = ux1 * ux1, xl2 = xl1 * xl1;
+      const double inside = (xi > al && xi < be) ? 1.0 : 0.0;
+      const double dL = inside / (2 * plam / (ux2 * ux1) + 2 * qlam / (xl2 * xl1));
+      double dh[M];
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        acc[j] += Pj[j] / ux1 + Qj[j] / xl1;
+        dh[j] = Pj[j] / ux2 - Qj[j] / xl2;
+      }
+      int t = M;
+#pragma unroll
+      for (int j = 0; j < M; ++j)
+#pragma unroll
+        for (int kk = j; kk < M; ++kk) acc[t++] += dh[j] * dL * dh[kk];
+    }
+    double *buf = a.part + (size_t)(phase & 1) * NV * G;
+    mma_store_parts<NV>(acc, buf, sh);
+    if (!grid_barrier(a.bar, a.fault)) return;
+    mma_sum_parts<NV>(buf, G, s_tot, sh);
+    ++phase;
+    if (threadIdx.x == 0) {
+      // y, z (XYZofLam) and the gradient (DualGrad) at lambda; Set_m's
+      // constants a0 = b0 = 1, a = 0, c = 1000, d = 1 (:40-52)
+      double Gd[M];
+#pragma unroll
+      for (int j = 0; j < M; ++j) Gd[j] = s_tot[j] - (b[j] + fmax(lam[j] - 1000.0, 0.0));
+      int done = 0;
+      for (;;) {
+        double rmax = 0.0;    // DualResidual (:417-427), infinity norm
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+          rmax = fmax(rmax, fabs(Gd[j] + eta[j]));
+          rmax = fmax(rmax, fabs(eta[j] * lam[j] - epsi));
+        }
+        if (rmax > 0.9 * epsi && it < 100) {
+          // DualHess (:507-515) and SearchDir (:532-544)
+          double A[M * M], r[M], dl[M], de[M];
+          int t = M;
+#pragma unroll
+          for (int j = 0; j < M; ++j)
+#pragma unroll
+            for (int kk = j; kk < M; ++kk) {
+              A[j * M + kk] = A[kk * M + j] = -s_tot[t];
+              ++t;
+            }
+          double tr = 0.0;
+#pragma unroll
+          for (int j = 0; j < M; ++j) {
+            if (lam[j] > 1000.0) A[j * M + j] -= 1.0;
+            A[j * M + j] -= eta[j] / lam[j];
+            tr += A[j * M + j];
+          }
+          const double shift = fmin(1e-4 * tr / M, -1e-7);
+#pragma unroll
+          for (int j = 0; j < M; ++j) {
+            A[j * M + j] += shift;
+            r[j] = -Gd[j] - epsi / lam[j];
+          }
+          if (!mma_solve_small<M>(A, r, dl)) {
+            status = 1;
+            done = 1;
+            break;
+          }
+          double theta = 1.0;   // SearchDis (:559-575)
+#pragma unroll
+          for (int j = 0; j < M; ++j) {
+            de[j] = -eta[j] + epsi / lam[j] - dl[j] * (eta[j] / lam[j]);
+            const double r1 = -0.99 * lam[j] / dl[j], r2 = -0.99 * eta[j] / de[j];
+            if (r1 >= 0) theta = fmin(theta, r1);
+            if (r2 >= 0) theta = fmin(theta, r2);
+          }
+#pragma unroll
+          for (int j = 0; j < M; ++j) {
+            lam[j] += theta * dl[j];
+            eta[j] += theta * de[j];
+          }
+          ++it;
+          ++steps;
+          break;
+        }
+        epsi *= 0.1;
+        it = 0;
+        if (!(epsi > a.epsimin)) {
+          done = 1;
+          break;
+        }
+      }
+      s_done = done;
+#pragma unroll
+      for (int j = 0; j < M; ++j) s_lam[j] = lam[j];
+    }
+    __syncthreads();
+    if (s_done) break;
+  }
+
+  // ---- Change (:309-310)
+  double mx = 0.0;
+  for (int64_t i = i0; i < n; i += di)
+    mx = fmax(mx, fabs((a.x[i] - a.x1[i]) / (a.xmax[i] - a.xmin[i])));
+  mx = warp_max(mx);
+  if ((threadIdx.x & 31) == 0)
+    atomicMax(reinterpret_cast<unsigned long long *>(a.out),
+              (unsigned long long)__double_as_longlong(mx));
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.out[1] = steps;
+    a.out[2] = status;
+  }
 }
 
 // x < 1e-6 -> 0 (MMA.cpp:166-173), then Change = max |x - xold| / (xmax - xmin)
@@ -481,31 +665,44 @@ bool launch_oc_bisect(const Ctx &c, int64_t n, double *x, const double *xold,
   return true;
 }
 
-void launch_mma_prepare(int64_t n, int m, bool fresh, const MmaConst &k, double *x,
-                        double *x1, double *x2, double *low, double *upp,
-                        const double *xmin, const double *xmax, const double *dfdx,
-                        const double *dgdx, double *alfa, double *beta, double *p0,
-                        double *q0, double *P, double *Q, double *part, cudaStream_t s) {
+template <int M>
+bool launch_mma_solve_m(MmaSolveArgs &a, cudaStream_t s, cudaError_t *err) {
+  static int cap[64] = {0}, sms[64] = {0};   // co-resident blocks, SMs, per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  dev &= 63;
+  if (!cap[dev]) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mma_solve<M>, 256, 0);
+    cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+    cap[dev] = per_sm * sms[dev] > 0 ? std::min(per_sm * sms[dev], kRedBlocks) : -1;
+  }
+  if (cap[dev] < 0) return false;
+  // about 4 elements per thread, at least one block per SM: every Newton
+  // step ends in a grid barrier and a sum over the blocks' partials, so
+  // small meshes run best on few blocks
+  const int64_t want = std::max<int64_t>(sms[dev], (a.n + 1023) / 1024);
+  const int grid = (int)std::min<int64_t>(want, cap[dev]);
   count_launch();
-  k_mma_prepare<<<kRedBlocks, 256, 0, s>>>(n, m, fresh, k, x, x1, x2, low, upp, xmin, xmax,
-                                           dfdx, dgdx, alfa, beta, p0, q0, P, Q, part);
+  *err = cudaMemsetAsync(a.out, 0, sizeof(double), s);
+  if (*err != cudaSuccess) return true;
+  void *args[] = {&a};
+  *err = cudaLaunchCooperativeKernel((const void *)k_mma_solve<M>, grid, 256, args, 0, s);
+  return true;
 }
 
-void launch_mma_dual(int64_t n, int m, const MmaLambda &lam, const double *alfa,
-                     const double *beta, const double *low, const double *upp,
-                     const double *p0, const double *q0, const double *P, const double *Q,
-                     double *x, double *part, cudaStream_t s) {
-  count_launch();
-  k_mma_dual<<<kRedBlocks, 256, 0, s>>>(n, m, lam, alfa, beta, low, upp, p0, q0, P, Q, x,
-                                        part);
-}
-
-void launch_max_change(int64_t n, const double *x, const double *xold, const double *xmin,
-                       const double *xmax, double *out, cudaStream_t s) {
-  count_launch();
-  cudaMemsetAsync(out, 0, sizeof(double), s);
-  k_max_change<<<grid_for(n, 256), 256, 0, s>>>(n, x, xold, xmin, xmax,
-                                                reinterpret_cast<unsigned long long *>(out));
+bool launch_mma_solve(MmaSolveArgs &a, cudaStream_t s, cudaError_t *err) {
+  switch (a.m) {
+    case 1: return launch_mma_solve_m<1>(a, s, err);
+    case 2: return launch_mma_solve_m<2>(a, s, err);
+    case 3: return launch_mma_solve_m<3>(a, s, err);
+    case 4: return launch_mma_solve_m<4>(a, s, err);
+    case 5: return launch_mma_solve_m<5>(a, s, err);
+    case 6: return launch_mma_solve_m<6>(a, s, err);
+    case 7: return launch_mma_solve_m<7>(a, s, err);
+    case 8: return launch_mma_solve_m<8>(a, s, err);
+    default: return false;
+  }
 }
 
 void launch_oc_finish(const Ctx &c, int64_t n, double *x, const double *xold,

@@ -212,6 +212,7 @@ struct Ctx {
   size_t fq_n = 0;
   double *mma_buf = nullptr;  // MMA workspace (device) and partials mirror
   size_t mma_n = 0;
+  int mma_steps = 0;   // dual Newton steps of the last tpo_mma_update
   double *mma_h = nullptr;
 
   // CUDA graphs of the CG iteration bodies, keyed on (x, columns)
@@ -417,26 +418,29 @@ void launch_oc_step(const Ctx &c, int64_t n, double *x, const double *xold,
                     const double *dgdx, double move, double lmid, double *out,
                     cudaStream_t s);
 void launch_oc_clip(int64_t n, double *dfdx, cudaStream_t s);
-// MMA for m >= 2 constraints (kernels_design.cu): per-block partials over
-// kRedBlocks blocks (m for b; m + m(m+1)/2 for the dual gradient/Hessian)
+// MMA for m >= 2 constraints (kernels_design.cu): MMAsub, DualSolve and
+// Change in one cooperative launch
 constexpr int kMmaMaxM = 8;
 struct MmaConst {
   double move, asyinit, asyincr, asydecr, albefa, raa0;
 };
-struct MmaLambda {
-  double v[kMmaMaxM];
+struct MmaSolveArgs {
+  int64_t n;
+  int m, fresh;
+  MmaConst k;
+  double epsimin;
+  double g[kMmaMaxM];
+  double *x, *x1, *x2, *low, *upp;             // in/out design state
+  const double *xmin, *xmax, *dfdx, *dgdx;     // dgdx n x m column-major
+  double *alfa, *beta, *p0, *q0, *P, *Q;       // n, n, n, n, n*m, n*m scratch
+  double *part;       // 2 * (m + m(m+1)/2) * kRedBlocks doubles
+  double *out;        // [0] Change (zeroed by the launcher), [1] Newton
+                      // steps, [2] status (0 ok, 1 singular Newton system)
+  unsigned int *bar;  // grid barrier counter (c.gbar)
+  double *fault;      // set when a grid-barrier wait runs out
 };
-void launch_mma_prepare(int64_t n, int m, bool fresh, const MmaConst &k, double *x,
-                        double *x1, double *x2, double *low, double *upp,
-                        const double *xmin, const double *xmax, const double *dfdx,
-                        const double *dgdx, double *alfa, double *beta, double *p0,
-                        double *q0, double *P, double *Q, double *part, cudaStream_t s);
-void launch_mma_dual(int64_t n, int m, const MmaLambda &lam, const double *alfa,
-                     const double *beta, const double *low, const double *upp,
-                     const double *p0, const double *q0, const double *P, const double *Q,
-                     double *x, double *part, cudaStream_t s);
-void launch_max_change(int64_t n, const double *x, const double *xold, const double *xmin,
-                       const double *xmax, double *out, cudaStream_t s);
+// false when no block of the kernel fits on an SM (nothing launched)
+bool launch_mma_solve(MmaSolveArgs &a, cudaStream_t s, cudaError_t *err);
 // the whole OC bisection in one cooperative launch of kRedBlocks CTAs (uses
 // c.part, c.gbar and the fault slot); false when the device cannot hold
 // them all at once, and the caller runs the per-trial launches instead

@@ -530,8 +530,7 @@ class OC:
 class MMA(OC):
     """MMA::Update (MMA.cpp:62-100): the OC branch for fewer than two
     constraints (as OC), otherwise MMA::MMAsub with MMA::DualSolve
-    (:185-595) -- the element passes on the GPU, the dual Newton steps on
-    the host.  xold1, xold2, low and upp are the method's state; they start
+    (:185-595) -- the whole update in one persistent GPU launch.  xold1, xold2, low and upp are the method's state; they start
     from xval as MMA::Set_Values does.  opts: tpo_mma_opts fields (move is
     taken from the dataclass field)."""
     xold1: np.ndarray = None
@@ -540,6 +539,7 @@ class MMA(OC):
     upp: np.ndarray = None
     fresh_start: bool = True
     mma_opts: dict = field(default_factory=dict)
+    newton_steps: int = 0        # dual Newton steps of the last update
 
     def Update(self, topOpt, dfdx, g, dgdx):
         g = np.atleast_1d(np.asarray(g, np.float64))
@@ -565,6 +565,9 @@ class MMA(OC):
             L.MEM_HOST), "MMA update")
         self.xold1, self.xold2, self.low, self.upp = st
         self.fresh_start = bool(fresh.value)
+        steps = C.c_int32()
+        topOpt._lib.tpo_mma_last_info(topOpt._h, C.byref(steps))
+        self.newton_steps = steps.value
         self.xval = x
         self.Change = ch.value
         return x
