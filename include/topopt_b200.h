@@ -277,7 +277,7 @@ TPO_API int tpo_mma_update(tpo_ctx *ctx, const tpo_mma_opts *opts, int32_t iter,
  * tpo_mma_update took */
 TPO_API int tpo_mma_last_info(const tpo_ctx *ctx, int32_t *newton_steps);
 
-/* U, F, x, rho, E, dEdz accessors: which = "U","F","x","rho","E","dEdz" */
+/* U, F, x, rho, E, dEdz, Es accessors: which = "U","F","x","rho","E","dEdz","Es" */
 TPO_API int tpo_get_vector(const tpo_ctx *ctx, const char *which, double *out, int mem);
 TPO_API int tpo_set_vector(tpo_ctx *ctx, const char *which, const double *in, int mem);
 
@@ -309,6 +309,63 @@ TPO_API int tpo_set_stream(tpo_ctx *ctx, void *stream);
 /* number of kernels this library has launched in the process (graph
  * launches count their kernel nodes).  No reference counterpart. */
 TPO_API int64_t tpo_kernel_launches(void);
+
+/* ---- the reference's output and restart files (TopOpt.cpp:97-508,
+ * RecMesh.cpp:34-412) ---------------------------------------------------
+ * index_bytes is sizeof(PetscInt) of the PETSc build the files belong to
+ * (4 by default, 8 with 64-bit indices).  Raw arrays are native-endian as
+ * the reference writes them with ofstream / MPI-IO; the PETSc binary
+ * viewer encoding is big-endian.  One process: the distributions are
+ * [0, nElem] and [0, nNode].  No .info side files are written.  Calls
+ * without a context report errors through tpo_last_error(NULL). */
+
+/* VecView / VecLoad on a binary viewer: [1211214, n] as PetscInt, then n
+ * doubles.  tpo_read_vec_bin with v = NULL returns the length only. */
+TPO_API int tpo_write_vec_bin(const char *path, const double *v, int64_t n,
+                              int32_t index_bytes);
+TPO_API int tpo_read_vec_bin(const char *path, double *v, int64_t cap, int64_t *n,
+                             int32_t index_bytes);
+/* MatView / MatLoad of an AIJ matrix: [1211216, M, N, nnz], the M row
+ * lengths, the column indices, the values; rowptr has M + 1 entries.
+ * tpo_read_mat_bin with rowptr = NULL returns the sizes only. */
+TPO_API int tpo_write_mat_bin(const char *path, int64_t M, int64_t N, const int64_t *rowptr,
+                              const int64_t *col, const double *val, int32_t index_bytes);
+TPO_API int tpo_read_mat_bin(const char *path, int64_t *M, int64_t *N, int64_t *nnz,
+                             int64_t *rowptr, int64_t *col, double *val, int64_t cap_rows,
+                             int64_t cap_nnz, int32_t index_bytes);
+/* TopOpt::MeshOut (TopOpt.cpp:97-359) into `folder`: Element_/Node_
+ * Distribution, elements, nodes, the load and support lists (eigen
+ * supports, springs and masses empty), Filter.bin (the density filter P),
+ * Max_Filter.bin and Void_Edge_Volume.bin (the max-length-scale filter of
+ * radius rmax, unscaled, and max(rowsum) - rowsum), active.bin and the
+ * interpolations P<l>.bin with P<l>.bin.split. */
+TPO_API int tpo_mesh_out(tpo_ctx *ctx, const char *folder, double rmax, int32_t index_bytes);
+/* TopOpt::PrintVals (TopOpt.cpp:445-508): U, x, V (the filtered density),
+ * Es, E as <name><name_suffix>.bin, and the mode shapes phiB (nB columns)
+ * and phiD (nD columns) of 3*nNode host doubles each as
+ * phiB<suffix>_mode<i>.bin and phiD_<suffix>_mode<i>.bin. */
+TPO_API int tpo_print_vals(tpo_ctx *ctx, const char *folder, const char *name_suffix,
+                           const double *phiB, int32_t nB, const double *phiD, int32_t nD,
+                           int32_t index_bytes);
+/* TopOpt::LoadMesh (RecMesh.cpp:34-412) for a structured hex8 box: a new
+ * context from a MeshOut folder.  nel and dx come from the files (params
+ * supplies E0, nu, rmin and mg_levels; mg_levels <= 0 takes one more than
+ * the P<l>.bin files present); the support and load lists become the BCs.
+ * A Filter.bin that is not the radius-rmin filter of the mesh, springs,
+ * eigen-only supports or passive elements are refused. */
+TPO_API int tpo_load_mesh(const char *folder, const tpo_mesh_params *params,
+                          int32_t index_bytes, tpo_ctx **out);
+/* The design part of LoadMesh (RecMesh.cpp:391-404) with Main.cpp:52-56:
+ * x (nElem) = 0.5, then x_pen<p>.bin for each penalty in turn until one is
+ * missing.  *penal (in: the current penalty, out: the penalty reached) and
+ * *start (the index of the first penalty still to run) may be NULL. */
+TPO_API int tpo_load_design(tpo_ctx *ctx, const char *folder, const double *penalties,
+                            int32_t npen, double *x, double *penal, int32_t *start,
+                            int32_t index_bytes);
+/* massNodes.bin / masses.bin (RecMesh.cpp:147-180) as the 3*nNode point
+ * mass vector tpo_frequency takes (summed where a node repeats). */
+TPO_API int tpo_load_point_masses(tpo_ctx *ctx, const char *folder, double *mlump,
+                                  int32_t index_bytes);
 
 /* Filtered compliance sensitivity that allocates nothing.  It has no
  * counterpart in the reference.  It serves callers that may not call

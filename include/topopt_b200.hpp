@@ -23,6 +23,8 @@
 #include <array>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
+#include <memory>
 #include <string>
 #include <utility>
 #include <vector>
@@ -52,6 +54,20 @@ class TopOpt {
     tpo_default_eig_opts(&eig);
   }
   ~TopOpt() { tpo_destroy(ctx_); }
+  // TopOpt::LoadMesh (RecMesh.cpp:34-412): a problem from a MeshOut folder
+  // of a structured box (null on failure; tpo_last_error(NULL) says why)
+  static std::unique_ptr<TopOpt> LoadMesh(const std::string &folder, double E0, double Nu0,
+                                          double rmin, int mg_levels = 0,
+                                          int index_bytes = 4) {
+    tpo_mesh_params p{};
+    p.E0 = E0;
+    p.nu = Nu0;
+    p.rmin = rmin;
+    p.mg_levels = mg_levels;
+    tpo_ctx *h = nullptr;
+    if (tpo_load_mesh(folder.c_str(), &p, index_bytes, &h) != 0) return nullptr;
+    return std::unique_ptr<TopOpt>(new TopOpt(h));
+  }
   TopOpt(const TopOpt &) = delete;
   TopOpt &operator=(const TopOpt &) = delete;
 
@@ -112,6 +128,20 @@ class TopOpt {
                                   dvdx.data(), nullptr, TPO_MEM_HOST, nullptr);
     return rc < 0 ? rc : 0;
   }
+  // TopOpt::MeshOut (TopOpt.cpp:97-359) and PrintVals (:445-508); modes
+  // are 3*nNode x n column-major
+  int MeshOut(const std::string &folder = ".", double rmax = 3.0, int index_bytes = 4) {
+    return tpo_mesh_out(ctx_, folder.c_str(), rmax, index_bytes);
+  }
+  int PrintVals(const std::string &name_suffix, const std::string &folder = ".",
+                const std::vector<double> &phiB = {}, const std::vector<double> &phiD = {},
+                int index_bytes = 4) {
+    const int64_t nd = 3 * nNode;
+    return tpo_print_vals(ctx_, folder.c_str(), name_suffix.c_str(),
+                          phiB.empty() ? nullptr : phiB.data(), (int32_t)(phiB.size() / nd),
+                          phiD.empty() ? nullptr : phiD.data(), (int32_t)(phiD.size() / nd),
+                          index_bytes);
+  }
   std::vector<double> get(const char *which) const {
     const bool nodal = which[0] == 'U' || which[0] == 'F';
     std::vector<double> out(nodal ? 3 * nNode : nElem);
@@ -130,6 +160,11 @@ class TopOpt {
   int KUF_reason = 0;
 
  private:
+  explicit TopOpt(tpo_ctx *h) : ctx_(h) {
+    tpo_sizes(ctx_, &nElem, &nNode, &levels);
+    tpo_default_solve_opts(&opts);
+    tpo_default_eig_opts(&eig);
+  }
   tpo_ctx *ctx_ = nullptr;
   int status_ = 0;
 };
@@ -142,6 +177,8 @@ class Function_Base {
       : weights(std::move(values)), min_val(min_val), max_val(max_val),
         objective(objective), calc_gradient(calc_gradient) {}
   virtual ~Function_Base() = default;
+  // Function_Base::name[func_type] (Functions.cpp:5)
+  virtual const char *name() const { return "Function"; }
 
   int Compute(TopOpt &t) {
     int rc = Function(t);
@@ -170,6 +207,7 @@ class Function_Base {
 class Compliance : public Function_Base {
  public:
   using Function_Base::Function_Base;
+  const char *name() const override { return "Compliance"; }
 
  protected:
   int Function(TopOpt &t) override {
@@ -188,6 +226,7 @@ class Volume : public Function_Base {
          bool objective, bool calc_gradient = true)
       : Function_Base(scale(values, min_val, max_val, objective), min_val,
                       max_val, objective, calc_gradient) {}
+  const char *name() const override { return "Volume"; }
 
  protected:
   static std::vector<double> scale(std::vector<double> v, double lo, double hi,
@@ -209,6 +248,7 @@ class Volume : public Function_Base {
 class Stability : public Function_Base {
  public:
   using Function_Base::Function_Base;
+  const char *name() const override { return "Stability"; }
 
  protected:
   int Function(TopOpt &t) override {
@@ -235,6 +275,7 @@ class Frequency : public Function_Base {
             bool calc_gradient, int nvals, double density)
       : Function_Base(std::move(values), min_val, max_val, objective, calc_gradient),
         nvals(nvals), density(density) {}
+  const char *name() const override { return "Frequency"; }
   int nvals;
   double density;
   std::vector<double> lambda;
@@ -312,6 +353,35 @@ class MMA {
   double minchange = 0.0;
   bool fresh_start = true;
 };
+
+// TopOpt::StepOut's Output.txt entry (TopOpt.cpp:386-401)
+inline void StepOut(std::FILE *out, double f, const std::vector<double> &cons, int it,
+                    const std::vector<Function_Base *> &functions) {
+  std::fprintf(out, "Iteration number: %u\n", (unsigned)it);
+  std::fprintf(out, "Objective: %1.6g\n", f);
+  std::fprintf(out, "Constraints:\n");
+  for (double c : cons) std::fprintf(out, "\t%1.12g\t", c);
+  std::fprintf(out, "\nAll function values:\n");
+  for (const Function_Base *fn : functions)
+    std::fprintf(out, "\t%12s: %1.8g\n", fn->name(), fn->value);
+  std::fprintf(out, "\n");
+}
+
+// TopOpt::ResultOut (TopOpt.cpp:415-435): the stiffness-to-volume line,
+// then PrintVals with the suffix _pen<penal> into `folder`
+inline int ResultOut(std::FILE *out, TopOpt &t, int it, const std::string &folder = ".") {
+  double Esum = 0, Vsum = 0;
+  for (double v : t.get("E")) Esum += v;
+  for (double v : t.get("rho")) Vsum += v;
+  std::fprintf(out,
+               "************************************************\nAfter %4i iterations "
+               "with a penalty of %1.4g the\nratio of stiffness sum to volume sum is "
+               "%1.4g\n************************************************\n\n",
+               it, t.penal, Esum / Vsum);
+  char sfx[30];
+  std::snprintf(sfx, sizeof sfx, "_pen%1.4g", t.penal);
+  return t.PrintVals(sfx, folder);
+}
 
 }  // namespace tpo
 

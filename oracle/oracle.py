@@ -63,6 +63,7 @@ def _declare(L):
     L.tor_constitutive.argtypes = [C.c_double, C.c_double, _dp]
     L.tor_element_stiffness.argtypes = [_dp, C.c_double, C.c_double, _dp]
     L.tor_element_nodes.argtypes = [C.POINTER(C.c_int), C.c_int64, _i64]
+    L.tor_node_coords.argtypes = [C.POINTER(C.c_int), _dp, _dp, C.c_int64, _dp]
     L.tor_select_nodes.restype = C.c_int64
     L.tor_select_nodes.argtypes = [C.POINTER(C.c_int), _dp, _dp, _dp, _dp, _dp, vp]
     L.tor_filter_build.restype = C.c_int64
@@ -132,6 +133,19 @@ def element_stiffness(dx=(1.0, 1.0, 1.0), E0=1.0, nu=0.3) -> np.ndarray:
 def element_nodes(nel, e) -> np.ndarray:
     out = np.zeros(8, np.int64)
     lib().tor_element_nodes(_ivec3(nel), int(e), out)
+    return out
+
+
+def node_coords(nel, dx, origin=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """all node coordinates (nNode x 3, RecMesh.cpp:582-597)"""
+    L = lib()
+    nn = int(np.prod([n + 1 for n in nel]))
+    out = np.zeros((nn, 3))
+    xyz = np.zeros(3)
+    dxa, oa = np.asarray(dx, float), np.asarray(origin, float)
+    for n in range(nn):
+        L.tor_node_coords(_ivec3(nel), dxa, oa, n, xyz)
+        out[n] = xyz
     return out
 
 

@@ -36,6 +36,9 @@ EXPORTS = (
     "tpo_sensitivity_noalloc", "tpo_default_eig_opts", "tpo_ks_assemble",
     "tpo_ks_apply", "tpo_buckling", "tpo_buckling_sensitivity", "tpo_frequency",
     "tpo_default_mma_opts", "tpo_mma_update", "tpo_mma_last_info",
+    "tpo_write_vec_bin", "tpo_read_vec_bin", "tpo_write_mat_bin", "tpo_read_mat_bin",
+    "tpo_mesh_out", "tpo_print_vals", "tpo_load_mesh", "tpo_load_design",
+    "tpo_load_point_masses",
 )
 NOALLOC_MAX_ELEMS = 1 << 20
 
@@ -146,6 +149,23 @@ def load(path: str | None = None):
         "tpo_mma_update": (C.c_int, [vp, C.POINTER(MmaOpts), i32, C.POINTER(i32), i32,
                                      vp, vp, vp, vp, vp, vp, vp, vp, dp, vp, dp, C.c_int]),
         "tpo_mma_last_info": (C.c_int, [vp, C.POINTER(i32)]),
+        "tpo_write_vec_bin": (C.c_int, [C.c_char_p, dp, C.c_int64, i32]),
+        "tpo_read_vec_bin": (C.c_int, [C.c_char_p, dp, C.c_int64,
+                                       C.POINTER(C.c_int64), i32]),
+        "tpo_write_mat_bin": (C.c_int, [C.c_char_p, C.c_int64, C.c_int64,
+                                        C.POINTER(C.c_int64), C.POINTER(C.c_int64), dp,
+                                        i32]),
+        "tpo_read_mat_bin": (C.c_int, [C.c_char_p, C.POINTER(C.c_int64),
+                                       C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                       C.POINTER(C.c_int64), C.POINTER(C.c_int64), dp,
+                                       C.c_int64, C.c_int64, i32]),
+        "tpo_mesh_out": (C.c_int, [vp, C.c_char_p, d, i32]),
+        "tpo_print_vals": (C.c_int, [vp, C.c_char_p, C.c_char_p, dp, i32, dp, i32, i32]),
+        "tpo_load_mesh": (C.c_int, [C.c_char_p, C.POINTER(MeshParams), i32,
+                                    C.POINTER(vp)]),
+        "tpo_load_design": (C.c_int, [vp, C.c_char_p, dp, i32, dp, dp, C.POINTER(i32),
+                                      i32]),
+        "tpo_load_point_masses": (C.c_int, [vp, C.c_char_p, dp, i32]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

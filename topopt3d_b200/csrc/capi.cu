@@ -10,6 +10,7 @@
 #include <string>
 
 #include "coarse.h"
+#include "io.h"
 #include "solver.h"
 
 using tpo::Ctx;
@@ -53,6 +54,21 @@ template <typename T>
 void dfree(T *&p) {
   if (p) cudaFree(p);
   p = nullptr;
+}
+
+// message of the last failed context-free call (file I/O, tpo_load_mesh),
+// per thread; tpo_last_error(NULL) returns it
+thread_local std::string g_io_err;
+
+int io_fail(const std::string &msg, int rc = TPO_E_ARG) {
+  g_io_err = msg;
+  return rc;
+}
+
+std::string folder_prefix(const char *folder) {
+  std::string d = folder;
+  if (!d.empty() && d.back() != '/') d += '/';
+  return d;
 }
 
 // Eigen 3.3 LinSpaced (floating point) as used for the node coordinates
@@ -255,6 +271,7 @@ double *vec_ptr(Ctx &c, const char *which, size_t *n) {
   if (!std::strcmp(which, "rho")) { *n = c.ne; return c.rho; }
   if (!std::strcmp(which, "E")) { *n = c.ne; return c.E64; }
   if (!std::strcmp(which, "dEdz")) { *n = c.ne; return c.dEdz; }
+  if (!std::strcmp(which, "Es")) { *n = c.ne; return c.Es64; }
   return nullptr;
 }
 
@@ -293,7 +310,8 @@ void tpo_default_solve_opts(tpo_solve_opts *o) {
 }
 
 const char *tpo_last_error(const tpo_ctx *ctx) {
-  return ctx ? ctx->c.err.c_str() : "null context";
+  if (ctx) return ctx->c.err.c_str();
+  return g_io_err.empty() ? "null context" : g_io_err.c_str();
 }
 
 int tpo_create(const tpo_mesh_params *p, tpo_ctx **out) {
@@ -480,11 +498,14 @@ int tpo_add_bc(tpo_ctx *ctx, int32_t type, const double center[3],
     }
     if (!(valid && dist <= 1)) continue;
     ++cnt;
+    (type == TPO_BC_SUPPORT ? c.supp_node : c.load_node).push_back(n);
     for (int d = 0; d < 3; ++d) {
       if (type == TPO_BC_SUPPORT) {
         if (values[d] != 0) c.fix_h[n] |= (uint8_t)(1u << d);
+        c.supp_val.push_back(values[d] != 0);
       } else {
         c.F_h[3 * n + d] += values[d];   // FEAnalysis.cpp:352-355
+        c.load_val.push_back(values[d]);
       }
     }
   }
@@ -507,6 +528,26 @@ int tpo_set_bc(tpo_ctx *ctx, const uint8_t *fixmask, const double *F, int mem) {
   const cudaMemcpyKind k = mem == TPO_MEM_DEVICE ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost;
   if (fixmask) CK(cudaMemcpy(c.fix_h.data(), fixmask, c.nn, k));
   if (F) CK(cudaMemcpy(c.F_h.data(), F, sizeof(double) * 3 * c.nn, k));
+  // the BC lists from the arrays: supported nodes and loaded nodes, in
+  // increasing order
+  if (fixmask) {
+    c.supp_node.clear();
+    c.supp_val.clear();
+    for (int64_t n = 0; n < c.nn; ++n)
+      if (c.fix_h[n]) {
+        c.supp_node.push_back(n);
+        for (int d = 0; d < 3; ++d) c.supp_val.push_back((c.fix_h[n] >> d) & 1);
+      }
+  }
+  if (F) {
+    c.load_node.clear();
+    c.load_val.clear();
+    for (int64_t n = 0; n < c.nn; ++n)
+      if (c.F_h[3 * n] != 0 || c.F_h[3 * n + 1] != 0 || c.F_h[3 * n + 2] != 0) {
+        c.load_node.push_back(n);
+        for (int d = 0; d < 3; ++d) c.load_val.push_back(c.F_h[3 * n + d]);
+      }
+  }
   if (c.initialized) {
     CK(cudaMemcpyAsync(c.fix, c.fix_h.data(), c.nn, cudaMemcpyHostToDevice, c.stream));
     CK(cudaMemcpyAsync(c.F, c.F_h.data(), sizeof(double) * 3 * c.nn, cudaMemcpyHostToDevice, c.stream));
@@ -1232,5 +1273,371 @@ int tpo_set_stream(tpo_ctx *ctx, void *stream) {
 }
 
 int64_t tpo_kernel_launches(void) { return tpo::g_launches.load(); }
+
+// ---- the reference's output and restart files ----------------------------
+
+int tpo_write_vec_bin(const char *path, const double *v, int64_t n, int32_t index_bytes) {
+  if (!path || (!v && n > 0) || n < 0) return io_fail("invalid Vec arguments");
+  std::string err;
+  return tpo::io::write_vec(path, v, n, index_bytes, err) ? TPO_OK : io_fail(err);
+}
+
+int tpo_read_vec_bin(const char *path, double *v, int64_t cap, int64_t *n,
+                     int32_t index_bytes) {
+  if (!path || !n) return io_fail("invalid Vec arguments");
+  std::string err;
+  std::vector<double> w;
+  if (!tpo::io::read_vec(path, w, index_bytes, err)) return io_fail(err);
+  *n = (int64_t)w.size();
+  if (!v) return TPO_OK;
+  if (cap < *n) return io_fail("Vec buffer too small");
+  std::copy(w.begin(), w.end(), v);
+  return TPO_OK;
+}
+
+int tpo_write_mat_bin(const char *path, int64_t M, int64_t N, const int64_t *rowptr,
+                      const int64_t *col, const double *val, int32_t index_bytes) {
+  if (!path || M < 0 || N < 0 || !rowptr) return io_fail("invalid matrix arguments");
+  const int64_t nnz = rowptr[M];
+  if (nnz > 0 && (!col || !val)) return io_fail("invalid matrix arguments");
+  tpo::io::Csr A;
+  A.M = M;
+  A.N = N;
+  A.rowptr.assign(rowptr, rowptr + M + 1);
+  A.col.assign(col, col + nnz);
+  A.val.assign(val, val + nnz);
+  std::string err;
+  return tpo::io::write_mat(path, A, index_bytes, err) ? TPO_OK : io_fail(err);
+}
+
+int tpo_read_mat_bin(const char *path, int64_t *M, int64_t *N, int64_t *nnz,
+                     int64_t *rowptr, int64_t *col, double *val, int64_t cap_rows,
+                     int64_t cap_nnz, int32_t index_bytes) {
+  if (!path || !M || !N || !nnz) return io_fail("invalid matrix arguments");
+  tpo::io::Csr A;
+  std::string err;
+  if (!tpo::io::read_mat(path, A, index_bytes, err)) return io_fail(err);
+  *M = A.M;
+  *N = A.N;
+  *nnz = A.rowptr.back();
+  if (!rowptr) return TPO_OK;
+  if (cap_rows < A.M + 1 || cap_nnz < *nnz || !col || !val)
+    return io_fail("matrix buffers too small");
+  std::copy(A.rowptr.begin(), A.rowptr.end(), rowptr);
+  std::copy(A.col.begin(), A.col.end(), col);
+  std::copy(A.val.begin(), A.val.end(), val);
+  return TPO_OK;
+}
+
+int tpo_mesh_out(tpo_ctx *ctx, const char *folder, double rmax, int32_t index_bytes) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  REQUIRE(folder, "null folder");
+  REQUIRE(rmax > 0, "rmax must be positive");
+  REQUIRE(index_bytes == 4 || index_bytes == 8, "PetscInt size must be 4 or 8 bytes");
+  const std::string d = folder_prefix(folder);
+  const int ib = index_bytes;
+  std::string err;
+  auto ints = [&](const char *name, const std::vector<int64_t> &v) {
+    return tpo::io::write_ints(d + name, v.data(), v.size(), ib, err);
+  };
+  auto raw = [&](const char *name, const void *p, size_t bytes) {
+    return tpo::io::write_raw(d + name, p, bytes, err);
+  };
+  // distributions of one process (TopOpt.cpp:103-110)
+  bool ok = ints("Element_Distribution.bin", {0, c.ne}) &&
+            ints("Node_Distribution.bin", {0, c.nn});
+  // elements (global node numbers, 8 per element) and node coordinates,
+  // both row-major (:127-155)
+  std::vector<int64_t> el(8 * (size_t)c.ne);
+  for (int64_t e = 0; ok && e < c.ne; ++e) tpo::io::element_nodes(c.nel, e, el.data() + 8 * e);
+  ok = ok && ints("elements.bin", el);
+  el.clear();
+  el.shrink_to_fit();
+  std::vector<double> xyz(3 * (size_t)c.nn);
+  const int64_t N[3] = {c.nel[0] + 1, c.nel[1] + 1, c.nel[2] + 1};
+  for (int64_t n = 0; n < c.nn; ++n) {
+    const int64_t idx[3] = {n % N[0], (n / N[0]) % N[1], n / (N[0] * N[1])};
+    for (int k = 0; k < 3; ++k)
+      xyz[3 * n + k] = linspaced(0.0, c.prm.dx[k] * c.nel[k], N[k], idx[k]);
+  }
+  ok = ok && raw("nodes.bin", xyz.data(), sizeof(double) * xyz.size());
+  // BC lists (:157-310): loads, supports; no eigen-only supports, springs
+  // or point masses are held by a context, so those files are empty
+  std::vector<uint8_t> sv(c.supp_val.begin(), c.supp_val.end());
+  ok = ok && ints("loadNodes.bin", c.load_node) &&
+       raw("loads.bin", c.load_val.data(), sizeof(double) * c.load_val.size()) &&
+       ints("supportNodes.bin", c.supp_node) && raw("supports.bin", sv.data(), sv.size()) &&
+       ints("eigenSupportNodes.bin", {}) && raw("eigenSupports.bin", nullptr, 0) &&
+       ints("springNodes.bin", {}) && raw("springs.bin", nullptr, 0) &&
+       ints("massNodes.bin", {}) && raw("masses.bin", nullptr, 0);
+  // the density filter, the max-length-scale filter and its edge vector
+  // (:312-328; RecMesh.cpp:705-718)
+  if (ok) ok = tpo::io::write_mat(d + "Filter.bin",
+                                  tpo::io::filter_matrix(c.nel, c.prm.dx, c.prm.rmin, true),
+                                  ib, err);
+  if (ok) {
+    const tpo::io::Csr R = tpo::io::filter_matrix(c.nel, c.prm.dx, rmax, false);
+    std::vector<double> edge(R.M, 0.0);
+    double mx = -INFINITY;
+    for (int64_t r = 0; r < R.M; ++r) {
+      double s = 0;
+      for (int64_t t = R.rowptr[r]; t < R.rowptr[r + 1]; ++t) s += R.val[t];
+      edge[r] = s;
+      mx = std::max(mx, s);
+    }
+    for (double &v : edge) v = mx - v;   // VecAYPX(REdge, -1, max)
+    ok = tpo::io::write_mat(d + "Max_Filter.bin", R, ib, err) &&
+         tpo::io::write_vec(d + "Void_Edge_Volume.bin", edge.data(), R.M, ib, err);
+  }
+  // every element active (:330-340)
+  if (ok) {
+    std::vector<uint8_t> act(c.ne, 1);
+    ok = raw("active.bin", act.data(), act.size());
+  }
+  // the multigrid interpolations and their column splits (:342-357)
+  for (int l = 0; ok && l + 1 < c.L; ++l) {
+    const tpo::io::Csr P = tpo::io::prolongation_matrix(c.lev[l].dims, c.lev[l + 1].dims);
+    const std::string name = "P" + std::to_string(l) + ".bin";
+    ok = tpo::io::write_mat(d + name, P, ib, err) &&
+         tpo::io::write_ints(d + name + ".split", &P.N, 1, ib, err);
+  }
+  if (!ok) {
+    c.err = err;
+    return TPO_E_ARG;
+  }
+  return TPO_OK;
+}
+
+int tpo_print_vals(tpo_ctx *ctx, const char *folder, const char *name_suffix,
+                   const double *phiB, int32_t nB, const double *phiD, int32_t nD,
+                   int32_t index_bytes) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  REQUIRE(folder && name_suffix, "null folder or suffix");
+  REQUIRE(c.initialized && c.have_material, "mesh not initialised or no material");
+  REQUIRE(nB >= 0 && nD >= 0 && (nB == 0 || phiB) && (nD == 0 || phiD), "invalid mode arrays");
+  const std::string d = folder_prefix(folder), sfx = name_suffix;
+  std::string err;
+  // U, x, V, Es, E (TopOpt.cpp:451-479)
+  struct Item {
+    const char *file, *vec;
+  } items[] = {{"U", "U"}, {"x", "x"}, {"V", "rho"}, {"Es", "Es"}, {"E", "E"}};
+  for (const Item &it : items) {
+    size_t n = 0;
+    double *p = vec_ptr(c, it.vec, &n);
+    REQUIRE(p, "vector not allocated");
+    std::vector<double> h(n);
+    CK(cudaMemcpyAsync(h.data(), p, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    if (!tpo::io::write_vec(d + it.file + sfx + ".bin", h.data(), (int64_t)n, index_bytes, err)) {
+      c.err = err;
+      return TPO_E_ARG;
+    }
+  }
+  // buckling and dynamic mode shapes, one file per column (:481-507)
+  const int64_t nd = 3 * c.nn;
+  for (int i = 0; i < nB; ++i)
+    if (!tpo::io::write_vec(d + "phiB" + sfx + "_mode" + std::to_string(i) + ".bin",
+                            phiB + nd * i, nd, index_bytes, err)) {
+      c.err = err;
+      return TPO_E_ARG;
+    }
+  for (int i = 0; i < nD; ++i)
+    if (!tpo::io::write_vec(d + "phiD_" + sfx + "_mode" + std::to_string(i) + ".bin",
+                            phiD + nd * i, nd, index_bytes, err)) {
+      c.err = err;
+      return TPO_E_ARG;
+    }
+  return TPO_OK;
+}
+
+int tpo_load_mesh(const char *folder, const tpo_mesh_params *params, int32_t index_bytes,
+                  tpo_ctx **out) {
+  if (!folder || !params || !out) return io_fail("invalid load arguments");
+  *out = nullptr;
+  const std::string d = folder_prefix(folder);
+  const int ib = index_bytes;
+  std::string err;
+  std::vector<int64_t> edist, ndist, el;
+  std::vector<char> nodes_raw;
+  // distributions, elements, nodes (RecMesh.cpp:42-86)
+  if (!tpo::io::read_ints(d + "Element_Distribution.bin", edist, ib, err) ||
+      !tpo::io::read_ints(d + "Node_Distribution.bin", ndist, ib, err) ||
+      !tpo::io::read_ints(d + "elements.bin", el, ib, err) ||
+      !tpo::io::read_raw(d + "nodes.bin", nodes_raw, err))
+    return io_fail(err);
+  if (edist.size() < 2 || ndist.size() < 2) return io_fail("empty distribution file");
+  const int64_t ne = edist.back(), nn = ndist.back();
+  if (ne < 1 || (int64_t)el.size() != 8 * ne || (int64_t)nodes_raw.size() != 24 * nn)
+    return io_fail("elements.bin / nodes.bin do not hold a 3-D hex8 mesh of the given sizes");
+  const double *xyz = reinterpret_cast<const double *>(nodes_raw.data());
+  // the structured grid: spacing from element 0 (as LoadMesh's elemSize,
+  // :300-306), counts from the extent, then every node and element checked
+  double dx[3], lo[3], hi[3];
+  const int corner[3] = {1, 3, 4};
+  for (int k = 0; k < 3; ++k) {
+    dx[k] = xyz[3 * el[corner[k]] + k] - xyz[3 * el[0] + k];
+    lo[k] = hi[k] = xyz[k];
+  }
+  for (int64_t n = 0; n < nn; ++n)
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = std::min(lo[k], xyz[3 * n + k]);
+      hi[k] = std::max(hi[k], xyz[3 * n + k]);
+    }
+  int nel[3];
+  for (int k = 0; k < 3; ++k) {
+    if (!(dx[k] > 0)) return io_fail("not a structured mesh: non-positive element size");
+    nel[k] = (int)std::llround((hi[k] - lo[k]) / dx[k]);
+  }
+  if ((int64_t)nel[0] * nel[1] * nel[2] != ne ||
+      (int64_t)(nel[0] + 1) * (nel[1] + 1) * (nel[2] + 1) != nn)
+    return io_fail("not a structured box mesh (element and node counts)");
+  for (int64_t e = 0; e < ne; ++e) {
+    int64_t nd[8];
+    tpo::io::element_nodes(nel, e, nd);
+    for (int a = 0; a < 8; ++a)
+      if (el[8 * e + a] != nd[a]) return io_fail("element connectivity is not the structured numbering");
+  }
+  const int64_t NN[3] = {nel[0] + 1, nel[1] + 1, nel[2] + 1};
+  for (int64_t n = 0; n < nn; ++n) {
+    const int64_t idx[3] = {n % NN[0], (n / NN[0]) % NN[1], n / (NN[0] * NN[1])};
+    for (int k = 0; k < 3; ++k) {
+      const double want = lo[k] + idx[k] * dx[k];
+      if (std::fabs(xyz[3 * n + k] - want) > 1e-9 * (std::fabs(hi[k] - lo[k]) + dx[k]))
+        return io_fail("node coordinates are not a regular grid");
+    }
+  }
+  // BC lists (:112-290); springs, eigen-only supports and passive elements
+  // have no counterpart in a context
+  std::vector<int64_t> ln, sn, spn, en;
+  std::vector<char> lv, sv, act;
+  if (!tpo::io::read_ints(d + "loadNodes.bin", ln, ib, err) ||
+      !tpo::io::read_raw(d + "loads.bin", lv, err) ||
+      !tpo::io::read_ints(d + "supportNodes.bin", sn, ib, err) ||
+      !tpo::io::read_raw(d + "supports.bin", sv, err) ||
+      !tpo::io::read_ints(d + "springNodes.bin", spn, ib, err))
+    return io_fail(err);
+  if (lv.size() != 24 * ln.size() || sv.size() != 3 * sn.size())
+    return io_fail("BC value files do not match their node lists");
+  if (!spn.empty()) return io_fail("springs are not supported", TPO_E_UNSUPPORTED);
+  if (tpo::io::read_ints(d + "eigenSupportNodes.bin", en, ib, err) && !en.empty())
+    return io_fail("eigen-analysis supports are not supported", TPO_E_UNSUPPORTED);
+  if (tpo::io::read_raw(d + "active.bin", act, err))
+    for (char a : act)
+      if (!a) return io_fail("passive elements are not supported", TPO_E_UNSUPPORTED);
+  for (int64_t n : ln)
+    if (n < 0 || n >= nn) return io_fail("load node out of range");
+  for (int64_t n : sn)
+    if (n < 0 || n >= nn) return io_fail("support node out of range");
+  // levels: as given, else one more than the interpolations saved
+  tpo_mesh_params p = *params;
+  for (int k = 0; k < 3; ++k) {
+    p.nel[k] = nel[k];
+    p.dx[k] = dx[k];
+  }
+  if (p.mg_levels <= 0) {
+    int cnt = 0;
+    std::vector<char> probe;
+    while (tpo::io::read_raw(d + "P" + std::to_string(cnt) + ".bin", probe, err)) ++cnt;
+    if (cnt > 0) p.mg_levels = cnt + 1;
+  }
+  tpo_ctx *ctx = nullptr;
+  if (int rc = tpo_create(&p, &ctx)) {
+    if (ctx) tpo_destroy(ctx);
+    return io_fail("context creation failed", rc);
+  }
+  Ctx &c = ctx->c;
+  // the saved filter must be the one this context rebuilds from rmin
+  // (:314-325 reads it instead)
+  tpo::io::Csr Pf;
+  if (tpo::io::read_mat(d + "Filter.bin", Pf, ib, err)) {
+    const tpo::io::Csr Q = tpo::io::filter_matrix(c.nel, c.prm.dx, c.prm.rmin, true);
+    bool same = Pf.M == Q.M && Pf.N == Q.N && Pf.rowptr == Q.rowptr && Pf.col == Q.col;
+    for (size_t t = 0; same && t < Q.val.size(); ++t)
+      same = std::fabs(Pf.val[t] - Q.val[t]) <= 1e-12 * std::fabs(Q.val[t]);
+    if (!same) {
+      tpo_destroy(ctx);
+      return io_fail("Filter.bin is not the density filter of radius rmin on this mesh");
+    }
+  }
+  // BCs as the Set_BC lists held them: support flags OR-ed, loads summed
+  const double *lval = reinterpret_cast<const double *>(lv.data());
+  for (size_t i = 0; i < sn.size(); ++i) {
+    c.supp_node.push_back(sn[i]);
+    for (int k = 0; k < 3; ++k) {
+      const bool f = sv[3 * i + k] != 0;
+      c.supp_val.push_back(f);
+      if (f) c.fix_h[sn[i]] |= (uint8_t)(1u << k);
+    }
+  }
+  for (size_t i = 0; i < ln.size(); ++i) {
+    c.load_node.push_back(ln[i]);
+    for (int k = 0; k < 3; ++k) {
+      c.load_val.push_back(lval[3 * i + k]);
+      c.F_h[3 * ln[i] + k] += lval[3 * i + k];
+    }
+  }
+  *out = ctx;
+  return TPO_OK;
+}
+
+int tpo_load_design(tpo_ctx *ctx, const char *folder, const double *penalties, int32_t npen,
+                    double *x, double *penal, int32_t *start, int32_t index_bytes) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  REQUIRE(folder && x && (npen == 0 || penalties), "invalid design-load arguments");
+  const std::string d = folder_prefix(folder);
+  // RecMesh.cpp:391-404: x = 0.5, then x_pen<p>.bin for each penalty in
+  // turn until one is missing; the penalty reached is the one the run
+  // resumes at (Main.cpp:52-56)
+  std::fill(x, x + c.ne, 0.5);
+  double pen = penal ? *penal : 0.0;
+  std::string err;
+  for (int32_t i = 0; i < npen; ++i) {
+    pen = penalties[i];
+    char name[64];
+    std::snprintf(name, sizeof name, "x_pen%g.bin", pen);   // ostream << double
+    std::vector<double> v;
+    std::vector<char> probe;
+    if (!tpo::io::read_raw(d + name, probe, err)) break;
+    if (!tpo::io::read_vec(d + name, v, index_bytes, err)) {
+      c.err = err;
+      return TPO_E_ARG;
+    }
+    REQUIRE((int64_t)v.size() == c.ne, "saved design has the wrong length");
+    std::copy(v.begin(), v.end(), x);
+  }
+  int32_t s = 0;
+  while (s < npen && penalties[s] < pen) ++s;
+  if (penal) *penal = pen;
+  if (start) *start = s;
+  return TPO_OK;
+}
+
+int tpo_load_point_masses(tpo_ctx *ctx, const char *folder, double *mlump,
+                          int32_t index_bytes) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  REQUIRE(folder && mlump, "invalid mass-load arguments");
+  const std::string d = folder_prefix(folder);
+  std::string err;
+  std::vector<int64_t> mn;
+  std::vector<char> mv;
+  // RecMesh.cpp:147-180: massNodes.bin and masses.bin (3 per node)
+  if (!tpo::io::read_ints(d + "massNodes.bin", mn, index_bytes, err) ||
+      !tpo::io::read_raw(d + "masses.bin", mv, err)) {
+    c.err = err;
+    return TPO_E_ARG;
+  }
+  REQUIRE(mv.size() == 24 * mn.size(), "masses.bin does not match massNodes.bin");
+  std::fill(mlump, mlump + 3 * c.nn, 0.0);
+  const double *m = reinterpret_cast<const double *>(mv.data());
+  for (size_t i = 0; i < mn.size(); ++i) {
+    REQUIRE(mn[i] >= 0 && mn[i] < c.nn, "mass node out of range");
+    for (int k = 0; k < 3; ++k) mlump[3 * mn[i] + k] += m[3 * i + k];
+  }
+  return TPO_OK;
+}
 
 }  // extern "C"

@@ -132,6 +132,11 @@ struct Ctx {
   // host-side boundary conditions
   std::vector<uint8_t> fix_h;
   std::vector<double> F_h;
+  // the Set_BC lists (Inputs.cpp:145-170) MeshOut writes: nodes in the
+  // order selected, with per node 3 support flags / 3 load values
+  std::vector<int64_t> supp_node, load_node;
+  std::vector<uint8_t> supp_val;
+  std::vector<double> load_val;
   bool initialized = false;
   bool have_material = false;
   bool assembled = false;

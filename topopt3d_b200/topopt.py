@@ -2,9 +2,13 @@
 
 ``TopOpt`` keeps the reference member names (TopOpt.h:210-292):
 ``Set_BC``, ``FEInitialize``, ``MatIntFnc``, ``FEAssemble``, ``FESolve``,
-``Chain_Filter``; ``Compliance`` and ``Volume`` follow ``Function_Base``
-(Functions.h:16-91) with ``Compute`` and ``Function_Call``; ``OC`` follows
-``MMA::Update`` for a single constraint (MMA.cpp:62-180).  Where the
+``Chain_Filter``, and the output and restart files ``MeshOut``,
+``PrintVals``, ``LoadMesh`` (TopOpt.cpp:97-508, RecMesh.cpp:34-412);
+``Compliance``, ``Volume``, ``Stability`` and ``Frequency`` follow
+``Function_Base`` (Functions.h:16-91) with ``Compute`` and
+``Function_Call``; ``OC`` and ``MMA`` follow ``MMA::Update``
+(MMA.cpp:62-595); ``optimize`` is the loop of Main.cpp:120-178 with the
+Output.txt log of StepOut and ResultOut (TopOpt.cpp:372-435).  Where the
 reference returns a non-zero PetscErrorCode these methods raise
 ``TopOptError``; solver non-convergence is reported, as KUF_reason is, in
 ``last_solve`` without raising.
@@ -16,6 +20,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -69,10 +74,13 @@ class TopOpt:
         rc = self._lib.tpo_create(C.byref(p), C.byref(h))
         if rc != 0:
             raise TopOptError(rc, "tpo_create failed (invalid mesh or no GPU)")
+        self._attach(h)
+
+    def _attach(self, h):
         self._h = h
         ne, nn, nl = C.c_int64(), C.c_int64(), C.c_int32()
         self._lib.tpo_sizes(h, C.byref(ne), C.byref(nn), C.byref(nl))
-        self.nel = tuple(int(t) for t in nel)
+        self.nel = tuple(int(t) - 1 for t in self.level_dims(0))
         self.nElem, self.nNode, self.mg_levels = ne.value, nn.value, nl.value
         self.penal = 3.0
         self.eps = 1e-10           # Material_Interpolation.cpp:28
@@ -264,6 +272,78 @@ class TopOpt:
             mem), "compliance")
         return c.value, dx, dr
 
+    # -- output and restart files (TopOpt.cpp:97-508, RecMesh.cpp:34-412) ---
+    def MeshOut(self, folder=".", rmax=3.0, index_bytes=4):
+        """TopOpt::MeshOut (TopOpt.cpp:97-359) into `folder`; rmax is the
+        max-length-scale filter radius (3 by default, Main.cpp:41).
+        index_bytes is sizeof(PetscInt) of the PETSc build that reads the
+        files."""
+        self._check(self._lib.tpo_mesh_out(self._h, os.fsencode(folder), float(rmax),
+                                           int(index_bytes)), "MeshOut")
+
+    def PrintVals(self, name_suffix, folder=".", phiB=None, phiD=None, index_bytes=4):
+        """TopOpt::PrintVals (TopOpt.cpp:445-508): U, x, V, Es, E and the
+        buckling (phiB) and dynamic (phiD) mode shapes, 3*nNode x modes."""
+        def modes(phi):
+            if phi is None:
+                return None, 0, None
+            a = np.asfortranarray(np.asarray(phi, np.float64).reshape(3 * self.nNode, -1))
+            return a.ctypes.data_as(C.POINTER(C.c_double)), a.shape[1], a
+        pb, nb, kb = modes(phiB)
+        pd, nd, kd = modes(phiD)
+        self._check(self._lib.tpo_print_vals(self._h, os.fsencode(folder),
+                                             str(name_suffix).encode(), pb, nb, pd, nd,
+                                             int(index_bytes)), "PrintVals")
+
+    @classmethod
+    def LoadMesh(cls, folder, E0=1.0, Nu0=0.3, rmin=1.5, mg_levels=0, index_bytes=4):
+        """TopOpt::LoadMesh (RecMesh.cpp:34-412): a problem from a MeshOut
+        folder of a structured hex8 box, with its supports and loads;
+        mg_levels 0 takes the levels the folder's interpolations hold."""
+        lib = L.load()
+        p = L.MeshParams((C.c_int32 * 3)(1, 1, 1), (C.c_double * 3)(1.0, 1.0, 1.0),
+                         float(E0), float(Nu0), float(rmin), int(mg_levels))
+        h = C.c_void_p()
+        rc = lib.tpo_load_mesh(os.fsencode(folder), C.byref(p), int(index_bytes),
+                               C.byref(h))
+        if rc != 0:
+            raise TopOptError(rc, "LoadMesh: " +
+                              lib.tpo_last_error(None).decode(errors="replace"))
+        self = cls.__new__(cls)
+        self._lib = lib
+        self._attach(h)
+        self.penal = 3.0
+        self.eps = 1e-10
+        self.opts = L.default_opts()
+        self.last_solve = None
+        self.function_list = []
+        return self
+
+    def load_design(self, folder, penalties, index_bytes=4):
+        """The design of a restart (RecMesh.cpp:391-404, Main.cpp:52-56):
+        x = 0.5, then x_pen<p>.bin for each penalty in turn until one is
+        missing.  Sets self.penal to the penalty reached and returns
+        (x, index of the first penalty still to run)."""
+        pen = np.ascontiguousarray(penalties, np.float64)
+        x = np.zeros(self.nElem)
+        pn = C.c_double(self.penal)
+        st = C.c_int32()
+        self._check(self._lib.tpo_load_design(
+            self._h, os.fsencode(folder), pen.ctypes.data_as(C.POINTER(C.c_double)),
+            pen.size, x.ctypes.data_as(C.POINTER(C.c_double)), C.byref(pn), C.byref(st),
+            int(index_bytes)), "load_design")
+        self.penal = pn.value
+        return x, st.value
+
+    def load_point_masses(self, folder, index_bytes=4):
+        """massNodes.bin / masses.bin (RecMesh.cpp:147-180) as the 3*nNode
+        point-mass vector `frequency` takes."""
+        m = np.zeros(3 * self.nNode)
+        self._check(self._lib.tpo_load_point_masses(
+            self._h, os.fsencode(folder), m.ctypes.data_as(C.POINTER(C.c_double)),
+            int(index_bytes)), "load_point_masses")
+        return m
+
     def set_stream(self, stream_handle):
         """Issue all work on a caller cudaStream_t (int handle) or None."""
         self._check(self._lib.tpo_set_stream(
@@ -378,6 +458,12 @@ class Function_Base:
 
     def Function(self, topOpt):  # pragma: no cover - abstract
         raise NotImplementedError
+
+    @property
+    def name(self):
+        """Function_Base::name[func_type] (Functions.cpp:5): the class name
+        of Compliance, Volume, Stability, Frequency."""
+        return type(self).__name__
 
     def Compute(self, topOpt):
         """Functions.cpp:39-62: weighted, normalised value and gradient."""
@@ -573,16 +659,71 @@ class MMA(OC):
         return x
 
 
-def optimize(topOpt, optmma, penalties=None, opts=None, callback=None):
-    """The optimisation loop of Main.cpp:130-170: per penalty, MatIntFnc ->
+_STARS = "*" * 48
+
+
+def step_out_text(f, cons, it, function_list):
+    """The Output.txt entry of TopOpt::StepOut (TopOpt.cpp:386-401)."""
+    s = "Iteration number: %d\nObjective: %1.6g\nConstraints:\n" % (it, f)
+    s += "".join("\t%1.12g\t" % c for c in cons)
+    s += "\nAll function values:\n"
+    s += "".join("\t%12s: %1.8g\n" % (fn.name, fn.value) for fn in function_list)
+    return s + "\n"
+
+
+def result_out_text(it, penal, Esum, Vsum):
+    """The Output.txt entry of TopOpt::ResultOut (TopOpt.cpp:421-425)."""
+    return ("%s\nAfter %4i iterations with a penalty of %1.4g the\n"
+            "ratio of stiffness sum to volume sum is %1.4g\n%s\n\n"
+            % (_STARS, it, penal, Esum / Vsum, _STARS))
+
+
+def optimize(topOpt, optmma, penalties=None, opts=None, callback=None, output=None,
+             folder=None, print_every=None, index_bytes=4):
+    """The optimisation loop of Main.cpp:120-178: per penalty, MatIntFnc ->
     FEAssemble -> FESolve -> Function_Call, then Update + re-evaluate until
     Check() (a do-while, so maxiter updates and maxiter + 1 evaluations).
     FESolve warm-starts from the previous U (FEAnalysis.cpp:389).
 
-    Returns one record per evaluation (the fields StepOut prints,
-    TopOpt.cpp:372-405, plus the solver outcome)."""
+    `output` (a path or a text file) receives the Output.txt log: the
+    penalty line of Main.cpp:134, StepOut after every evaluation and
+    ResultOut after every penalty (TopOpt.cpp:372-435).  With `folder`,
+    PrintVals writes the state there every `print_every` iterations
+    (_pen<p>_it<i>) and at the end of every penalty (_pen<p>), as StepOut
+    and ResultOut do.
+
+    Returns one record per evaluation (the fields StepOut prints plus the
+    solver outcome)."""
     hist = []
     penalties = [topOpt.penal] if penalties is None else list(penalties)
+    own = isinstance(output, (str, bytes, os.PathLike))
+    log = open(output, "w") if own else output
+    every = print_every if print_every else 2**31 - 1     # INT_MAX by default
+    last_print = 0
+
+    def step_out(f, g, it):
+        nonlocal last_print
+        last_print += 1
+        if every - last_print == 0:
+            if folder is not None:
+                topOpt.PrintVals("_pen%1.4g_it%i" % (topOpt.penal, it), folder,
+                                 index_bytes=index_bytes)
+            last_print = 0
+        last_print *= it > 0
+        if log is not None:
+            log.write(step_out_text(f, g, it, topOpt.function_list))
+
+    def result_out(it):
+        nonlocal last_print
+        if log is not None:
+            E = np.zeros(topOpt.nElem)
+            V = np.zeros(topOpt.nElem)
+            topOpt.get("E", E)
+            topOpt.get("rho", V)
+            log.write(result_out_text(it, topOpt.penal, E.sum(), V.sum()))
+        if folder is not None:
+            topOpt.PrintVals("_pen%1.4g" % topOpt.penal, folder, index_bytes=index_bytes)
+        last_print = 0
 
     def evaluate(it):
         topOpt.MatIntFnc(optmma.xval)
@@ -595,15 +736,23 @@ def optimize(topOpt, optmma, penalties=None, opts=None, callback=None):
         hist.append(rec)
         if callback is not None:
             callback(rec)
+        step_out(f, g, it)
         return dfdx, g, dgdx
 
-    for p in penalties:
-        topOpt.penal = float(p)
-        optmma.iter = 0
-        dfdx, g, dgdx = evaluate(0)
-        while True:
-            optmma.Update(topOpt, dfdx, g, dgdx)
-            dfdx, g, dgdx = evaluate(optmma.iter + 1)
-            if optmma.Check():
-                break
+    try:
+        for p in penalties:
+            topOpt.penal = float(p)
+            if log is not None:
+                log.write("\nPenalty increased to %1.3g\n" % topOpt.penal)
+            optmma.iter = 0
+            dfdx, g, dgdx = evaluate(0)
+            while True:
+                optmma.Update(topOpt, dfdx, g, dgdx)
+                dfdx, g, dgdx = evaluate(optmma.iter + 1)
+                if optmma.Check():
+                    break
+            result_out(optmma.iter)
+    finally:
+        if own:
+            log.close()
     return hist
