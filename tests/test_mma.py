@@ -58,7 +58,7 @@ def test_oracle_mma_solves_a_convex_problem(oracle):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("m", [2, 3])
+@pytest.mark.parametrize("m", [2, 3, 8])
 def test_mma_update_matches_oracle(T, oracle, m):
     nel = (12, 6, 6)
     t = T.TopOpt(nel)
@@ -71,7 +71,7 @@ def test_mma_update_matches_oracle(T, oracle, m):
     for it in range(6):
         dfdx = -rng.uniform(0.1, 2.0, n)
         dgdx = rng.uniform(0.0, 1.0, (n, m)) / n
-        if m == 3:
+        if m >= 3:
             dgdx[:, 2] -= 0.5 / n          # a constraint with mixed-sign gradient
         g = rng.uniform(-0.05, 0.05, m)
         ch_o = oracle.mma_update(st_o, dfdx, g, dgdx, it)
@@ -126,3 +126,45 @@ def test_mma_compliance_two_volume_constraints(T, oracle):
     np.testing.assert_allclose(C_gpu, np.array(C_o), rtol=1e-7)
     assert C_gpu[-1] < C_gpu[0]
     assert abs(hist[-1]["values"][1] - limits[0]) < 5e-3
+
+
+@pytest.mark.gpu
+def test_mma_abi_one_constraint_and_limits(T, oracle):
+    """tpo_mma_update is MMAsub for any 1 <= m <= 8 (MMA::Update sends
+    m < 2 to OCsub before it, as the MMA classes do): m = 1 against the
+    oracle over four updates; m = 0 and m = 9 are refused."""
+    import ctypes as C
+    from topopt3d_b200 import _lib as L
+    t = T.TopOpt((8, 4, 4))
+    n = t.nElem
+    rng = np.random.default_rng(5)
+    x0 = rng.uniform(0.2, 0.8, n)
+    st_o = new_state(x0)
+    state = [x0.copy(), x0.copy(), x0.copy(), np.zeros(n), np.ones(n)]
+    bounds = [np.zeros(n), np.ones(n)]
+    ptr = lambda a: a.ctypes.data_as(C.c_void_p)
+    opts = L.default_mma_opts()
+    fresh, ch = C.c_int32(1), C.c_double()
+
+    def call(m, dfdx, g, dgdx, it):
+        gg = np.ascontiguousarray(g, np.float64)
+        return t._lib.tpo_mma_update(t._h, C.byref(opts), it, C.byref(fresh), m,
+                                     *[ptr(a) for a in state], *[ptr(a) for a in bounds],
+                                     ptr(dfdx), gg.ctypes.data_as(C.POINTER(C.c_double)),
+                                     ptr(np.asfortranarray(dgdx)), C.byref(ch), L.MEM_HOST)
+
+    for it in range(4):
+        dfdx = -rng.uniform(0.1, 2.0, n)
+        dgdx = rng.uniform(0.0, 1.0, (n, 1)) / n
+        g = rng.uniform(-0.05, 0.05, 1)
+        ch_o = oracle.mma_update(st_o, dfdx, g, dgdx, it)
+        assert call(1, dfdx, g, dgdx, it) == 0
+        np.testing.assert_allclose(state[0], st_o["x"], rtol=0, atol=1e-9)
+        np.testing.assert_allclose(state[3], st_o["low"], rtol=1e-9, atol=1e-12)
+        np.testing.assert_allclose(state[4], st_o["upp"], rtol=1e-9, atol=1e-12)
+        assert abs(ch.value - ch_o) <= 1e-9
+        assert bool(fresh.value) == st_o["fresh_start"]
+    dfdx = -np.ones(n)
+    for m in (0, 9):
+        assert call(m, dfdx, np.zeros(max(m, 1)), np.zeros((n, max(m, 1))), 0) < 0
+        assert b"1 <= m <= 8" in t._lib.tpo_last_error(t._h)

@@ -457,15 +457,16 @@ __global__ void __launch_bounds__(256) k_mma_solve(MmaSolveArgs a) {
       const double pr = sqrt(plam), qr = sqrt(qlam);
       const double xi = fmax(fmin((pr * lo + qr * up) / (pr + qr), be), al);
       a.x[i] = xi;
-      const double ux1 = up - xi, xl1 = xi - lo;
-      const double ux2 = ux1 * ux1, xl2 = xl1 * xl1;
+      // 1/(U - x) and 1/(x - L) once; the sums and dLdxx from products
+      const double iu = 1.0 / (up - xi), il = 1.0 / (xi - lo);
+      const double iu2 = iu * iu, il2 = il * il;
       const double inside = (xi > al && xi < be) ? 1.0 : 0.0;
-      const double dL = inside / (2 * plam / (ux2 * ux1) + 2 * qlam / (xl2 * xl1));
+      const double dL = inside / (2 * plam * (iu2 * iu) + 2 * qlam * (il2 * il));
       double dh[M];
 #pragma unroll
       for (int j = 0; j < M; ++j) {
-        acc[j] += Pj[j] / ux1 + Qj[j] / xl1;
-        dh[j] = Pj[j] / ux2 - Qj[j] / xl2;
+        acc[j] += Pj[j] * iu + Qj[j] * il;
+        dh[j] = Pj[j] * iu2 - Qj[j] * il2;
       }
       int t = M;
 #pragma unroll
