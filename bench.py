@@ -54,7 +54,7 @@ def parse():
     # --config also selects the reference arm's problem (default 192x96x96)
     ap.add_argument("--kernel", default=None,
                     choices=["apply32", "apply64", "vcycle32", "vcycle64",
-                             "solve_mixed", "solve_fp64", "mma"])
+                             "solve_mixed", "solve_fp64", "mma", "setup"])
     ap.add_argument("--config", default=CONFIG)
     ap.add_argument("--reps", type=int, default=3)
     return ap.parse_args()
@@ -739,6 +739,10 @@ def run_kernel_case(args):
                                     g2.ctypes.data_as(C.POINTER(C.c_double)), ptr(dgd),
                                     C.byref(ch), L.MEM_DEVICE)
             assert rc == 0, lib.tpo_last_error(t._h)
+            continue
+        if args.kernel == "setup":
+            # FEAssemble / PCSetUp for the same design: the whole hierarchy
+            t.FEAssemble()
             continue
         if args.kernel == "apply32":
             rc = lib.tpo_apply_f32(t._h, C.c_void_p(u32.data_ptr()),
