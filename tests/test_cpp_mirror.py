@@ -28,6 +28,27 @@ def test_cpp_mirror_compiles(tmp_path):
     assert os.path.exists(build_mirror(tmp_path))
 
 
+def test_cpp_step_out_matches_python_log(tmp_path):
+    """tpo::StepOut and the Python optimize log write the same Output.txt
+    entry for the same values."""
+    from topopt3d_b200 import build
+    from topopt3d_b200.topopt import step_out_text
+    build.build()
+    exe = str(tmp_path / "stepout_main")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "stepout_main.cpp"), "-o", exe, "-L",
+                    LIBDIR, "-ltopopt_b200", "-Wl,-rpath," + LIBDIR], check=True)
+    out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout
+
+    class Fn:
+        def __init__(self, name, value):
+            self.name, self.value = name, value
+
+    assert out == step_out_text(12.3456789, [-0.00123456789012345, 0.5], 7,
+                                [Fn("Compliance", 12.3456789),
+                                 Fn("Volume", -0.00123456789012345)])
+
+
 @pytest.mark.gpu
 def test_cpp_mirror_matches_oracle(tmp_path, oracle):
     exe = build_mirror(tmp_path)

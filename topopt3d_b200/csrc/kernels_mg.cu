@@ -255,34 +255,56 @@ __global__ void k_galerkin_dim(int nx, int ny, int nz, const double *__restrict_
 }
 
 
+// 32 nodes x 9 neighbour rows per CTA: thread (lane, g) takes node
+// 32 * block + lane and the three neighbour blocks of row g = (dj, dk),
+// i.e. 27 coefficient and 9 u loads, so the loads of a node are spread
+// over 9 threads instead of one 324-load chain (the levels this kernel
+// serves are small and latency-bound); the 9 partial sums are combined in
+// shared memory in a fixed order.  Lanes span consecutive nodes, so each
+// coefficient load is coalesced.
+constexpr int kStencilRows = 9;
 template <typename T, bool RESID>
-__global__ void k_apply_stencil(int nx, int ny, int nz, const T *__restrict__ S,
-                                const T *__restrict__ u, const T *__restrict__ b,
-                                T *__restrict__ y) {
+__global__ void __launch_bounds__(32 * kStencilRows)
+    k_apply_stencil(int nx, int ny, int nz, const T *__restrict__ S,
+                    const T *__restrict__ u, const T *__restrict__ b,
+                    T *__restrict__ y) {
+  __shared__ T part[kStencilRows][3][32];
   const int64_t nn = (int64_t)nx * ny * nz;
-  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
-       n += (int64_t)gridDim.x * blockDim.x) {
-    const int i = n % nx, j = (n / nx) % ny, k = n / ((int64_t)nx * ny);
+  const int lane = threadIdx.x, g = threadIdx.y;
+  const int dj = g % 3 - 1, dk = g / 3 - 1;
+  for (int64_t n0 = (int64_t)blockIdx.x * 32; n0 < nn; n0 += (int64_t)gridDim.x * 32) {
+    const int64_t n = n0 + lane;
     T a0 = 0, a1 = 0, a2 = 0;
+    if (n < nn) {
+      const int i = (int)(n % nx), j = (int)((n / nx) % ny), k = (int)(n / ((int64_t)nx * ny));
+      const int mj = j + dj, mk = k + dk;
+      if (mj >= 0 && mj < ny && mk >= 0 && mk < nz) {
 #pragma unroll
-    for (int nb = 0; nb < 27; ++nb) {
-      const int mi = i + nb % 3 - 1, mj = j + (nb / 3) % 3 - 1, mk = k + nb / 9 - 1;
-      if (mi < 0 || mi >= nx || mj < 0 || mj >= ny || mk < 0 || mk >= nz) continue;
-      const int64_t m = ((int64_t)mk * ny + mj) * nx + mi;
-      const T u0 = u[3 * m], u1 = u[3 * m + 1], u2 = u[3 * m + 2];
-      const T *s = S + (int64_t)nb * 9 * nn + n;
-      a0 += s[0] * u0 + s[nn] * u1 + s[2 * nn] * u2;
-      a1 += s[3 * nn] * u0 + s[4 * nn] * u1 + s[5 * nn] * u2;
-      a2 += s[6 * nn] * u0 + s[7 * nn] * u1 + s[8 * nn] * u2;
+        for (int di = -1; di <= 1; ++di) {
+          const int mi = i + di;
+          if (mi < 0 || mi >= nx) continue;
+          const int nb = g * 3 + di + 1;
+          const int64_t m = ((int64_t)mk * ny + mj) * nx + mi;
+          const T u0 = u[3 * m], u1 = u[3 * m + 1], u2 = u[3 * m + 2];
+          const T *s = S + (int64_t)nb * 9 * nn + n;
+          a0 += s[0] * u0 + s[nn] * u1 + s[2 * nn] * u2;
+          a1 += s[3 * nn] * u0 + s[4 * nn] * u1 + s[5 * nn] * u2;
+          a2 += s[6 * nn] * u0 + s[7 * nn] * u1 + s[8 * nn] * u2;
+        }
+      }
     }
-    if (RESID) {
-      a0 = b[3 * n] - a0;
-      a1 = b[3 * n + 1] - a1;
-      a2 = b[3 * n + 2] - a2;
+    part[g][0][lane] = a0;
+    part[g][1][lane] = a1;
+    part[g][2][lane] = a2;
+    __syncthreads();
+    if (g < 3 && n < nn) {
+      T a = 0;
+#pragma unroll
+      for (int r = 0; r < kStencilRows; ++r) a += part[r][g][lane];
+      if (RESID) a = b[3 * n + g] - a;
+      y[3 * n + g] = a;
     }
-    y[3 * n] = a0;
-    y[3 * n + 1] = a1;
-    y[3 * n + 2] = a2;
+    __syncthreads();
   }
 }
 
@@ -586,12 +608,13 @@ template <typename T>
 void launch_apply_stencil(const Level &v, const T *S, const T *u, const T *b,
                           T *y, cudaStream_t s) {
   count_launch();
-  const int g = grid_for(v.nn, 128);
+  const int g = grid_for(v.nn, 32);
+  const dim3 blk(32, kStencilRows);
   if (b)
-    k_apply_stencil<T, true><<<g, 128, 0, s>>>(v.dims[0], v.dims[1], v.dims[2],
+    k_apply_stencil<T, true><<<g, blk, 0, s>>>(v.dims[0], v.dims[1], v.dims[2],
                                                S, u, b, y);
   else
-    k_apply_stencil<T, false><<<g, 128, 0, s>>>(v.dims[0], v.dims[1], v.dims[2],
+    k_apply_stencil<T, false><<<g, blk, 0, s>>>(v.dims[0], v.dims[1], v.dims[2],
                                                 S, u, b, y);
 }
 template void launch_apply_stencil<double>(const Level &, const double *,
