@@ -5,7 +5,9 @@ LoadMesh and the Output.txt log.
 CPU: the library's PETSc-binary writers and readers against the oracle's
 independent numpy restatement, both ways, for 4- and 8-byte PetscInt, with
 the error cases; the StepOut / ResultOut text against literal strings
-written from the reference's printf formats.
+written from the reference's printf formats; LoadMesh's refusals of folders
+that are not a structured box or hold springs, eigen-only supports or
+passive elements.
 
 GPU: MeshOut's files against the oracle's mesh, BC selection, filters and
 interpolation weights; PrintVals against the context's vectors; LoadMesh of
@@ -340,3 +342,110 @@ def test_optimize_output_log_and_print_schedule(T, tmp_path):
     assert not os.path.exists(tmp_path / "U_pen3_it1.bin")
     assert not os.path.exists(tmp_path / "U_pen3_it3.bin")
     np.testing.assert_array_equal(PIO.read_vec(str(tmp_path / "x_pen3.bin")), oc.xval)
+
+
+# ------------------------------------------------ LoadMesh refusals (CPU)
+
+def write_mesh_folder(d, oracle, nel=(3, 2, 2), ib=4):
+    """A MeshOut-style folder of a structured box written with numpy from
+    the oracle's mesh data (one support node, one load node)."""
+    d.mkdir(exist_ok=True)
+    idt = "<i4" if ib == 4 else "<i8"
+    ne, nn = int(np.prod(nel)), int(np.prod([n + 1 for n in nel]))
+    w = lambda name, a, dt: np.asarray(a, dt).tofile(str(d / name))
+    w("Element_Distribution.bin", [0, ne], idt)
+    w("Node_Distribution.bin", [0, nn], idt)
+    w("elements.bin", np.stack([oracle.element_nodes(nel, e) for e in range(ne)]), idt)
+    w("nodes.bin", oracle.node_coords(nel, (1.0, 1.0, 1.0)), "<f8")
+    w("supportNodes.bin", [0], idt)
+    w("supports.bin", [1, 1, 1], np.uint8)
+    w("loadNodes.bin", [nn - 1], idt)
+    w("loads.bin", [0.0, 0.0, -1.0], "<f8")
+    for name in ("eigenSupportNodes", "springNodes", "massNodes"):
+        w(name + ".bin", [], idt)
+    for name in ("eigenSupports", "springs", "masses"):
+        w(name + ".bin", [], np.uint8)
+    w("active.bin", np.ones(ne), np.uint8)
+    return ne, nn
+
+
+def load_mesh_error(folder, ib=4):
+    lib = L.load()
+    p = L.MeshParams((C.c_int32 * 3)(1, 1, 1), (C.c_double * 3)(1.0, 1.0, 1.0),
+                     1.0, 0.3, 1.5, 0)
+    h = C.c_void_p()
+    rc = lib.tpo_load_mesh(str(folder).encode(), C.byref(p), ib, C.byref(h))
+    if rc == 0:
+        lib.tpo_destroy(h)
+    return rc, lib.tpo_last_error(None)
+
+
+def test_load_mesh_refusals(tmp_path, oracle):
+    """The checks of tpo_load_mesh that run before a context exists: a
+    folder that is not a structured hex8 box, or that holds data a context
+    cannot represent, is refused with a message."""
+    ne, nn = write_mesh_folder(tmp_path / "ok", oracle)
+    rc, msg = load_mesh_error(tmp_path / "ok")
+    # a valid folder passes every check; creating the context then needs a GPU
+    assert rc == 0 or b"context creation failed" in msg, msg
+
+    d = tmp_path / "perm"
+    write_mesh_folder(d, oracle)
+    el = np.fromfile(str(d / "elements.bin"), "<i4").reshape(ne, 8)
+    el[1, [1, 3]] = el[1, [3, 1]]
+    el.tofile(str(d / "elements.bin"))
+    rc, msg = load_mesh_error(d)
+    assert rc < 0 and b"structured numbering" in msg
+    el[1, [1, 3]] = el[1, [3, 1]]
+    el[0, [1, 3]] = el[0, [3, 1]]        # element 0 sets the spacing
+    el.tofile(str(d / "elements.bin"))
+    rc, msg = load_mesh_error(d)
+    assert rc < 0 and b"element size" in msg
+
+    d = tmp_path / "skew"
+    write_mesh_folder(d, oracle)
+    xyz = np.fromfile(str(d / "nodes.bin"), "<f8").reshape(nn, 3)
+    xyz[5, 1] += 0.25
+    xyz.tofile(str(d / "nodes.bin"))
+    rc, msg = load_mesh_error(d)
+    assert rc < 0 and b"regular grid" in msg
+
+    d = tmp_path / "spring"
+    write_mesh_folder(d, oracle)
+    np.asarray([2], "<i4").tofile(str(d / "springNodes.bin"))
+    np.asarray([1.0, 1.0, 1.0], "<f8").tofile(str(d / "springs.bin"))
+    rc, msg = load_mesh_error(d)
+    assert rc == L.TPO_E_UNSUPPORTED and b"springs" in msg
+
+    d = tmp_path / "eigen"
+    write_mesh_folder(d, oracle)
+    np.asarray([1], "<i4").tofile(str(d / "eigenSupportNodes.bin"))
+    rc, msg = load_mesh_error(d)
+    assert rc == L.TPO_E_UNSUPPORTED and b"eigen-analysis supports" in msg
+
+    d = tmp_path / "passive"
+    write_mesh_folder(d, oracle)
+    act = np.ones(ne, np.uint8)
+    act[1] = 0
+    act.tofile(str(d / "active.bin"))
+    rc, msg = load_mesh_error(d)
+    assert rc == L.TPO_E_UNSUPPORTED and b"passive" in msg
+
+    d = tmp_path / "bcsize"
+    write_mesh_folder(d, oracle)
+    np.asarray([0.0, 1.0], "<f8").tofile(str(d / "loads.bin"))
+    rc, msg = load_mesh_error(d)
+    assert rc < 0 and b"do not match" in msg
+
+    d = tmp_path / "missing"
+    write_mesh_folder(d, oracle)
+    os.remove(d / "nodes.bin")
+    rc, msg = load_mesh_error(d)
+    assert rc < 0 and b"cannot open" in msg and b"nodes.bin" in msg
+
+    # 8-byte PetscInt files read with 8, refused with 4
+    write_mesh_folder(tmp_path / "ib8", oracle, ib=8)
+    rc, msg = load_mesh_error(tmp_path / "ib8", ib=8)
+    assert rc == 0 or b"context creation failed" in msg, msg
+    rc, msg = load_mesh_error(tmp_path / "ib8", ib=4)
+    assert rc < 0
