@@ -281,6 +281,14 @@ def test_print_vals_load_mesh_and_restart(T, oracle, tmp_path):
     m2, F2 = t2.get_bc()
     np.testing.assert_array_equal(m1, m2)
     np.testing.assert_array_equal(F1, F2)
+    # MeshOut of the reloaded problem writes the same files, byte for byte
+    os.makedirs(tmp_path / "again")
+    t2.MeshOut(str(tmp_path / "again"))
+    names = sorted(n for n in os.listdir(tmp_path) if n.endswith((".bin", ".split"))
+                   and not n.endswith("_pen3.bin") and "_mode" not in n)
+    assert len(names) == 20
+    for n in names:
+        assert (tmp_path / n).read_bytes() == (tmp_path / "again" / n).read_bytes(), n
     xr, start = t2.load_design(str(tmp_path), [3.0, 4.0])
     np.testing.assert_array_equal(xr, x)
     assert t2.penal == 4.0 and start == 1
