@@ -435,6 +435,14 @@ __global__ void k_apply_stencil_sym(int nx, int ny, int nz,
     for (int h = 0; h < 14; ++h) {
       const int nb = 13 + h;
       const int di = nb % 3 - 1, dj = (nb / 3) % 3 - 1, dk = nb / 9 - 1;
+      // FP32: the forward block two steps ahead into L2, as in the
+      // single-column kernel
+      if (sizeof(T) == 4 && h + 2 < 14) {
+        const T *pf = H + (int64_t)(h + 2) * 9 * nn + n;
+#pragma unroll
+        for (int q = 0; q < 9; ++q)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(pf + q * (int64_t)nn));
+      }
       // forward block A(n, n+d): zero when n+d is outside, index clamped
       {
         const int mi = min(i + di, nx - 1), mj = min(max(j + dj, 0), ny - 1),
