@@ -57,6 +57,36 @@ def test_oracle_mma_solves_a_convex_problem(oracle):
     assert ch < 1e-4
 
 
+def test_oracle_mma_nonlinear_constraints(oracle):
+    """min |x|^2 subject to two sphere constraints |x - c_i|^2 <= 9 over
+    [0, 5]^3 (the curvature enters both asymptote terms P and Q), by 60
+    MMA updates from (4, 3, 2), against scipy's SLSQP."""
+    from scipy.optimize import minimize
+    c1, c2 = np.array([5.0, 2.0, 1.0]), np.array([3.0, 4.0, 3.0])
+
+    def cons(x):
+        return np.array([np.sum((x - c1) ** 2) - 9.0, np.sum((x - c2) ** 2) - 9.0])
+
+    def cons_grad(x):
+        return np.stack([2 * (x - c1), 2 * (x - c2)], axis=1)
+
+    x0 = np.array([4.0, 3.0, 2.0])
+    st = new_state(x0, np.zeros(3), np.full(3, 5.0))
+    for it in range(60):
+        x = st["x"]
+        oracle.mma_update(st, 2 * x, cons(x), cons_grad(x), it)
+    x = st["x"]
+    ref = minimize(lambda v: np.sum(v ** 2), x0, jac=lambda v: 2 * v,
+                   bounds=[(0, 5)] * 3, method="SLSQP",
+                   constraints=[{"type": "ineq", "fun": lambda v: -cons(v),
+                                 "jac": lambda v: -cons_grad(v).T}],
+                   options={"ftol": 1e-14, "maxiter": 500})
+    # SLSQP stops on its line search at this ftol; its point is feasible
+    assert np.all(cons(ref.x) <= 1e-9)
+    assert np.all(cons(x) <= 1e-6)
+    np.testing.assert_allclose(x, ref.x, atol=1e-5)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("m", [2, 3, 8])
 def test_mma_update_matches_oracle(T, oracle, m):
