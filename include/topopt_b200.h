@@ -316,8 +316,10 @@ TPO_API int64_t tpo_kernel_launches(void);
  * (4 by default, 8 with 64-bit indices).  Raw arrays are native-endian as
  * the reference writes them with ofstream / MPI-IO; the PETSc binary
  * viewer encoding is big-endian.  One process: the distributions are
- * [0, nElem] and [0, nNode].  No .info side files are written.  Calls
- * without a context report errors through tpo_last_error(NULL). */
+ * [0, nElem] and [0, nNode].  No .info side files are written.  Writers
+ * expect `folder` to exist (the reference writes into the working
+ * directory).  Calls without a context report errors through
+ * tpo_last_error(NULL). */
 
 /* VecView / VecLoad on a binary viewer: [1211214, n] as PetscInt, then n
  * doubles.  tpo_read_vec_bin with v = NULL returns the length only. */
