@@ -261,8 +261,11 @@ def run_ours(args, rank, world, local):
     fp64 = T.default_opts(precision=T.PREC_FP64)
     ms_mx, launches, clocks = timed(mixed, args.steps, args.warmup, sample_clocks=True)
     info_mx = infos[-1]
+    # the last timed step's solution, for the comparison with the oracle
+    sol_mx = (t.U, info_mx[1], dc.cpu().numpy())
     ms_64, _, _ = timed(fp64, args.steps, args.warmup)
     info_64 = infos[-1]
+    sol_64 = (t.U, info_64[1], dc.cpu().numpy())
     ms_mx = max_over_ranks(ms_mx, world)
     ms_64 = max_over_ranks(ms_64, world)
     value = world * args.steps / (ms_mx / 1e3)
@@ -342,7 +345,18 @@ def run_ours(args, rank, world, local):
     if not args.no_e2e:
         line["e2e"] = run_e2e(args, T, P, t, x, world, dev, torch)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(sample_its=3)
+        cb = cpu_baseline()
+        Uo, Co, dco = cb.pop("_solution")
+        line["cpu_baseline"] = cb
+        # the acceptance check: both GPU forms against the FP64 oracle's
+        # solution of the same problem (relative 2-norm errors)
+        nrel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        line["vs_oracle"] = {
+            form: {"compliance_rel_err": abs(sol[1] - Co) / abs(Co),
+                   "u_rel_err": nrel(sol[0], Uo), "dcdx_rel_err": nrel(sol[2], dco)}
+            for form, sol in (("mixed", sol_mx), ("fp64", sol_64))}
+        line["vs_oracle"]["oracle_iterations"] = cb["iterations"]
+        line["compliance_rel_err_vs_oracle"] = line["vs_oracle"]["mixed"]["compliance_rel_err"]
     return line
 
 
@@ -617,12 +631,13 @@ def run_e2e(args, T, P, t, x, world, dev, torch):
 
 # ------------------------------------------------------------ CPU baseline
 
-def cpu_baseline(sample_its=3, steps=None, warmup=0, cfg=CONFIG):
+def cpu_baseline(steps=None, warmup=0, cfg=CONFIG):
     """The oracle's assembled FP64 PCG + GMG (OpenMP, all host threads) on
-    the same problem (192x96x96 unless `cfg` names another).  Without `steps`: one complete solve from
-    U = 0 is timed (solves/s = 1 / its time).  With `steps` (the reference
-    arm): each step runs `sample_its` PCG iterations and solves/s = 1 /
-    (per-iteration time x iterations of the full solve)."""
+    the same problem (192x96x96 unless `cfg` names another).  Without
+    `steps`: one complete solve from U = 0 is timed (solves/s = 1 / its
+    time) and its solution is returned under "_solution".  With `steps`
+    (the reference arm): `warmup` untimed and `steps` timed complete solves
+    from U = 0; solves/s = 1 / their mean time."""
     from oracle import oracle as O
     from topopt3d_b200 import problems as P
     c = P.CONFIGS[cfg]
@@ -635,42 +650,37 @@ def cpu_baseline(sample_its=3, steps=None, warmup=0, cfg=CONFIG):
     ref.assemble(O.default_opts())
     setup_s = time.perf_counter() - t0
     t0 = time.perf_counter()
-    _, st, its_full, rr = ref.solve(opts=O.default_opts())
+    U, st, its_full, rr = ref.solve(opts=O.default_opts())
     full_s = time.perf_counter() - t0
     if not steps:
+        C, dc, _ = ref.compliance(U)
         return {"value": round(1.0 / full_s, 6), "unit": UNIT, "cores": cores,
                 "kind": "port",
                 "sample": f"one complete FP64 PCG+GMG solve from U=0 of the {mesh} "
                           f"problem ({its_full} iterations, relres {rr:.2e}, status {st}; "
                           f"assembled BSR SpMV, Galerkin PtAP, OpenMP); set-up "
                           f"{setup_s:.1f} s untimed",
-                "full_solve_s": full_s, "setup_s": setup_s}
+                "full_solve_s": full_s, "setup_s": setup_s, "iterations": its_full,
+                "_solution": (U, C, dc)}
 
-    def sample():
-        o0 = O.default_opts(rtol=1e-300, maxit=0)
+    def full_solve():
         t0 = time.perf_counter()
-        ref.solve(opts=o0)
-        base = time.perf_counter() - t0
-        o = O.default_opts(rtol=1e-300, maxit=sample_its)
-        t0 = time.perf_counter()
-        ref.solve(opts=o)
-        return (time.perf_counter() - t0 - base) / sample_its
+        _, st_s, its_s, _ = ref.solve(opts=O.default_opts())
+        if st_s != 0:
+            raise RuntimeError(f"oracle solve failed: status {st_s}")
+        return time.perf_counter() - t0, its_s
 
-    per_it = sample()
-    out = {"value": round(1.0 / (per_it * its_full), 6), "unit": UNIT,
-           "cores": cores, "kind": "port",
-           "sample": f"{sample_its} PCG+GMG iterations of the {mesh} problem "
-                     f"(assembled BSR SpMV, FP64, OpenMP) x {its_full} iterations of "
-                     f"the full solve; setup {setup_s:.1f} s and a full solve "
-                     f"({full_s:.1f} s, status {st}) untimed",
-           "per_iteration_s": per_it, "full_solve_s": full_s}
-    if steps:
-        for _ in range(warmup):
-            sample()
-        ts = [sample() for _ in range(steps)]
-        out["per_iteration_s"] = statistics.mean(ts)
-        out["value"] = round(1.0 / (out["per_iteration_s"] * its_full), 6)
-    return out
+    for _ in range(warmup):
+        full_solve()
+    runs = [full_solve() for _ in range(steps)]
+    mean_s = statistics.mean(r[0] for r in runs)
+    return {"value": round(1.0 / mean_s, 6), "unit": UNIT, "cores": cores,
+            "kind": "port",
+            "sample": f"{steps} complete FP64 PCG+GMG solves from U=0 of the {mesh} "
+                      f"problem ({its_full} iterations each; assembled BSR SpMV, "
+                      f"Galerkin PtAP, OpenMP), mean time per solve; set-up "
+                      f"{setup_s:.1f} s and {warmup + 1} warm-up solve(s) untimed",
+            "solve_s": mean_s, "iterations": its_full}
 
 
 def run_reference(args, rank, world):
@@ -679,8 +689,8 @@ def run_reference(args, rank, world):
     so its CPU path runs as the oracle restatement."""
     if rank != 0:
         return None
-    cb = cpu_baseline(sample_its=2, steps=args.steps, warmup=min(args.warmup, 1),
-                      cfg=args.config)
+    # the first complete solve (for the iteration count) is the warm-up
+    cb = cpu_baseline(steps=args.steps, warmup=0, cfg=args.config)
     return {"impl": "reference", "metric": METRIC, "value": cb["value"],
             "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",

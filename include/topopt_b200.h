@@ -369,6 +369,24 @@ TPO_API int tpo_load_design(tpo_ctx *ctx, const char *folder, const double *pena
 TPO_API int tpo_load_point_masses(tpo_ctx *ctx, const char *folder, double *mlump,
                                   int32_t index_bytes);
 
+/* Self-test of the failure detection of the persistent kernels.  It has no
+ * counterpart in the reference, whose only failure reporting is the solver
+ * status (FEAnalysis.cpp:677-684).  The coarse-grid V-cycle, the OC
+ * bisection and the MMA update each run as one cooperative launch whose
+ * phases are separated by a grid barrier with a bounded wait; a wait that
+ * runs out sets a fault flag, every block returns, and the next read-back
+ * reports TPO_E_CUDA and resets the barrier.  This call runs that
+ * machinery on its own: `blocks` (1..64) co-resident blocks cross `phases`
+ * (1..1024) barriers; when skip_block is in [0, blocks) that block leaves
+ * before its first arrival, so the other blocks' waits run out after
+ * max_polls (1..2^22) polls each.  *completed (optional) receives the
+ * number of blocks that passed every barrier.  Returns TPO_OK when all
+ * arrived, TPO_E_CUDA with a message after a wait ran out (the counter and
+ * the flag are reset, the context stays usable). */
+TPO_API int tpo_barrier_selftest(tpo_ctx *ctx, int32_t blocks, int32_t phases,
+                                 int32_t skip_block, int32_t max_polls,
+                                 int32_t *completed);
+
 /* Filtered compliance sensitivity that allocates nothing.  It has no
  * counterpart in the reference.  It serves callers that may not call
  * cudaMalloc: a plugin whose host framework owns all device memory through

@@ -33,6 +33,59 @@ def test_library_exports_every_declared_symbol():
     assert L.tpo_kernel_launches() >= 0
 
 
+def test_noalloc_argument_checks_need_no_gpu():
+    """The allocation-free sensitivity refuses a null buffer (TPO_E_ARG) and
+    a filter radius whose template exceeds its 128 taps (TPO_E_UNSUPPORTED)
+    before it touches the GPU, so both answers come back on a CPU host."""
+    import ctypes as C
+
+    from topopt3d_b200 import _lib
+    L = _lib.load()
+    nel = (C.c_int32 * 3)(8, 4, 4)
+    dx = (C.c_double * 3)(1.0, 1.0, 1.0)
+    msg = C.create_string_buffer(256)
+    dummy = C.c_void_p(16)          # never dereferenced: refused first
+    rc = L.tpo_sensitivity_noalloc(nel, dx, 1.0, 0.3, 1.5, None, dummy, dummy,
+                                   None, msg, 256)
+    assert rc == _lib.TPO_E_ARG and b"null buffer" in msg.value
+    rc = L.tpo_sensitivity_noalloc(nel, dx, 1.0, 0.3, 6.0, dummy, dummy, dummy,
+                                   None, msg, 256)
+    assert rc == _lib.TPO_E_UNSUPPORTED and b"128 taps" in msg.value
+    for bad in (float("inf"), float("nan"), -1.0):
+        rc = L.tpo_sensitivity_noalloc(nel, dx, 1.0, 0.3, bad, dummy, dummy, dummy,
+                                       None, msg, 256)
+        assert rc in (_lib.TPO_E_ARG, _lib.TPO_E_UNSUPPORTED), bad
+
+
+def test_k0_anisotropic_elements_decouple(oracle):
+    """K0 of box elements with unequal edges and other materials keeps the
+    properties the modal apply relies on: symmetric, 6 rigid-body modes,
+    the 45-entry Hadamard block pattern, and the patch test."""
+    xyz = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0],
+                    [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], float)
+    s = 2 * xyz - 1
+    H = np.array([[1, a[0], a[1], a[0] * a[1], a[2], a[0] * a[2], a[1] * a[2],
+                   a[0] * a[1] * a[2]] for a in s]).T
+    Tm = np.kron(H, np.eye(3))
+    for dx, E0, nu in (((1.0, 0.5, 2.0), 1.0, 0.3), ((2.0, 1.0, 1.0), 210.0, 0.25),
+                       ((1.0, 0.5, 0.75), 3.0, 0.3)):
+        K = oracle.element_stiffness(dx, E0, nu)
+        sc = np.abs(K).max()
+        assert np.abs(K - K.T).max() < 1e-14 * sc
+        w = np.linalg.eigvalsh(K)
+        assert np.sum(np.abs(w) < 1e-12 * sc) == 6 and w.min() > -1e-12 * sc
+        Kh = Tm @ K @ Tm.T / 64
+        assert np.sum(np.abs(Kh) > 1e-12 * sc) == 45
+        # uniform strain eps_xx = 1 on the physical element: the +x face
+        # carries sigma_xx = D[0,0] over its area dy*dz
+        D = np.zeros(36)
+        oracle.lib().tor_constitutive(E0, nu, D)
+        u = np.zeros((8, 3))
+        u[:, 0] = xyz[:, 0] * dx[0]
+        f = (K @ u.ravel()).reshape(8, 3)
+        assert abs(f[xyz[:, 0] == 1, 0].sum() - D[0] * dx[1] * dx[2]) < 1e-12 * sc
+
+
 # ----------------------------------------------------------------- oracle KATs
 
 def test_k0_known_answers(oracle):

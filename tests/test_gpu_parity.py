@@ -318,3 +318,56 @@ def test_full_size_properties(T):
     assert abs(u @ Kv - v @ Ku) < 1e-10 * abs(u @ Kv)
     r = t.F - t.apply(U64, np.zeros_like(U64))
     assert np.linalg.norm(r) <= 1.0001e-8 * np.linalg.norm(t.F)
+
+
+def test_grid_barrier_wait_runs_out_and_recovers(T, oracle):
+    """Failure detection of the persistent kernels without a GPU fault: in a
+    small cooperative grid one block never arrives at the barrier; the
+    others give up after 4,096 polls and return, the call reports
+    TPO_E_CUDA, the counter is reset, and the context keeps working (a
+    full barrier run and a solve that uses the persistent coarse cycle)."""
+    import ctypes as C
+    nel = (24, 12, 12)
+    t, ref = pair(T, oracle, nel, levels=3, seed=13)
+    lib = t._lib
+    done = C.c_int32(-1)
+    assert lib.tpo_barrier_selftest(t._h, 8, 4, -1, 1 << 22, C.byref(done)) == 0
+    assert done.value == 8
+    for skip in (3, 0):
+        rc = lib.tpo_barrier_selftest(t._h, 8, 4, skip, 4096, C.byref(done))
+        assert rc == T._lib.TPO_E_CUDA
+        assert b"grid-barrier wait ran out" in lib.tpo_last_error(t._h)
+        assert done.value == 0
+        assert lib.tpo_barrier_selftest(t._h, 8, 4, -1, 1 << 22, C.byref(done)) == 0
+        assert done.value == 8
+    Uo, st, _, _ = ref.solve()
+    info = t.FESolve()
+    assert st == 0 and info["status"] == 0
+    assert np.linalg.norm(t.U - Uo) / np.linalg.norm(Uo) < 1e-8
+
+
+def test_device_flag_refuses_host_pointers(T, oracle):
+    """A host buffer passed with TPO_MEM_DEVICE is refused (TPO_E_ARG)
+    before anything is launched, instead of reaching a kernel."""
+    import ctypes as C
+    nel = (8, 4, 4)
+    t, _ = pair(T, oracle, nel, levels=2, seed=14)
+    lib = t._lib
+    u = np.ones(3 * t.nNode)
+    y = np.full(3 * t.nNode, 5.0)
+    before = lib.tpo_kernel_launches()
+    ptr = lambda a: a.ctypes.data_as(C.c_void_p)
+    rc = lib.tpo_apply(t._h, ptr(u), ptr(y), 1, T.PREC_FP64, T._lib.MEM_DEVICE)
+    assert rc == T._lib.TPO_E_ARG
+    assert b"host memory" in lib.tpo_last_error(t._h)
+    dc = np.full(t.nElem, 5.0)
+    assert lib.tpo_filter(t._h, ptr(dc), ptr(dc), 1, T._lib.MEM_DEVICE) == T._lib.TPO_E_ARG
+    c = C.c_double()
+    assert lib.tpo_compliance(t._h, C.byref(c), ptr(dc), None,
+                              T._lib.MEM_DEVICE) == T._lib.TPO_E_ARG
+    x32 = np.ones(3 * t.nNode, np.float32)
+    assert lib.tpo_apply_f32(t._h, ptr(x32), ptr(x32[::-1].copy())) == T._lib.TPO_E_ARG
+    assert lib.tpo_kernel_launches() == before
+    assert np.all(y == 5.0) and np.all(dc == 5.0)
+    # the same buffers as host memory are fine
+    assert lib.tpo_apply(t._h, ptr(u), ptr(y), 1, T.PREC_FP64, T._lib.MEM_HOST) == 0

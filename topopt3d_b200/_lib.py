@@ -38,7 +38,7 @@ EXPORTS = (
     "tpo_default_mma_opts", "tpo_mma_update", "tpo_mma_last_info",
     "tpo_write_vec_bin", "tpo_read_vec_bin", "tpo_write_mat_bin", "tpo_read_mat_bin",
     "tpo_mesh_out", "tpo_print_vals", "tpo_load_mesh", "tpo_load_design",
-    "tpo_load_point_masses",
+    "tpo_load_point_masses", "tpo_barrier_selftest",
 )
 NOALLOC_MAX_ELEMS = 1 << 20
 
@@ -131,6 +131,7 @@ def load(path: str | None = None):
         "tpo_filter": (C.c_int, [vp, vp, vp, i32, C.c_int]),
         "tpo_oc_update": (C.c_int, [vp, vp, vp, vp, vp, d, vp, d, dp, C.c_int]),
         "tpo_sync": (C.c_int, [vp]),
+        "tpo_barrier_selftest": (C.c_int, [vp, i32, i32, i32, i32, C.POINTER(i32)]),
         "tpo_set_stream": (C.c_int, [vp, vp]),
         "tpo_kernel_launches": (C.c_int64, []),
         "tpo_sensitivity_noalloc": (C.c_int, [C.POINTER(i32), dp, d, d, d, vp, vp,

@@ -7,9 +7,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <initializer_list>
 #include <string>
 
 #include "coarse.h"
+#include "grid_barrier.cuh"
 #include "io.h"
 #include "solver.h"
 
@@ -131,8 +133,38 @@ void refresh_idm(Ctx &c) {
   if (c.have_material) tpo::launch_identity_mask(c, c.stream);
 }
 
-int check_mem(Ctx &c, int mem) {
+// a caller buffer flagged TPO_MEM_DEVICE must be device (or managed)
+// memory of the context's GPU: a host pointer handed to a kernel would be
+// an illegal-address fault, so it is refused before anything is issued
+int check_device_ptr(Ctx &c, const void *p) {
+  if (!p) return TPO_OK;
+  cudaPointerAttributes a{};
+  const cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();   // clear the sticky-free error of the query
+    c.err = std::string("TPO_MEM_DEVICE buffer is not device memory (") +
+            cudaGetErrorString(e) + ")";
+    return TPO_E_ARG;
+  }
+  if (a.type == cudaMemoryTypeManaged) return TPO_OK;
+  if (a.type != cudaMemoryTypeDevice) {
+    c.err = "TPO_MEM_DEVICE buffer is host memory";
+    return TPO_E_ARG;
+  }
+  if (a.device != c.device) {
+    c.err = "TPO_MEM_DEVICE buffer lives on another GPU than the context";
+    return TPO_E_ARG;
+  }
+  return TPO_OK;
+}
+
+// `mem` is one of the two flags, and with TPO_MEM_DEVICE every buffer the
+// call reads or writes in `mem` is device memory of the context's GPU
+int check_mem(Ctx &c, int mem, std::initializer_list<const void *> bufs = {}) {
   REQUIRE(mem == TPO_MEM_HOST || mem == TPO_MEM_DEVICE, "mem must be TPO_MEM_HOST or TPO_MEM_DEVICE");
+  if (mem == TPO_MEM_DEVICE)
+    for (const void *p : bufs)
+      if (int rc = check_device_ptr(c, p)) return rc;
   return TPO_OK;
 }
 
@@ -524,7 +556,7 @@ int tpo_add_bc(tpo_ctx *ctx, int32_t type, const double center[3],
 int tpo_set_bc(tpo_ctx *ctx, const uint8_t *fixmask, const double *F, int mem) {
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
-  if (int rc = check_mem(c, mem)) return rc;
+  if (int rc = check_mem(c, mem, {fixmask, F})) return rc;
   const cudaMemcpyKind k = mem == TPO_MEM_DEVICE ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost;
   if (fixmask) CK(cudaMemcpy(c.fix_h.data(), fixmask, c.nn, k));
   if (F) CK(cudaMemcpy(c.F_h.data(), F, sizeof(double) * 3 * c.nn, k));
@@ -562,7 +594,7 @@ int tpo_get_bc(const tpo_ctx *cctx, uint8_t *fixmask, double *F, int mem) {
   tpo_ctx *ctx = const_cast<tpo_ctx *>(cctx);
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
-  if (int rc = check_mem(c, mem)) return rc;
+  if (int rc = check_mem(c, mem, {fixmask, F})) return rc;
   const cudaMemcpyKind k = mem == TPO_MEM_DEVICE ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost;
   if (fixmask) CK(cudaMemcpy(fixmask, c.fix_h.data(), c.nn, k));
   if (F) CK(cudaMemcpy(F, c.F_h.data(), sizeof(double) * 3 * c.nn, k));
@@ -587,7 +619,7 @@ int tpo_mat_int_fnc(tpo_ctx *ctx, const double *x, double penal, double eps,
                     int mem) {
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
-  if (int rc = check_mem(c, mem)) return rc;
+  if (int rc = check_mem(c, mem, {x})) return rc;
   REQUIRE(x, "null design vector");
   REQUIRE(penal > 0 && eps >= 0 && eps < 1, "invalid penalty or eps");
   if (mem == TPO_MEM_DEVICE)
@@ -605,7 +637,7 @@ int tpo_mat_int_fnc(tpo_ctx *ctx, const double *x, double penal, double eps,
 int tpo_set_moduli(tpo_ctx *ctx, const double *E, const double *dEdz, int mem) {
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
-  if (int rc = check_mem(c, mem)) return rc;
+  if (int rc = check_mem(c, mem, {E, dEdz})) return rc;
   REQUIRE(E, "null E");
   const cudaMemcpyKind k = mem == TPO_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   CK(cudaMemcpyAsync(c.E64, E, sizeof(double) * c.ne, k, c.stream));
@@ -709,7 +741,7 @@ int tpo_solve(tpo_ctx *ctx, const double *b, double *U, int32_t nrhs, int mem,
               const tpo_solve_opts *opts, tpo_solve_info *info) {
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
-  if (int rc = check_mem(c, mem)) return rc;
+  if (int rc = check_mem(c, mem, {b, U})) return rc;
   REQUIRE(b && U && nrhs >= 1, "invalid solve arguments");
   tpo_solve_opts o;
   if (opts) o = *opts; else tpo_default_solve_opts(&o);
@@ -758,7 +790,7 @@ int tpo_apply(tpo_ctx *ctx, const double *u, double *y, int32_t nrhs,
               int32_t precision, int mem) {
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
-  if (int rc = check_mem(c, mem)) return rc;
+  if (int rc = check_mem(c, mem, {u, y})) return rc;
   REQUIRE(u && y && nrhs >= 1, "invalid apply arguments");
   REQUIRE(c.initialized && c.have_material, "mesh not initialised or no material");
   REQUIRE(precision == TPO_PREC_FP64 || precision == TPO_PREC_MIXED, "invalid precision");
@@ -812,7 +844,7 @@ int tpo_ks_assemble(tpo_ctx *ctx) {
 int tpo_ks_apply(tpo_ctx *ctx, const double *u, double *y, int32_t nrhs, int mem) {
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
-  if (int rc = check_mem(c, mem)) return rc;
+  if (int rc = check_mem(c, mem, {u, y})) return rc;
   REQUIRE(u && y && nrhs >= 1, "invalid apply arguments");
   REQUIRE(c.ks_ready, "tpo_ks_assemble must be called first");
   const size_t n = 3 * c.nn;
@@ -838,7 +870,7 @@ int tpo_buckling(tpo_ctx *ctx, const tpo_eig_opts *opts, double *lambda,
                  double *phi, int mem, tpo_eig_info *info) {
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
-  if (int rc = check_mem(c, mem)) return rc;
+  if (int rc = check_mem(c, mem, {phi})) return rc;
   tpo_eig_opts o;
   if (opts) o = *opts; else tpo_default_eig_opts(&o);
   REQUIRE(lambda, "null lambda");
@@ -861,7 +893,7 @@ int tpo_buckling_sensitivity(tpo_ctx *ctx, int32_t nev, const double *lambda,
                              tpo_solve_info *info) {
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
-  if (int rc = check_mem(c, mem)) return rc;
+  if (int rc = check_mem(c, mem, {phi, dvdx, dvdrho})) return rc;
   REQUIRE(lambda && phi && value && dvdx, "null lambda, phi, value or dvdx");
   REQUIRE(nev >= 1 && nev <= tpo::kMaxEigPairs, "need 1 <= nev <= 32");
   REQUIRE(std::isfinite(p) && p >= 1.0, "the aggregation power p must be >= 1");
@@ -903,7 +935,7 @@ int tpo_frequency(tpo_ctx *ctx, int32_t nvals, double density, const double *mlu
                   double *value, double *dvdx, int mem, tpo_eig_info *info) {
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
-  if (int rc = check_mem(c, mem)) return rc;
+  if (int rc = check_mem(c, mem, {mlump, dvdx})) return rc;
   tpo_eig_opts o;
   if (opts) o = *opts; else tpo_default_eig_opts(&o);
   REQUIRE(lambda && nconv && value, "null lambda, nconv or value");
@@ -963,7 +995,7 @@ int tpo_mma_update(tpo_ctx *ctx, const tpo_mma_opts *opts, int32_t iter,
                    const double *dgdx, double *change, int mem) {
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
-  if (int rc = check_mem(c, mem)) return rc;
+  if (int rc = check_mem(c, mem, {x, xold1, xold2, low, upp, xmin, xmax, dfdx, dgdx})) return rc;
   tpo_mma_opts o;
   if (opts) o = *opts; else tpo_default_mma_opts(&o);
   REQUIRE(fresh_start && x && xold1 && xold2 && low && upp && xmin && xmax && dfdx && g &&
@@ -1057,6 +1089,7 @@ int tpo_apply_f32(tpo_ctx *ctx, const float *u, float *y) {
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
   REQUIRE(u && y && u != y, "invalid apply arguments");
+  if (int rc = check_mem(c, TPO_MEM_DEVICE, {u, y})) return rc;
   REQUIRE(c.initialized && c.have_material, "mesh not initialised or no material");
   tpo::launch_apply_fine<float>(c, c.E32, u, nullptr, y, c.stream);
   return finish(c, TPO_OK);
@@ -1066,7 +1099,7 @@ int tpo_apply_level(tpo_ctx *ctx, int32_t level, const double *u, double *y,
                     int mem) {
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
-  if (int rc = check_mem(c, mem)) return rc;
+  if (int rc = check_mem(c, mem, {u, y})) return rc;
   REQUIRE(c.assembled, "tpo_fe_assemble must be called first");
   REQUIRE(level >= 0 && level < c.L && u && y, "invalid level or buffer");
   const size_t n = 3 * c.lev[level].nn;
@@ -1084,7 +1117,7 @@ int tpo_apply_level(tpo_ctx *ctx, int32_t level, const double *u, double *y,
 int tpo_vcycle(tpo_ctx *ctx, const double *r, double *z, int32_t precision, int mem) {
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
-  if (int rc = check_mem(c, mem)) return rc;
+  if (int rc = check_mem(c, mem, {r, z})) return rc;
   REQUIRE(c.assembled, "tpo_fe_assemble must be called first");
   REQUIRE(r && z, "null buffer");
   const size_t n = 3 * c.nn;
@@ -1106,7 +1139,7 @@ int tpo_get_vector(const tpo_ctx *cctx, const char *which, double *out, int mem)
   tpo_ctx *ctx = const_cast<tpo_ctx *>(cctx);
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
-  if (int rc = check_mem(c, mem)) return rc;
+  if (int rc = check_mem(c, mem, {out})) return rc;
   size_t n = 0;
   double *p = vec_ptr(c, which, &n);
   REQUIRE(p && out, "unknown vector name or null buffer");
@@ -1120,7 +1153,7 @@ int tpo_get_vector(const tpo_ctx *cctx, const char *which, double *out, int mem)
 int tpo_set_vector(tpo_ctx *ctx, const char *which, const double *in, int mem) {
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
-  if (int rc = check_mem(c, mem)) return rc;
+  if (int rc = check_mem(c, mem, {in})) return rc;
   size_t n = 0;
   double *p = vec_ptr(c, which, &n);
   REQUIRE(p && in, "unknown vector name or null buffer");
@@ -1141,7 +1174,7 @@ int tpo_set_vector(tpo_ctx *ctx, const char *which, const double *in, int mem) {
 int tpo_compliance(tpo_ctx *ctx, double *C, double *dCdx, double *dCdrho, int mem) {
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
-  if (int rc = check_mem(c, mem)) return rc;
+  if (int rc = check_mem(c, mem, {dCdx, dCdrho})) return rc;
   REQUIRE(c.initialized && c.have_material, "mesh not initialised or no material");
   const int64_t n = 3 * c.nn;
   if (C) {
@@ -1165,7 +1198,7 @@ int tpo_compliance(tpo_ctx *ctx, double *C, double *dCdx, double *dCdrho, int me
 int tpo_volume(tpo_ctx *ctx, double *V, double *dVdx, int mem) {
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
-  if (int rc = check_mem(c, mem)) return rc;
+  if (int rc = check_mem(c, mem, {dVdx})) return rc;
   REQUIRE(c.have_material, "no material");
   if (V) {
     tpo::launch_fill(c.ne, c.tmpe2, 1.0, c.stream);
@@ -1184,7 +1217,7 @@ int tpo_volume(tpo_ctx *ctx, double *V, double *dVdx, int mem) {
 int tpo_filter(tpo_ctx *ctx, const double *in, double *out, int32_t transpose, int mem) {
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
-  if (int rc = check_mem(c, mem)) return rc;
+  if (int rc = check_mem(c, mem, {in, out})) return rc;
   REQUIRE(in && out, "null buffer");
   const double *din = nullptr;
   if (int rc = stage_in(c, in, c.ne, mem, c.io_a, &din)) return rc;
@@ -1200,7 +1233,7 @@ int tpo_oc_update(tpo_ctx *ctx, double *x, const double *xmin, const double *xma
                   double *change, int mem) {
   if (int rc = begin(ctx)) return rc;
   Ctx &c = ctx->c;
-  if (int rc = check_mem(c, mem)) return rc;
+  if (int rc = check_mem(c, mem, {x, xmin, xmax, dfdx, dgdx})) return rc;
   REQUIRE(x && xmin && xmax && dfdx && dgdx, "null OC argument");
   const int64_t n = c.ne;
   if (!c.oc_ws) CK(cudaMalloc(&c.oc_ws, sizeof(double) * 6 * n));
@@ -1246,6 +1279,34 @@ int tpo_oc_update(tpo_ctx *ctx, double *x, const double *xmin, const double *xma
     return TPO_E_CUDA;
   }
   if (change) *change = c.scal_h[tpo::SC_OC_CHANGE];
+  return finish(c, TPO_OK);
+}
+
+int tpo_barrier_selftest(tpo_ctx *ctx, int32_t blocks, int32_t phases,
+                         int32_t skip_block, int32_t max_polls, int32_t *completed) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  REQUIRE(blocks >= 1 && blocks <= 64, "need 1 <= blocks <= 64");
+  REQUIRE(phases >= 1 && phases <= 1024, "need 1 <= phases <= 1024");
+  REQUIRE(max_polls >= 1 && max_polls <= tpo::kBarrierPolls, "need 1 <= max_polls <= 2^22");
+  if (completed) *completed = 0;
+  CK(tpo::launch_barrier_selftest(c, blocks, phases, skip_block, max_polls, c.stream));
+  CK(cudaMemcpyAsync(c.scal_h + tpo::SC_SELFTEST, c.scal + tpo::SC_SELFTEST, sizeof(double),
+                     cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaMemcpyAsync(c.scal_h + tpo::kSlotFault, c.scal + tpo::kSlotFault, sizeof(double),
+                     cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  if (completed) *completed = (int32_t)c.scal_h[tpo::SC_SELFTEST];
+  if (c.scal_h[tpo::kSlotFault] != 0.0) {
+    // the same recovery as the persistent kernels' read-backs: the blocks
+    // returned, the counter may be mid-barrier, so clear it and the flag
+    c.scal_h[tpo::kSlotFault] = 0.0;
+    CK(cudaMemsetAsync(c.gbar, 0, sizeof(unsigned int), c.stream));
+    CK(cudaMemsetAsync(c.scal + tpo::kSlotFault, 0, sizeof(double), c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    c.err = "barrier self-test: a grid-barrier wait ran out";
+    return TPO_E_CUDA;
+  }
   return finish(c, TPO_OK);
 }
 

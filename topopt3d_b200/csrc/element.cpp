@@ -227,8 +227,14 @@ bool build_filter_taps(const int nel[3], const double dx[3], double R,
   // RecFilter (Filter.cpp:28-52): N = floor(R/dx) neighbours per side,
   // weight 1 - d/R for d < R (strict), template in (k, j, i) order which is
   // increasing column order of the assembled filter matrix.
-  short N[3];
-  for (int d = 0; d < 3; ++d) N[d] = static_cast<short>(R / dx[d]);
+  // offsets are stored as int8: refuse radii that do not fit (and
+  // non-finite or non-positive input) before the conversion
+  if (!std::isfinite(R) || !(R > 0)) return false;
+  int N[3];
+  for (int d = 0; d < 3; ++d) {
+    if (!std::isfinite(dx[d]) || !(dx[d] > 0) || !(R / dx[d] <= 127.0)) return false;
+    N[d] = static_cast<int>(R / dx[d]);
+  }
   taps.n = 0;
   for (int k = -N[2]; k <= N[2]; ++k)
     for (int j = -N[1]; j <= N[1]; ++j)
@@ -245,7 +251,7 @@ bool build_filter_taps(const int nel[3], const double dx[3], double R,
         ++taps.n;
       }
   (void)nel;
-  return true;
+  return taps.n > 0;
 }
 
 }  // namespace tpo

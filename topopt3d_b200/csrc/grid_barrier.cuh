@@ -19,9 +19,11 @@ constexpr int kBarrierPolls = 1 << 22;
 // acquire on to the other threads.  (A barrier on a counter of our own is
 // used rather than the cooperative-groups grid sync: with the latter the
 // phase after each sync ran about twice as long on B200.)  A wait that runs
-// out of polls sets *fault (a device scalar the host reads back) and
-// returns false; the caller then returns from the kernel.
-__device__ __forceinline__ bool grid_barrier(unsigned int *bar, double *fault) {
+// out of polls (max_polls; the persistent kernels use kBarrierPolls, the
+// self-test a few thousand) sets *fault (a device scalar the host reads
+// back) and returns false; the caller then returns from the kernel.
+__device__ __forceinline__ bool grid_barrier(unsigned int *bar, double *fault,
+                                             int max_polls = kBarrierPolls) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -33,7 +35,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned int *bar, double *fault) {
     ok = 1;
     do {
       asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(cur) : "l"(bar) : "memory");
-      if (++polls > kBarrierPolls) {
+      if (++polls > max_polls) {
         ok = 0;
         *(volatile double *)fault = 1.0;
         break;

@@ -92,6 +92,19 @@ __global__ void k_na_adjoint(int nx, int ny, int nz, const NaTaps T,
 
 std::mutex g_na_mutex;
 double *g_na_ptr[64] = {nullptr};   // device address of the array, per device
+int g_na_sms[64] = {0};             // multiprocessor count, per device
+
+// a caller buffer must be device (or managed) memory of the current GPU;
+// a host pointer would reach the kernels as an illegal address
+bool na_device_buffer(const void *p, int dev) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (a.type == cudaMemoryTypeManaged) return true;
+  return a.type == cudaMemoryTypeDevice && a.device == dev;
+}
 
 void na_message(char *msg, int32_t len, const char *text) {
   if (!msg || len <= 0) return;
@@ -144,7 +157,7 @@ extern "C" int tpo_sensitivity_noalloc(const int32_t nel[3], const double dx[3],
   }
   const int nel3[3] = {nel[0], nel[1], nel[2]};
   if (!build_filter_taps(nel3, dx, rmin, host.taps) || host.taps.n > kNaMaxTaps) {
-    na_message(msg, msg_len, "filter radius too large for this entry point (> 128 taps)");
+    na_message(msg, msg_len, "filter radius invalid or too large for this entry point (> 128 taps)");
     return TPO_E_UNSUPPORTED;
   }
   NaTaps taps{};
@@ -153,17 +166,32 @@ extern "C" int tpo_sensitivity_noalloc(const int32_t nel[3], const double dx[3],
     for (int d = 0; d < 3; ++d) taps.off[t][d] = host.taps.off[t][d];
     taps.w[t] = host.taps.w[t];
   }
-  // the array's device address, looked up once per device with that device
-  // current (the host-side symbol is not a device address)
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
     na_message(msg, msg_len, "no CUDA device");
     return TPO_E_CUDA;
   }
+  if (!na_device_buffer(U, dev) || !na_device_buffer(dEdz, dev) ||
+      !na_device_buffer(dCdx, dev)) {
+    na_message(msg, msg_len, "U, dEdz and dCdx must be device memory of the current GPU");
+    return TPO_E_ARG;
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+    cudaGetLastError();
+    na_message(msg, msg_len, "invalid stream");
+    return TPO_E_ARG;
+  }
+  // the array's device address, looked up with the device current (the
+  // host-side symbol is not a device address): at the first call on each
+  // device, and again on every call made outside a stream capture, so that
+  // a context re-created after cudaDeviceReset gets its own address
   double *scratch = nullptr;
+  int sms = 0;
   {
     std::lock_guard<std::mutex> lock(g_na_mutex);
-    if (!g_na_ptr[dev]) {
+    if (!g_na_ptr[dev] || cap == cudaStreamCaptureStatusNone) {
       void *p = nullptr;
       const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
       if (e != cudaSuccess || !p) {
@@ -171,12 +199,17 @@ extern "C" int tpo_sensitivity_noalloc(const int32_t nel[3], const double dx[3],
         return TPO_E_CUDA;
       }
       g_na_ptr[dev] = static_cast<double *>(p);
+      if (cudaDeviceGetAttribute(&g_na_sms[dev], cudaDevAttrMultiProcessorCount, dev) !=
+          cudaSuccess) {
+        cudaGetLastError();
+        g_na_sms[dev] = 1;
+      }
     }
     scratch = g_na_ptr[dev];
+    sms = g_na_sms[dev] > 0 ? g_na_sms[dev] : 1;
   }
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   int64_t blocks = (ne + 127) / 128;
-  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (blocks > (int64_t)sms * 32) blocks = (int64_t)sms * 32;
   k_na_energy<<<(int)blocks, 128, 0, s>>>(nel[0], nel[1], nel[2], U, dEdz,
                                           scratch, host.kh64);
   k_na_adjoint<<<(int)blocks, 128, 0, s>>>(nel[0], nel[1], nel[2], taps,

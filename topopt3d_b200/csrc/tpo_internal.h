@@ -253,7 +253,9 @@ constexpr int kColScal = 8;
 constexpr int kScalMisc = kMaxBatch * kColScal;   // 64
 enum { SC_COMPLIANCE = kScalMisc, SC_VOLUME, SC_OC_DG, SC_OC_CHANGE, SC_POWER };
 constexpr int SC_POWER_PREV = SC_POWER + kMaxLevels;
-constexpr int kScalCount = SC_POWER_PREV + kMaxLevels;
+// blocks that passed every barrier of tpo_barrier_selftest
+constexpr int SC_SELFTEST = SC_POWER_PREV + kMaxLevels;
+constexpr int kScalCount = SC_SELFTEST + 1;
 constexpr int kSlotFault = 7;
 
 // fixed reduction grid (blocks per column) for a block of nb columns
@@ -456,6 +458,12 @@ bool launch_oc_bisect(const Ctx &c, int64_t n, double *x, const double *xold,
 void launch_oc_finish(const Ctx &c, int64_t n, double *x, const double *xold,
                       const double *xmin, const double *xmax, double *out,
                       cudaStream_t s);
+// the grid-barrier self-test (selftest.cu): `blocks` co-resident CTAs cross
+// `phases` barriers on c.gbar, block `skip` (if in range) leaves before its
+// first arrival, waits give up after max_polls polls; the count of blocks
+// that passed every barrier goes to c.scal[SC_SELFTEST]
+cudaError_t launch_barrier_selftest(const Ctx &c, int blocks, int phases, int skip,
+                                    int max_polls, cudaStream_t s);
 
 // host-side element constants (element.cpp)
 int build_element_constants(Ctx &c);

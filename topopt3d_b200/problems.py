@@ -16,13 +16,13 @@ TINY = 1e-10
 OPEN = (-1e30, 1e30, -1e30, 1e30, -1e30, 1e30)
 
 
-def cantilever_bcs(nel):
+def cantilever_bcs(nel, dx=(1.0, 1.0, 1.0)):
     """x = 0 face clamped; total load -1 in z split evenly over the nodes of
-    the (x = max, z = 0) edge."""
+    the (x = max, z = 0) edge.  Coordinates are physical: element edges dx."""
     nx, ny, nz = nel
     return [
         ("support", (0.0, 0.0, 0.0), (TINY, BIG, BIG), OPEN, (1.0, 1.0, 1.0)),
-        ("load", (float(nx), 0.0, 0.0), (TINY, BIG, TINY), OPEN,
+        ("load", (float(nx) * dx[0], 0.0, 0.0), (TINY, BIG, TINY), OPEN,
          (0.0, 0.0, -1.0 / (ny + 1))),
     ]
 
