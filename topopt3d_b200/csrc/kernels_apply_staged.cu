@@ -19,20 +19,23 @@
 //   the two faces sharing the edge --x^T--> node contributions, summed over
 //   the two edges sharing the node.
 //
-// This needs ~165 FP operations per element instead of ~210 for a separate
-// butterfly per element (and 1152 for the dense 24x24 product).
+// About 150 FP operations per element (the dense 24x24 product is 1152):
+// x 6, y 12, z 21, Kh 45, and the z transpose with the modulus E_e and the
+// sum over the two elements of a face folded into 42 multiply-adds.
 //
 // Thread (tx, ty) of a 32 x TY CTA owns the grid column (gx, gy) = tile
 // origin + (tx, ty): its node, the x-edge to gx+1, the xy-face spanning
 // (gx..gx+1, gy..gy+1) and the element column above that face; the CTA
 // marches up z.  x-neighbours exchange values by warp shuffles (a warp is
 // one tile row), y-neighbours through shared memory with one barrier per
-// plane.  Lane 0 and row 0 are the halo: the CTA writes nodes tx >= 1,
-// ty >= 1.  Lane 31 and row TY-1 load one extra node (column/row) so every
-// face of the tile is complete.  Node values of the next plane are
-// prefetched into registers one plane ahead.  The pipeline: at step p the
-// plane p is loaded into edges and faces, element layer p-1 is applied, the
-// faces of plane p-1 are complete, and nodes of plane p-2 are written.
+// plane.  Lanes 0 and 31 and row 0 are the halo: the CTA writes the nodes of
+// lanes 1..30 and rows 1..TY-1, so every lane's work is the same (lane 31
+// only supplies its node to lane 30's edge); the last row (a warp-uniform
+// role) also loads the row above the tile so every face of the tile is
+// complete.  Node values of the next plane are prefetched into registers
+// one plane ahead.  The pipeline: at step p the plane p is loaded into
+// edges and faces, element layer p-1 is applied, the faces of plane p-1 are
+// complete, and nodes of plane p-2 are written.
 #include "modal.cuh"
 
 namespace tpo {
@@ -40,12 +43,7 @@ namespace tpo {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-
-template <typename T>
-struct NodeReg {
-  T v[3];
-  unsigned f;
-};
+constexpr int kLanesOut = 30;   // written nodes per tile row
 
 // the input vector of dof i: u_i (IN_U) or the Chebyshev start from a zero
 // guess, invtheta * dinv_i * b_i (IN_CHEB)
@@ -53,23 +51,6 @@ template <typename T, int IN>
 __device__ __forceinline__ T input_value(const ApplyArgs<T> &a, int64_t i) {
   if (IN == IN_CHEB) return a.invtheta * (__ldg(a.dinv + i) * __ldg(a.b + i));
   return __ldg(a.u + i);
-}
-
-template <typename T, int IN>
-__device__ __forceinline__ void fetch_node(const ApplyArgs<T> &a,
-                                           const uint8_t *__restrict__ fix,
-                                           int gx, int gy, int z, int Nx, int Ny,
-                                           int Nz, NodeReg<T> &r) {
-  if (gx >= 0 && gx < Nx && gy >= 0 && gy < Ny && z >= 0 && z < Nz) {
-    const int n = (z * Ny + gy) * Nx + gx;
-    r.f = __ldg(fix + n);
-    r.v[0] = input_value<T, IN>(a, 3 * n);
-    r.v[1] = input_value<T, IN>(a, 3 * n + 1);
-    r.v[2] = input_value<T, IN>(a, 3 * n + 2);
-  } else {
-    r.f = 7u;   // outside the mesh: contributes zero
-    r.v[0] = r.v[1] = r.v[2] = T(0);
-  }
 }
 
 // epilogue of dof i with Au_i = (M K M u + (1-M) u)_i and u_i the input:
@@ -102,22 +83,71 @@ __device__ __forceinline__ void finish_dof(const ApplyArgs<T> &a, int64_t i,
   }
 }
 
+// six values per thread in shared memory with 16-byte accesses: FP32 as one
+// float4 (v0, w0, v1, w1) and one float2 (v2, w2) per lane; FP64 as three
+// double2 (v_c, w_c)
 template <typename T>
-__device__ __forceinline__ T masked(const NodeReg<T> &r, int c) {
-  return ((r.f >> c) & 1u) ? T(0) : r.v[c];
-}
+struct Six;
+
+template <>
+struct Six<float> {
+  float4 *a;   // [row][32]
+  float2 *b;
+  __device__ __forceinline__ void put(int row, int lane, const float (&v)[3],
+                                      const float (&w)[3]) const {
+    a[row * 32 + lane] = make_float4(v[0], w[0], v[1], w[1]);
+    b[row * 32 + lane] = make_float2(v[2], w[2]);
+  }
+  __device__ __forceinline__ void get(int row, int lane, float (&v)[3],
+                                      float (&w)[3]) const {
+    const float4 p = a[row * 32 + lane];
+    const float2 q = b[row * 32 + lane];
+    v[0] = p.x; w[0] = p.y; v[1] = p.z; w[1] = p.w; v[2] = q.x; w[2] = q.y;
+  }
+  static constexpr size_t bytes_per_row() { return 32 * (16 + 8); }
+  __device__ __forceinline__ void bind(unsigned char *base, int rows) {
+    a = reinterpret_cast<float4 *>(base);
+    b = reinterpret_cast<float2 *>(base + (size_t)rows * 32 * 16);
+  }
+};
+
+template <>
+struct Six<double> {
+  double2 *a;   // [c][row][32]
+  int stride;
+  __device__ __forceinline__ void put(int row, int lane, const double (&v)[3],
+                                      const double (&w)[3]) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) a[c * stride + row * 32 + lane] = make_double2(v[c], w[c]);
+  }
+  __device__ __forceinline__ void get(int row, int lane, double (&v)[3],
+                                      double (&w)[3]) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double2 p = a[c * stride + row * 32 + lane];
+      v[c] = p.x;
+      w[c] = p.y;
+    }
+  }
+  static constexpr size_t bytes_per_row() { return 32 * 3 * 16; }
+  __device__ __forceinline__ void bind(unsigned char *base, int rows) {
+    a = reinterpret_cast<double2 *>(base);
+    stride = rows * 32;
+  }
+};
 
 // COLS: a block of columns, blockIdx.z = column * nchunk + z chunk, the
 // column selecting u, b, y, y2 (stride ld).  The single-column
 // instantiation reads the parameters in place.
 template <typename T, int TY, int IN, int OUT, bool COLS>
-__global__ void __launch_bounds__(32 * TY)
+__global__ void __launch_bounds__(32 * TY, sizeof(T) == 4 ? 2 : 1)
     k_apply_staged(int nelx, int nely, int nelz, int zchunk,
                    const T *__restrict__ E, const uint8_t *__restrict__ fix,
                    const ApplyArgs<T> args_in, const Kh<T> kh) {
+  constexpr bool kNeedU = OUT == OUT_CHEB2 || OUT == OUT_POST0 || OUT == OUT_POST1;
   const int Nx = nelx + 1, Ny = nely + 1, Nz = nelz + 1;
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int gx = (int)blockIdx.x * 31 - 1 + tx;
+  const int gx = (int)blockIdx.x * kLanesOut - 1 + tx;
   const int gy = (int)blockIdx.y * (TY - 1) - 1 + ty;
   int zs;
   ApplyArgs<T> args_col;
@@ -135,167 +165,199 @@ __global__ void __launch_bounds__(32 * TY)
   }
   const ApplyArgs<T> &args = COLS ? args_col : args_in;
   const int ze = min(zs + zchunk, Nz);
-  const bool lane31 = (tx == 31);
-  const bool lastrow = (ty == TY - 1);
+  const bool lastrow = (ty == TY - 1);   // warp-uniform
+
+  // plane-invariant per-thread offsets and predicates
+  const bool xin = gx >= 0 && gx < Nx;
+  const bool nin = xin && gy >= 0 && gy < Ny;
+  const bool nin2 = lastrow && xin && gy + 1 < Ny;
   const bool exy = gx >= 0 && gx < nelx && gy >= 0 && gy < nely;
+  const bool own = tx >= 1 && tx <= kLanesOut && ty >= 1 && nin;
+  const int NP = Nx * Ny, EP = nelx * nely;
+  const int nofs = nin ? gy * Nx + gx : 0;
+  const int nofs2 = nin2 ? (gy + 1) * Nx + gx : 0;
+  const int eofs = exy ? gy * nelx + gx : 0;
 
-  // dynamic shared memory (the FP64 tiles exceed the 48 KB static limit):
-  // se = x-edge (s, d) per row plus the extra row, sc = upper-edge
-  // contributions, both double-buffered by plane parity
+  // dynamic shared memory: se = x-edge (s, d) per row plus the row above
+  // the tile, sc = edge contributions of the upper row of a face (row index
+  // ty + 1 written by row ty), both double-buffered by plane parity
+  // (rows buf * kRows + r of one array per buffer pair)
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T(*se)[6][TY + 1][32] = reinterpret_cast<T(*)[6][TY + 1][32]>(smem_raw);
-  T(*sc)[6][TY][32] = reinterpret_cast<T(*)[6][TY][32]>(
-      smem_raw + sizeof(T) * 2 * 6 * (TY + 1) * 32);
+  constexpr int kRows = TY + 1;
+  Six<T> se, sc;
+  se.bind(smem_raw, 2 * kRows);
+  sc.bind(smem_raw + 2 * kRows * Six<T>::bytes_per_row(), 2 * kRows);
 
-  NodeReg<T> n0, n1, n2, n3;   // next plane: own, +x, +y, +x+y
-  n1.f = n2.f = n3.f = 7u;
+  // prefetched next plane: own node, the row-above node (last row), the
+  // fixed-component bits and the modulus of the element layer below it
+  T pu[3] = {T(0), T(0), T(0)}, pq[3] = {T(0), T(0), T(0)};
+  unsigned pf = 0u, pf2 = 0u;
+  T pE = T(0);
+  auto fetch = [&](int z) {   // z is uniform over the CTA
+    // fresh zeros every plane let the loads target renamed registers
+    pf = pf2 = 0u;
 #pragma unroll
-  for (int c = 0; c < 3; ++c) n1.v[c] = n2.v[c] = n3.v[c] = T(0);
-  T nE = T(0);
-  auto fetch = [&](int z) {
-    fetch_node<T, IN>(args, fix, gx, gy, z, Nx, Ny, Nz, n0);
-    if (lane31) fetch_node<T, IN>(args, fix, gx + 1, gy, z, Nx, Ny, Nz, n1);
-    if (lastrow) {
-      fetch_node<T, IN>(args, fix, gx, gy + 1, z, Nx, Ny, Nz, n2);
-      if (lane31) fetch_node<T, IN>(args, fix, gx + 1, gy + 1, z, Nx, Ny, Nz, n3);
+    for (int c = 0; c < 3; ++c) pu[c] = pq[c] = T(0);
+    pE = T(0);
+    if (z >= 0 && z < Nz) {
+      const int n = nofs + z * NP;
+      if (nin) {
+        pf = __ldg(fix + n);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) pu[c] = input_value<T, IN>(args, 3 * (int64_t)n + c);
+      }
+      if (nin2) {
+        const int n2 = nofs2 + z * NP;
+        pf2 = __ldg(fix + n2);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) pq[c] = input_value<T, IN>(args, 3 * (int64_t)n2 + c);
+      }
     }
-    // element layer z-1 is applied when plane z is the top plane
     const int ez = z - 1;
-    nE = (exy && ez >= 0 && ez < nelz)
-             ? __ldg(E + (ez * nely + gy) * nelx + gx)
-             : T(0);
+    if (exy && ez >= 0 && ez < nelz) pE = __ldg(E + eofs + ez * EP);
   };
 
-  T Fprev[4][3], ctop[4][3], les[3], led[3];
+  T FA[4][3], FB[4][3], CA[4][3], CB[4][3], les[3], led[3];
 #pragma unroll
   for (int m = 0; m < 4; ++m)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) Fprev[m][c] = ctop[m][c] = T(0);
+    for (int c = 0; c < 3; ++c) FA[m][c] = FB[m][c] = CA[m][c] = CB[m][c] = T(0);
 #pragma unroll
   for (int c = 0; c < 3; ++c) les[c] = led[c] = T(0);
+  unsigned fpipe = 0u;   // fixed bits of the last three planes, 8 bits each
 
-  fetch(zs - 1);
-#pragma unroll 2
-  for (int p = zs - 1; p <= ze + 1; ++p) {
-    // ---- plane p: take the prefetched values, prefetch plane p + 1
-    T cu[3], cr[3], cq[3], crq[3];
+  // one step of the z-march at plane p: Fprev = faces of plane p-1 (in),
+  // Fp = faces of plane p (out), ctop = contributions of element layer p-2
+  // to face p-1 (in), top = those of layer p-1 to face p (out)
+  auto step = [&](int p, const T(&Fprev)[4][3], T(&Fp)[4][3], const T(&ctop)[4][3],
+                  T(&top)[4][3]) {
+    T cu[3], cq[3];
+    const unsigned f = pf;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      cu[c] = masked(n0, c);
-      cr[c] = masked(n1, c);
-      cq[c] = masked(n2, c);
-      crq[c] = masked(n3, c);
+      cu[c] = ((f >> c) & 1u) ? T(0) : pu[c];
+      cq[c] = ((pf2 >> c) & 1u) ? T(0) : pq[c];
     }
-    const T Ee = nE;
-    if (p + 1 <= ze + 1) fetch(p + 1);
-    const int buf = p & 1;
+    const T Ee = pE;
+    fpipe = (fpipe << 8) | f;
+    if (p + 1 <= ze) fetch(p + 1);
+    const int rb = (p & 1) * kRows, rb1 = kRows - rb;   // this / the other buffer
 
-    // ---- x-edges of plane p: s = u(x+1) + u(x), d = u(x+1) - u(x)
-    T s0[3], d0[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      T r = __shfl_down_sync(kFull, cu[c], 1);
-      if (lane31) r = cr[c];
-      s0[c] = r + cu[c];
-      d0[c] = r - cu[c];
-      se[buf][c][ty][tx] = s0[c];
-      se[buf][3 + c][ty][tx] = d0[c];
-    }
-    if (lastrow) {
+    // ---- x-edges of plane p (s = u(x+1) + u(x), d = u(x+1) - u(x)) and
+    // the xy-faces: modes (1, x, y, xy)
+    if (p <= ze) {
+      T s0[3], d0[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        T r = __shfl_down_sync(kFull, cq[c], 1);
-        if (lane31) r = crq[c];
-        se[buf][c][TY][tx] = r + cq[c];
-        se[buf][3 + c][TY][tx] = r - cq[c];
+        const T r = __shfl_down_sync(kFull, cu[c], 1);
+        s0[c] = r + cu[c];
+        d0[c] = r - cu[c];
       }
-    }
-    __syncthreads();
-
-    // ---- xy-face of plane p: modes (1, x, y, xy)
-    T Fp[4][3];
+      se.put(rb + ty, tx, s0, d0);
+      if (lastrow) {
+        T s2[3], d2[3];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const T s1 = se[buf][c][ty + 1][tx], d1 = se[buf][3 + c][ty + 1][tx];
-      Fp[0][c] = s0[c] + s1;
-      Fp[1][c] = d0[c] + d1;
-      Fp[2][c] = s1 - s0[c];
-      Fp[3][c] = d1 - d0[c];
-    }
-
-    // ---- nodes of plane p-2: complete the edge, transpose the x stage
-    if (p - 2 >= zs && p - 2 < ze) {
-      T val[3];
+        for (int c = 0; c < 3; ++c) {
+          const T r = __shfl_down_sync(kFull, cq[c], 1);
+          s2[c] = r + cq[c];
+          d2[c] = r - cq[c];
+        }
+        se.put(rb + TY, tx, s2, d2);
+      }
+      __syncthreads();
+      T s1[3], d1[3];
+      se.get(rb + ty + 1, tx, s1, d1);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        T es = les[c], ed = led[c];
-        if (ty > 0) {
-          es += sc[buf ^ 1][c][ty - 1][tx];
-          ed += sc[buf ^ 1][3 + c][ty - 1][tx];
-        }
+        Fp[0][c] = s0[c] + s1[c];
+        Fp[1][c] = d0[c] + d1[c];
+        Fp[2][c] = s1[c] - s0[c];
+        Fp[3][c] = d1[c] - d0[c];
+      }
+    } else {
+      __syncthreads();
+    }
+
+    // ---- nodes of plane p-2: complete the edge (the face of row ty-1
+    // left its part in sc row ty), transpose the x stage
+    if (p - 2 >= zs && p - 2 < ze) {
+      T gs[3], gd[3], val[3];
+      sc.get(rb1 + ty, tx, gs, gd);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const T es = les[c] + gs[c], ed = led[c] + gd[c];
         const T right = es + ed;
         const T left = __shfl_up_sync(kFull, right, 1);
         val[c] = (es - ed) + left;
       }
-      if (tx >= 1 && ty >= 1 && gx < Nx && gy < Ny) {
-        const int n = ((p - 2) * Ny + gy) * Nx + gx;
-        const unsigned f = __ldg(fix + n);
+      if (own) {
+        const int64_t n = nofs + (int64_t)(p - 2) * NP;
+        const unsigned fo = (fpipe >> 16) & 0xffu;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          // the input is needed for fixed dofs (identity rows) and by the
+          const bool fixed = (fo >> c) & 1u;
+          // the input is needed on fixed dofs (identity rows) and by the
           // Chebyshev epilogues
-          const bool need_u = ((f >> c) & 1u) || OUT == OUT_CHEB2 ||
-                              OUT == OUT_POST0 || OUT == OUT_POST1;
-          const T uv = need_u ? input_value<T, IN>(args, 3 * n + c) : T(0);
-          const T Au = ((f >> c) & 1u) ? uv : val[c];
-          finish_dof<T, OUT>(args, 3 * n + c, Au, uv);
+          const T uv = (kNeedU || fixed) ? input_value<T, IN>(args, 3 * n + c) : T(0);
+          finish_dof<T, OUT>(args, 3 * n + c, fixed ? uv : val[c], uv);
         }
       }
     }
 
-    // ---- element layer p-1 between faces p-1 (Fprev) and p (Fp)
-    T top[4][3], bot[4][3];
+    // ---- element layer p-1 between faces p-1 (Fprev) and p (Fp); the face
+    // of plane p-1 is then complete: G = ctop + bottom contributions
+    T G[4][3];
     if (p - 1 >= zs - 1 && p - 1 < ze) {
       T v[8][3], o[8][3];
 #pragma unroll
-      for (int m = 0; m < 4; ++m)
+      for (int c = 0; c < 3; ++c) {
+        v[0][c] = T(0);   // rigid translation: not coupled
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          v[m][c] = (Fp[m][c] + Fprev[m][c]) * Ee;
-          v[m + 4][c] = (Fp[m][c] - Fprev[m][c]) * Ee;
-        }
+        for (int m = 1; m < 4; ++m) v[m][c] = Fp[m][c] + Fprev[m][c];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) v[m + 4][c] = Fp[m][c] - Fprev[m][c];
+      }
       modal_couple(v, o, kh);
 #pragma unroll
-      for (int m = 0; m < 4; ++m)
+      for (int c = 0; c < 3; ++c) {
+        top[0][c] = Ee * o[4][c];
+        G[0][c] = fma(-Ee, o[4][c], ctop[0][c]);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          top[m][c] = o[m][c] + o[m + 4][c];
-          bot[m][c] = o[m][c] - o[m + 4][c];
+        for (int m = 1; m < 4; ++m) {
+          const T a = Ee * o[m][c];
+          top[m][c] = fma(Ee, o[m + 4][c], a);
+          G[m][c] = fma(-Ee, o[m + 4][c], ctop[m][c] + a);
         }
+      }
     } else {
 #pragma unroll
       for (int m = 0; m < 4; ++m)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) top[m][c] = bot[m][c] = T(0);
+        for (int c = 0; c < 3; ++c) {
+          top[m][c] = T(0);
+          G[m][c] = ctop[m][c];
+        }
     }
 
-    // ---- face of plane p-1 is complete: transpose the y stage
+    // ---- transpose the y stage of face p-1: the lower edge (own row) keeps
+    // its part in registers, the upper edge's part goes to sc row ty + 1
+    T gs[3], gd[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const T G0 = ctop[0][c] + bot[0][c], G1 = ctop[1][c] + bot[1][c];
-      const T G2 = ctop[2][c] + bot[2][c], G3 = ctop[3][c] + bot[3][c];
-      les[c] = G0 - G2;
-      led[c] = G1 - G3;
-      sc[buf][c][ty][tx] = G0 + G2;
-      sc[buf][3 + c][ty][tx] = G1 + G3;
+      les[c] = G[0][c] - G[2][c];
+      led[c] = G[1][c] - G[3][c];
+      gs[c] = G[0][c] + G[2][c];
+      gd[c] = G[1][c] + G[3][c];
     }
-#pragma unroll
-    for (int m = 0; m < 4; ++m)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        ctop[m][c] = top[m][c];
-        Fprev[m][c] = Fp[m][c];
-      }
+    sc.put(rb + ty + 1, tx, gs, gd);
+  };
+
+  fetch(zs - 1);
+  // two steps per trip with the state arrays swapping roles, so nothing is
+  // copied between planes
+  for (int p = zs - 1; p <= ze + 1; p += 2) {
+    step(p, FA, FB, CA, CB);
+    if (p + 1 <= ze + 1) step(p + 1, FB, FA, CB, CA);
   }
 }
 
@@ -303,7 +365,7 @@ constexpr int kTY = 8;
 
 template <typename T>
 size_t staged_smem() {
-  return sizeof(T) * 2 * 6 * (2 * kTY + 1) * 32;
+  return 4 * Six<T>::bytes_per_row() * (kTY + 1);
 }
 
 template <typename T, int IN, int OUT>
@@ -316,13 +378,14 @@ void set_smem_attr() {
                        (int)staged_smem<T>());
 }
 
-// grid of the staged kernel: 31 x (kTY-1) owned node columns per CTA, and z
+// grid of the staged kernel: 30 x (kTY-1) owned node columns per CTA, and z
 // chunks that fill whole waves of co-resident CTAs (a partial last wave
-// idles SMs for the length of a chunk; each chunk costs 3 extra planes)
+// idles SMs for the length of a chunk; each chunk recomputes one element
+// layer and two face planes)
 template <typename T>
 void staged_grid(const Ctx &c, int nb, dim3 &grid, int &zchunk) {
   const int Nx = c.nel[0] + 1, Ny = c.nel[1] + 1, Nz = c.nel[2] + 1;
-  const int gx = (Nx + 30) / 31, gy = (Ny + kTY - 2) / (kTY - 1);
+  const int gx = (Nx + kLanesOut - 1) / kLanesOut, gy = (Ny + kTY - 2) / (kTY - 1);
   const int dev = c.device & 63;
   static unsigned long long attr_set = 0;   // bit per device
   static int slots_cache[64] = {0};
