@@ -2,7 +2,6 @@
 // conditions, the TopOpt call surface and data movement between caller
 // buffers and the context's HBM-resident state.
 #include <cublas_v2.h>
-#include <cusolverDn.h>
 
 #include <algorithm>
 #include <cmath>
@@ -234,7 +233,7 @@ int alloc_solver(Ctx &c) {
   }
   if (c.L > 2) A(c.gd_tmp, tpo::galerkin_dims_scratch(c.lev[1]));
   const int64_t nc = 3 * c.lev[c.L - 1].nn;
-  A(c.Adense, (size_t)(nc * nc));
+  A(c.Adense, tpo::coarse_inverse_work(nc));   // inversion workspace
   A(c.Ainv, (size_t)(nc * nc));
   A(c.w64, 3 * c.nn);
 #undef A
@@ -252,7 +251,7 @@ void free_all(Ctx &c) {
   dfree(c.E64); dfree(c.dEdz); dfree(c.E32); dfree(c.S0); dfree(c.K0lex);
   dfree(c.GMi); dfree(c.gk_slot); dfree(c.gk_elem); dfree(c.gk_count);
   dfree(c.gk_G); c.gk_cap = 0; dfree(c.gd_tmp);
-  dfree(c.Ainv); dfree(c.Adense); dfree(c.solver_work); dfree(c.dev_info);
+  dfree(c.Ainv); dfree(c.Adense); dfree(c.dev_info);
   dfree(c.finv); dfree(c.taps_d);
   dfree(c.w64);
   dfree(c.Es64); dfree(c.dEsdz64); dfree(c.bk_buf); c.bk_n = 0; dfree(c.fq_buf); c.fq_n = 0; dfree(c.mma_buf); c.mma_n = 0;
@@ -266,8 +265,6 @@ void free_all(Ctx &c) {
   dfree(c.oc_ws);
   if (c.scal_h) cudaFreeHost(c.scal_h);
   c.scal_h = nullptr;
-  if (c.cusolver) cusolverDnDestroy(static_cast<cusolverDnHandle_t>(c.cusolver));
-  c.cusolver = nullptr;
   for (cudaStream_t &q : c.aux_stream)
     if (q) cudaStreamSynchronize(q);
   for (cudaEvent_t &e : c.lev_ev) {

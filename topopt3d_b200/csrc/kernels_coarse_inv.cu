@@ -1,0 +1,289 @@
+// Dense inverse of the coarsest-level operator, in place, by blocked
+// symmetric sweeps (Gauss-Jordan elimination without pivoting).
+//
+// The coarsest operator is symmetric positive definite (the Galerkin
+// product of the clamped fine operator; the reference factorises it with a
+// direct solver, FEAnalysis.cpp:555-573), so every pivot block -- a Schur
+// complement -- is SPD and no pivoting is needed.  The V-cycle applies the
+// explicit inverse as one bandwidth-parallel matrix-vector product.
+//
+// The sweep of block K (P = A_KK^-1, F = the column block A_{.K}, G = F P):
+//   A_KK <- -P;  A_iK <- G_i;  A_Kj <- G_j^T;  A_ij <- A_ij - G_i F_j^T
+// keeps the matrix symmetric, so only the tiles on or below the diagonal
+// are updated (the row block K left of the diagonal holds G^T); after every
+// block has been swept the matrix is -A^-1, and a last pass negates it and
+// fills the upper triangle.  A sweep is two launches: F and G for every row
+// block (k_sw_fg), and the rank-64 update of the lower tiles on 64 x 64
+// FP64 tiles (k_sw_update), one CTA of which then inverts the next
+// diagonal block by scalar Gauss-Jordan with a 4 x 4 block of it in each
+// thread's registers (sweep_diag; k_sw_diag for the first block).
+#include "tpo_internal.h"
+
+namespace tpo {
+
+namespace {
+
+constexpr int kGB = 64;    // block size (rows / columns of a pivot block)
+constexpr int kGT = 256;   // threads per CTA: 16 x 16, 4 x 4 outputs each
+constexpr int kKC = 32;    // k-chunk staged in shared memory
+
+// the staging buffers of tile_gemm, declared once by each calling kernel
+struct GemmSmem {
+  double Xs[kKC][kGB];
+  double Ys[kKC][kGB + 2];
+};
+
+// C (M x N, column-major, ldc) = (ACC ? C : 0) + s X Y for M, N <= 64 and a
+// depth Kd <= kGB, with X[i][k] = X[k * ldx + i] and Y[k][j] = Y[k * ldy + j]
+// (YT) or Y[j * ldy + k].  Every read of X and Y happens before the first
+// write of C.  X and Y are plain (coherent) loads: the caller may have
+// written them earlier in the same kernel.
+template <bool ACC, bool YT>
+__device__ __forceinline__ void tile_gemm(GemmSmem &sm, int M, int N, int Kd,
+                                          const double *X, int ldx, const double *Y,
+                                          int ldy, double *C,
+                                          int ldc, double s) {
+  auto &Xs = sm.Xs;
+  auto &Ys = sm.Ys;
+  const int t = threadIdx.x;
+  const int tx = t % 16, ty = t / 16;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int kc = 0; kc < Kd; kc += kKC) {
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kKC * kGB / kGT; ++q) {
+      const int e = t + q * kGT;
+      const int i = e % kGB, k = e / kGB;   // rows contiguous
+      Xs[k][i] = (i < M && kc + k < Kd) ? X[(int64_t)(kc + k) * ldx + i] : 0.0;
+      if (YT) {
+        Ys[k][i] = (i < N && kc + k < Kd) ? Y[(int64_t)(kc + k) * ldy + i] : 0.0;
+      } else {
+        const int k2 = e % kKC, j = e / kKC;   // depth contiguous
+        Ys[k2][j] = (j < N && kc + k2 < Kd) ? Y[(int64_t)j * ldy + kc + k2] : 0.0;
+      }
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int k = 0; k < kKC; ++k) {
+      const double2 x01 = *reinterpret_cast<const double2 *>(&Xs[k][tx * 4]);
+      const double2 x23 = *reinterpret_cast<const double2 *>(&Xs[k][tx * 4 + 2]);
+      const double2 y01 = *reinterpret_cast<const double2 *>(&Ys[k][ty * 4]);
+      const double2 y23 = *reinterpret_cast<const double2 *>(&Ys[k][ty * 4 + 2]);
+      const double xv[4] = {x01.x, x01.y, x23.x, x23.y};
+      const double yv[4] = {y01.x, y01.y, y23.x, y23.y};
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(xv[a], yv[b], acc[a][b]);
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const int j = ty * 4 + b;
+    if (j >= N) continue;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int i = tx * 4 + a;
+      if (i >= M) continue;
+      double *c = C + (int64_t)j * ldc + i;
+      *c = ACC ? fma(s, acc[a][b], *c) : s * acc[a][b];
+    }
+  }
+}
+
+// P = A_KK^-1 of the bs x bs diagonal block at (K0, K0) by scalar
+// Gauss-Jordan; thread (tx, ty) keeps rows 4tx.. and columns 4ty.. in
+// registers, and each step broadcasts the pivot row and column through
+// shared memory (double-buffered, one barrier per step).  P goes to the
+// workspace (ld kGB) and -P to A.  A pivot that is not positive records
+// its global index + 1 in *info (the first one wins).
+__device__ __forceinline__ void sweep_diag(int n, double *A, int K0, int bs, double *P,
+                                           int *info) {
+  __shared__ double rowk[2][kGB], colk[2][kGB];
+  const int t = threadIdx.x, tx = t % 16, ty = t / 16;
+  const int r0 = tx * 4, c0 = ty * 4;
+  double m[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int r = r0 + a, cc = c0 + b;
+      // identity outside the block, so the padding never pivots on zero
+      m[a][b] = (r < bs && cc < bs) ? A[(int64_t)(K0 + cc) * n + K0 + r]
+                                    : (r == cc ? 1.0 : 0.0);
+    }
+#pragma unroll 4
+  for (int k = 0; k < kGB; ++k) {
+    const int buf = k & 1;
+    // publish the pivot row (owners: rows 4tx..4tx+3 hold k) and column
+    // (the row/column index is selected with unrolled compares so m stays
+    // in registers)
+    if ((k >> 2) == tx) {
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+        if (a == (k & 3)) {
+#pragma unroll
+          for (int b = 0; b < 4; ++b) rowk[buf][c0 + b] = m[a][b];
+        }
+    }
+    if ((k >> 2) == ty) {
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+        if (b == (k & 3)) {
+#pragma unroll
+          for (int a = 0; a < 4; ++a) colk[buf][r0 + a] = m[a][b];
+        }
+    }
+    __syncthreads();
+    const double p = rowk[buf][k];
+    const bool ok = p > 0.0 && p < INFINITY;
+    if (!ok && t == 0 && k < bs) atomicCAS(info, 0, K0 + k + 1);
+    const double ip = ok ? 1.0 / p : 0.0;
+    double rk[4], ck[4];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) rk[b] = rowk[buf][c0 + b] * ip;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) ck[a] = colk[buf][r0 + a];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int r = r0 + a, cc = c0 + b;
+        double v = fma(-ck[a], rk[b], m[a][b]);   // generic entry
+        if (r == k) v = rk[b];                     // pivot row: a / p
+        if (cc == k) v = (r == k) ? ip : -ck[a] * ip;   // pivot column
+        m[a][b] = v;
+      }
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int r = r0 + a, cc = c0 + b;
+      if (r < bs && cc < bs) {
+        P[cc * kGB + r] = m[a][b];
+        A[(int64_t)(K0 + cc) * n + K0 + r] = -m[a][b];
+      }
+    }
+}
+
+__global__ void __launch_bounds__(kGT) k_sw_diag(int n, double *A, int K0, int bs,
+                                                  double *P, int *info) {
+  sweep_diag(n, A, K0, bs, P, info);
+}
+
+// CTA I (I != K): F_I = the rows of tile I of the column block K (below the
+// diagonal: tile (I, K); above: the transposed tile (K, I) of the row
+// block), and G_I = F_I P; both n x bs, column-major
+__global__ void __launch_bounds__(kGT) k_sw_fg(int n, const double *A, int K0, int bs,
+                                               const double *P, double *F, double *G) {
+  const int I = blockIdx.x, i0 = I * kGB;
+  if (i0 == K0) return;
+  const int rows = min(kGB, n - i0);
+  // 16 independent copies per thread, unrolled so the loads overlap
+  if (i0 > K0) {
+#pragma unroll
+    for (int q = 0; q < kGB * kGB / kGT; ++q) {
+      const int e = threadIdx.x + q * kGT, i = e % kGB, k = e / kGB;
+      if (i < rows && k < bs) F[(int64_t)k * n + i0 + i] = A[(int64_t)(K0 + k) * n + i0 + i];
+    }
+  } else {
+    // A(K0 + k, i0 + i): k fastest for coalesced reads
+#pragma unroll
+    for (int q = 0; q < kGB * kGB / kGT; ++q) {
+      const int e = threadIdx.x + q * kGT, k = e % kGB, i = e / kGB;
+      if (i < rows && k < bs) F[(int64_t)k * n + i0 + i] = A[(int64_t)(i0 + i) * n + K0 + k];
+    }
+  }
+  __syncthreads();
+  __shared__ __align__(16) GemmSmem sm;
+  // G_I (rows x bs) = F_I (rows x bs) P (bs x bs); P[k][j] = P[j * kGB + k]
+  tile_gemm<false, false>(sm, rows, bs, bs, F + i0, n, P, kGB, G + i0, n, 1.0);
+}
+
+// lower tile (I, J), I >= J: the column block gets G_I, the row block left
+// of the diagonal G_J^T, every other tile A_IJ - G_I F_J^T.  The CTA of the
+// next diagonal tile (K+1, K+1) runs as block (0, 0), the first one
+// dispatched, and after its update inverts that block for the next sweep
+// (P and -P as k_sw_diag), so the diagonal inversion overlaps the rest of
+// the update instead of running alone between sweeps.
+__global__ void __launch_bounds__(kGT) k_sw_update(int n, double *A, int K0, int bs,
+                                                    const double *F, const double *G,
+                                                    double *P, int *info) {
+  int I = blockIdx.x, J = blockIdx.y;
+  const int Kn = K0 / kGB + 1;   // the next diagonal tile
+  const bool look = Kn * kGB < n;
+  if (look) {
+    if (I == 0 && J == 0) I = J = Kn;
+    else if (I == Kn && J == Kn) I = J = 0;
+  }
+  if (J > I) return;
+  const int i0 = I * kGB, j0 = J * kGB;
+  const int M = min(kGB, n - i0), N = min(kGB, n - j0);
+  if (i0 == K0 && j0 == K0) return;   // the diagonal block: swept already
+  if (j0 == K0) {                      // A(i0 + i, K0 + k) = G(i0 + i, k)
+    for (int e = threadIdx.x; e < M * bs; e += kGT) {
+      const int i = e % M, k = e / M;
+      A[(int64_t)(K0 + k) * n + i0 + i] = G[(int64_t)k * n + i0 + i];
+    }
+    return;
+  }
+  if (i0 == K0) {                      // A(K0 + k, j0 + j) = G(j0 + j, k)
+    for (int e = threadIdx.x; e < N * bs; e += kGT) {
+      const int k = e % bs, j = e / bs;
+      A[(int64_t)(j0 + j) * n + K0 + k] = G[(int64_t)k * n + j0 + j];
+    }
+    return;
+  }
+  __shared__ __align__(16) GemmSmem sm;
+  // Y[k][j] = F(j0 + j, k) = F[k * n + j0 + j]
+  tile_gemm<true, true>(sm, M, N, bs, G + i0, n, F + j0, n, A + (int64_t)j0 * n + i0, n,
+                        -1.0);
+  if (look && I == Kn && J == Kn) {
+    __syncthreads();   // the tile's update is visible to the whole CTA
+    sweep_diag(n, A, i0, M, P, info);
+  }
+}
+
+// A <- -A on the lower triangle, mirrored into the upper one
+__global__ void k_sw_final(int n, double *A) {
+  const int I = blockIdx.x, J = blockIdx.y;
+  if (J > I) return;
+  const int i0 = I * kGB, j0 = J * kGB;
+  const int M = min(kGB, n - i0), N = min(kGB, n - j0);
+  for (int e = threadIdx.x; e < M * N; e += blockDim.x) {
+    const int i = e % M, j = e / M;
+    const int gi = i0 + i, gj = j0 + j;
+    if (gi < gj) continue;   // diagonal tiles: the lower half writes both
+    const double v = -A[(int64_t)gj * n + gi];
+    A[(int64_t)gj * n + gi] = v;
+    if (gi != gj) A[(int64_t)gi * n + gj] = v;
+  }
+}
+
+}  // namespace
+
+size_t coarse_inverse_work(int64_t n) { return 2 * (size_t)n * kGB + kGB * kGB; }
+
+void launch_coarse_inverse(int64_t n64, double *A, double *work, int *info, cudaStream_t s) {
+  const int n = (int)n64;
+  const int nt = (n + kGB - 1) / kGB;
+  double *P = work, *F = work + kGB * kGB, *G = F + (size_t)n * kGB;
+  cudaMemsetAsync(info, 0, sizeof(int), s);
+  count_launch();
+  k_sw_diag<<<1, kGT, 0, s>>>(n, A, 0, std::min(kGB, n), P, info);
+  for (int K0 = 0; K0 < n; K0 += kGB) {
+    const int bs = std::min(kGB, n - K0);
+    count_launch(2);
+    k_sw_fg<<<nt, kGT, 0, s>>>(n, A, K0, bs, P, F, G);
+    k_sw_update<<<dim3(nt, nt), kGT, 0, s>>>(n, A, K0, bs, F, G, P, info);
+  }
+  count_launch();
+  k_sw_final<<<dim3(nt, nt), kGT, 0, s>>>(n, A);
+}
+
+}  // namespace tpo

@@ -817,25 +817,6 @@ void launch_to_dense(const Level &v, const double *S, double *A,
 }
 
 namespace {
-__global__ void k_eye(int64_t n, double *A) {
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * n;
-       t += (int64_t)gridDim.x * blockDim.x)
-    A[t] = (t / n == t % n) ? 1.0 : 0.0;
-}
-
-// full symmetric n x n matrix from the lower triangle of a column-major one:
-// A(r, c) = L(max(r, c), min(r, c))
-__global__ void k_sym_from_lower(int64_t n, const double *__restrict__ L,
-                                 double *__restrict__ A) {
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * n;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t c = t / n, r = t - c * n;
-    A[t] = r >= c ? L[t] : L[r * n + c];
-  }
-}
-}  // namespace
-
-namespace {
 __global__ void k_soa_to_aos(int64_t nn, const double *__restrict__ S,
                              double *__restrict__ A64, float *__restrict__ A32) {
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nn * 243;
@@ -854,16 +835,6 @@ void launch_soa_to_aos(int64_t nn, const double *S, double *A64, float *A32,
                        cudaStream_t s) {
   count_launch();
   k_soa_to_aos<<<grid_for(nn * 243, 256), 256, 0, s>>>(nn, S, A64, A32);
-}
-
-void launch_eye(int64_t n, double *A, cudaStream_t s) {
-  count_launch();
-  k_eye<<<grid_for(n * n, 256), 256, 0, s>>>(n, A);
-}
-
-void launch_sym_from_lower(int64_t n, const double *L, double *A, cudaStream_t s) {
-  count_launch();
-  k_sym_from_lower<<<grid_for(n * n, 256), 256, 0, s>>>(n, L, A);
 }
 
 template <typename T>

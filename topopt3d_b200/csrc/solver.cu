@@ -5,9 +5,6 @@
 // :673): KSP CG, nonzero initial guess, convergence on the unpreconditioned
 // residual ||b - K u|| <= rtol ||b||, PCMG with Galerkin coarse operators,
 // Chebyshev/Jacobi smoothing and a direct (here Cholesky) coarse solve.
-#include <cublas_v2.h>
-#include <cusolverDn.h>
-
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -473,76 +470,22 @@ int setup_on(Ctx &c, const tpo_solve_opts &o, cudaStream_t s) {
     }
   }
   CK(cudaGetLastError());
-  // coarsest level: dense Cholesky A = L L^T, then the explicit inverse
-  // A^-1 = X^T X with X = L^-1 (one triangular solve against the identity
-  // and a symmetric rank-n product, about half the time of solving
-  // A Y = I with both factors) for a bandwidth-parallel GEMV inside the
-  // V-cycle
+  // coarsest level: the explicit inverse of the dense operator (blocked
+  // Gauss-Jordan, kernels_coarse_inv.cu) for a bandwidth-parallel GEMV
+  // inside the V-cycle
   Level &cl = c.lev[c.L - 1];
   const double *Sc = (c.L == 1) ? c.S0 : cl.S64;
   const int64_t nc = 3 * cl.nn;
   c.nc = nc;
-  launch_to_dense(cl, Sc, c.Adense, s);
-  launch_eye(nc, c.Ainv, s);
+  launch_to_dense(cl, Sc, c.Ainv, s);
+  launch_coarse_inverse(nc, c.Ainv, c.Adense, c.dev_info, s);
   CK(cudaGetLastError());
-  cusolverDnHandle_t h = static_cast<cusolverDnHandle_t>(c.cusolver);
-  if (!h) {
-    if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) {
-      c.err = "cusolverDnCreate failed";
-      join();
-      return TPO_E_CUDA;
-    }
-    c.cusolver = h;
-  }
-  cusolverDnSetStream(h, s);
-  int lwork = 0;
-  if (cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, (int)nc, c.Adense,
-                                  (int)nc, &lwork) != CUSOLVER_STATUS_SUCCESS) {
-    c.err = "cusolverDnDpotrf_bufferSize failed";
-    join();
-    return TPO_E_CUDA;
-  }
-  if ((size_t)lwork > c.solver_work_n) {
-    if (c.solver_work) cudaFree(c.solver_work);
-    c.solver_work = nullptr;
-    CK(cudaMalloc(&c.solver_work, sizeof(double) * (size_t)lwork));
-    c.solver_work_n = lwork;
-  }
-  if (cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, (int)nc, c.Adense, (int)nc,
-                       c.solver_work, lwork, c.dev_info) != CUSOLVER_STATUS_SUCCESS) {
-    c.err = "coarse Cholesky factorisation failed";
-    join();
-    return TPO_E_CUDA;
-  }
-  cublasHandle_t hb = static_cast<cublasHandle_t>(c.cublas);
-  if (!hb) {
-    if (cublasCreate(&hb) != CUBLAS_STATUS_SUCCESS) {
-      c.err = "cublasCreate failed";
-      join();
-      return TPO_E_CUDA;
-    }
-    c.cublas = hb;
-  }
-  const double one = 1.0, zero = 0.0;
-  // Ainv <- L^-1 (Ainv holds the identity); Adense <- lower(X^T X)
-  if (cublasSetStream(hb, s) != CUBLAS_STATUS_SUCCESS ||
-      cublasSetPointerMode(hb, CUBLAS_POINTER_MODE_HOST) != CUBLAS_STATUS_SUCCESS ||
-      cublasDtrsm(hb, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
-                  CUBLAS_DIAG_NON_UNIT, (int)nc, (int)nc, &one, c.Adense, (int)nc,
-                  c.Ainv, (int)nc) != CUBLAS_STATUS_SUCCESS ||
-      cublasDsyrk(hb, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, (int)nc, (int)nc, &one,
-                  c.Ainv, (int)nc, &zero, c.Adense, (int)nc) != CUBLAS_STATUS_SUCCESS) {
-    c.err = "coarse inverse from the Cholesky factor failed";
-    join();
-    return TPO_E_CUDA;
-  }
-  launch_sym_from_lower(nc, c.Adense, c.Ainv, s);
   int info_h = 0;
   CK(cudaMemcpyAsync(&info_h, c.dev_info, sizeof(int), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   if (info_h != 0) {
-    c.err = "coarsest operator is not positive definite (potrf info " +
-            std::to_string(info_h) + ")";
+    c.err = "coarsest operator is not positive definite (pivot " +
+            std::to_string(info_h - 1) + ")";
     join();
     return TPO_E_BREAKDOWN;
   }

@@ -195,11 +195,8 @@ struct Ctx {
   double *oc_ws = nullptr;                    // OC update workspace (6 nElem)
   size_t io_bytes = 0;
 
-  // coarse factorisation
-  void *cusolver = nullptr;
-  double *Adense = nullptr;     // coarsest operator, dense (factorised in place)
-  double *solver_work = nullptr;
-  size_t solver_work_n = 0;
+  // coarsest inverse
+  double *Adense = nullptr;     // workspace of the coarsest inversion
   int *dev_info = nullptr;
 
   // stress stiffness: 27-point scalar stencil S[d * nn + n] and the
@@ -328,13 +325,15 @@ void launch_prolong_add(const Level &fine, const Level &coarse, const T *xc,
                         T *xf, cudaStream_t s, int nb = 1);
 void launch_to_dense(const Level &v, const double *S, double *A,
                      cudaStream_t s);
-void launch_eye(int64_t n, double *A, cudaStream_t s);
-// full symmetric matrix from the lower triangle of a column-major one
-void launch_sym_from_lower(int64_t n, const double *L, double *A, cudaStream_t s);
 // stencil SoA S[(nb*9 + 3r+s)*nn + n] -> node-major A[n*243 + (3r+s)*27 + nb]
 // (FP64 and an FP32 copy)
 void launch_soa_to_aos(int64_t nn, const double *S, double *A64, float *A32,
                        cudaStream_t s);
+// A (n x n, column-major, SPD) <- A^-1 in place by blocked Gauss-Jordan
+// (kernels_coarse_inv.cu); work holds coarse_inverse_work(n) doubles; *info
+// becomes the global index + 1 of the first pivot that is not positive
+size_t coarse_inverse_work(int64_t n);
+void launch_coarse_inverse(int64_t n, double *A, double *work, int *info, cudaStream_t s);
 template <typename T>
 void launch_coarse_gemv(int64_t n, const double *Ainv, const T *b, T *x,
                         cudaStream_t s, int nb = 1);
