@@ -53,7 +53,7 @@ def build(verbose: bool = False, force: bool = False, jobs: int = 8) -> str:
             _wait(procs, verbose)
             procs = []
     _wait(procs, verbose)
-    link = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcublas"]
+    link = [NVCC, *ARCH, "-shared", "-o", LIB, *objs]
     subprocess.run(link, check=True)
     return LIB
 

@@ -1,7 +1,6 @@
 // The C ABI (include/topopt_b200.h): context life cycle, boundary
 // conditions, the TopOpt call surface and data movement between caller
 // buffers and the context's HBM-resident state.
-#include <cublas_v2.h>
 
 #include <algorithm>
 #include <cmath>
@@ -258,8 +257,6 @@ void free_all(Ctx &c) {
   if (c.mma_h) cudaFreeHost(c.mma_h);
   c.mma_h = nullptr; dfree(c.ks_S); dfree(c.ks_H); dfree(c.eig_buf);
   c.eig_n = 0;
-  if (c.cublas) cublasDestroy(static_cast<cublasHandle_t>(c.cublas));
-  c.cublas = nullptr;
   dfree(c.scal); dfree(c.part); dfree(c.ticket); dfree(c.gbar); dfree(c.tmpe); dfree(c.tmpe2);
   dfree(c.io_a); dfree(c.io_b);
   dfree(c.oc_ws);

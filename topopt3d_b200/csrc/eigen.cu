@@ -10,16 +10,16 @@
 //
 // Per iteration, with X the m current Ritz vectors (AX = Ks X, BX = K X):
 //   R = AX - BX diag(theta);  W = mask(T R)  (T = one V-cycle)
-//   Rayleigh-Ritz of (Ks, K) on span[X W P]: Gram blocks by DGEMM, the
+//   Rayleigh-Ritz of (Ks, K) on span[X W P]: every Gram block in one pass
+//   over the basis and its images (kernels_eig.cu), the
 //   small generalized problem solved on the host by SVQB (eigen-
 //   decomposition of the diagonally scaled K-Gram, directions below a
 //   relative 1e-13 dropped) and Jacobi;
 //   X <- [X W P] C,  P <- [0 W P] C  (images AX, BX, AP, BP updated by the
-//   same coefficients; recomputed from scratch every 20 iterations).
+//   same coefficients, all six in one pass; recomputed from scratch every
+//   20 iterations).
 // Fixed degrees of freedom are masked out of every block (their rows and
 // columns are zero in Ks and identity in K, i.e. lambda = 0 there).
-#include <cublas_v2.h>
-
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -79,20 +79,6 @@ __global__ void k_mask(int64_t n, int m, const uint8_t *__restrict__ fix,
        t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = t % n;
     if ((fix[i / 3] >> (i % 3)) & 1u) X[t] = 0.0;
-  }
-}
-
-struct Theta {
-  double v[32];
-};
-
-// R[:, j] = AX[:, j] - theta_j BX[:, j]
-__global__ void k_resid(int64_t n, int m, const double *__restrict__ AX,
-                        const double *__restrict__ BX, Theta th, double *R) {
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * m;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int j = (int)(t / n);
-    R[t] = AX[t] - th.v[j] * BX[t];
   }
 }
 
@@ -219,14 +205,6 @@ int rayleigh_ritz(int k, int m, const std::vector<double> &H,
     }                                                                  \
   } while (0)
 
-#define CB(call)                                                       \
-  do {                                                                 \
-    if ((call) != CUBLAS_STATUS_SUCCESS) {                             \
-      c.err = std::string(#call) + " failed";                          \
-      return TPO_E_CUDA;                                               \
-    }                                                                  \
-  } while (0)
-
 struct Blocks {
   double *X, *AX, *BX, *W, *AW, *BW, *P, *AP, *BP;
   double *Xn, *AXn, *BXn, *Pn, *APn, *BPn, *R;
@@ -255,19 +233,10 @@ int buckling(Ctx &c, const tpo_eig_opts &o, double *lambda, double *phi,
   const int64_t n = 3 * c.nn;
   const int m = o.block, nev = o.nev;
   cudaStream_t s = c.stream;
-  cublasHandle_t h = static_cast<cublasHandle_t>(c.cublas);
-  if (!h) {
-    if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) {
-      c.err = "cublasCreate failed";
-      return TPO_E_CUDA;
-    }
-    c.cublas = h;
-  }
-  CB(cublasSetStream(h, s));
-  CB(cublasSetPointerMode(h, CUBLAS_POINTER_MODE_HOST));
   // workspace: 16 blocks of n x m and the small Gram/coefficient matrices
   const size_t blk = (size_t)n * m;
-  const size_t need = 16 * blk + 2 * (size_t)(3 * m) * (3 * m) + (size_t)(3 * m) * m + 2 * m;
+  const size_t need = 16 * blk + 2 * (size_t)(3 * m) * (3 * m) + (size_t)(3 * m) * m + 2 * m +
+                      eig_gram_scratch(3 * m);
   if (c.eig_n < need) {
     if (c.eig_buf) cudaFree(c.eig_buf);
     c.eig_buf = nullptr;
@@ -282,7 +251,7 @@ int buckling(Ctx &c, const tpo_eig_opts &o, double *lambda, double *phi,
   for (int i = 0; i < 16; ++i) *slots[i] = base + i * blk;
   const int K3 = 3 * m;
   double *dH = base + 16 * blk, *dG = dH + K3 * K3, *dC = dG + K3 * K3,
-         *dnrm = dC + K3 * m;
+         *dnrm = dC + K3 * m, *dpart = dnrm + 2 * m;
   if (int rc = ensure_columns(c, kMaxBatch)) return rc;
   tpo_solve_opts so = c.setup_opts;
 
@@ -302,53 +271,21 @@ int buckling(Ctx &c, const tpo_eig_opts &o, double *lambda, double *phi,
   // Gram blocks of the basis [X W P] (first nblk of them): out (k x k)
   std::vector<double> Hh, Gh;
   auto gram = [&](int nblk) -> int {
-    const double *V[3] = {b.X, b.W, b.P};
-    const double *AV[3] = {b.AX, b.AW, b.AP};
-    const double *BV[3] = {b.BX, b.BW, b.BP};
+    const EigCols cols{{b.X, b.W, b.P}, {b.AX, b.AW, b.AP}, {b.BX, b.BW, b.BP}};
     const int k = nblk * m;
-    const double one = 1.0, zero = 0.0;
-    for (int bi = 0; bi < nblk; ++bi)
-      for (int bj = bi; bj < nblk; ++bj) {
-        CB(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, m, m, (int)n, &one, V[bi], (int)n,
-                       AV[bj], (int)n, &zero, dH + (size_t)bj * m * k + bi * m, k));
-        CB(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, m, m, (int)n, &one, V[bi], (int)n,
-                       BV[bj], (int)n, &zero, dG + (size_t)bj * m * k + bi * m, k));
-      }
+    launch_eig_gram(n, m, nblk, cols, dpart, dH, dG, s);
     Hh.assign((size_t)k * k, 0.0);
     Gh.assign((size_t)k * k, 0.0);
     CK(cudaMemcpyAsync(Hh.data(), dH, sizeof(double) * k * k, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(Gh.data(), dG, sizeof(double) * k * k, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    // the upper block triangle was formed; mirror it
-    for (int bi = 0; bi < nblk; ++bi)
-      for (int bj = 0; bj < bi; ++bj)
-        for (int jj = 0; jj < m; ++jj)
-          for (int ii = 0; ii < m; ++ii) {
-            const int r = bi * m + ii, q = bj * m + jj;
-            Hh[(size_t)q * k + r] = Hh[(size_t)r * k + q];
-            Gh[(size_t)q * k + r] = Gh[(size_t)r * k + q];
-          }
-    for (int j = 0; j < k; ++j)   // symmetrise the diagonal blocks
+    for (int j = 0; j < k; ++j)   // symmetrise
       for (int i = 0; i < j; ++i) {
         const double hv = 0.5 * (Hh[(size_t)j * k + i] + Hh[(size_t)i * k + j]);
         const double gv = 0.5 * (Gh[(size_t)j * k + i] + Gh[(size_t)i * k + j]);
         Hh[(size_t)j * k + i] = Hh[(size_t)i * k + j] = hv;
         Gh[(size_t)j * k + i] = Gh[(size_t)i * k + j] = gv;
       }
-    return TPO_OK;
-  };
-  // out = sum over the basis blocks of V_b C_b (rows of C of block b),
-  // skipping block 0 when with_x is false
-  auto combine = [&](int nblk, const double *Cd, int k, bool with_x,
-                     const double *const V[3], double *out) -> int {
-    const double one = 1.0, zero = 0.0;
-    bool first = true;
-    for (int bi = with_x ? 0 : 1; bi < nblk; ++bi) {
-      CB(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, m, m, &one, V[bi], (int)n,
-                     Cd + bi * m, k, first ? &zero : &one, out, (int)n));
-      first = false;
-    }
-    if (first) CK(cudaMemsetAsync(out, 0, sizeof(double) * blk, s));
     return TPO_OK;
   };
 
@@ -365,13 +302,10 @@ int buckling(Ctx &c, const tpo_eig_opts &o, double *lambda, double *phi,
   }
   CK(cudaMemcpyAsync(dC, C.data(), sizeof(double) * m * m, cudaMemcpyHostToDevice, s));
   {
-    const double one = 1.0, zero = 0.0;
-    CB(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, m, m, &one, b.X, (int)n, dC, m,
-                   &zero, b.Xn, (int)n));
-    CB(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, m, m, &one, b.AX, (int)n, dC, m,
-                   &zero, b.AXn, (int)n));
-    CB(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, m, m, &one, b.BX, (int)n, dC, m,
-                   &zero, b.BXn, (int)n));
+    const EigCols cols{{b.X, nullptr, nullptr}, {b.AX, nullptr, nullptr},
+                       {b.BX, nullptr, nullptr}};
+    const EigOut out{{b.Xn, b.AXn, b.BXn}, {nullptr, nullptr, nullptr}};
+    launch_eig_combine(n, m, 1, cols, dC, out, false, s);
     std::swap(b.X, b.Xn);
     std::swap(b.AX, b.AXn);
     std::swap(b.BX, b.BXn);
@@ -383,16 +317,9 @@ int buckling(Ctx &c, const tpo_eig_opts &o, double *lambda, double *phi,
   std::vector<double> nrm(2 * m);
   for (;;) {
     // residuals and their relative norms
-    Theta th{};
+    EigTheta th{};
     for (int j = 0; j < m; ++j) th.v[j] = theta[j];
-    count_launch();
-    k_resid<<<grid_for(n * m, 256), 256, 0, s>>>(n, m, b.AX, b.BX, th, b.R);
-    CB(cublasSetPointerMode(h, CUBLAS_POINTER_MODE_DEVICE));
-    for (int j = 0; j < m; ++j) {
-      CB(cublasDnrm2(h, (int)n, b.R + j * n, 1, dnrm + j));
-      CB(cublasDnrm2(h, (int)n, b.BX + j * n, 1, dnrm + m + j));
-    }
-    CB(cublasSetPointerMode(h, CUBLAS_POINTER_MODE_HOST));
+    launch_eig_resid_norms(n, m, b.AX, b.BX, th, b.R, dpart, dnrm, s);
     CK(cudaMemcpyAsync(nrm.data(), dnrm, sizeof(double) * 2 * m, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     nconv = 0;
@@ -428,15 +355,11 @@ int buckling(Ctx &c, const tpo_eig_opts &o, double *lambda, double *phi,
     }
     const int k = nblk * m;
     CK(cudaMemcpyAsync(dC, C.data(), sizeof(double) * k * m, cudaMemcpyHostToDevice, s));
-    const double *V[3] = {b.X, b.W, b.P};
-    const double *AV[3] = {b.AX, b.AW, b.AP};
-    const double *BV[3] = {b.BX, b.BW, b.BP};
-    if (int rc = combine(nblk, dC, k, true, V, b.Xn)) return rc;
-    if (int rc = combine(nblk, dC, k, true, AV, b.AXn)) return rc;
-    if (int rc = combine(nblk, dC, k, true, BV, b.BXn)) return rc;
-    if (int rc = combine(nblk, dC, k, false, V, b.Pn)) return rc;
-    if (int rc = combine(nblk, dC, k, false, AV, b.APn)) return rc;
-    if (int rc = combine(nblk, dC, k, false, BV, b.BPn)) return rc;
+    {
+      const EigCols cols{{b.X, b.W, b.P}, {b.AX, b.AW, b.AP}, {b.BX, b.BW, b.BP}};
+      const EigOut out{{b.Xn, b.AXn, b.BXn}, {b.Pn, b.APn, b.BPn}};
+      launch_eig_combine(n, m, nblk, cols, dC, out, true, s);
+    }
     std::swap(b.X, b.Xn);
     std::swap(b.AX, b.AXn);
     std::swap(b.BX, b.BXn);

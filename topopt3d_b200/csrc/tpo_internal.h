@@ -204,8 +204,7 @@ struct Ctx {
   KsConst ksc{};
   double *ks_S = nullptr, *ks_H = nullptr;
   bool ks_ready = false;
-  // eigensolver: cuBLAS handle and the block workspace
-  void *cublas = nullptr;
+  // eigensolver block workspace
   double *eig_buf = nullptr;
   size_t eig_n = 0;
   double *bk_buf = nullptr;   // buckling-sensitivity workspace
@@ -405,6 +404,32 @@ struct BkCoef {
 // d(phi^T ks_e phi)/du_e (W: 24 x nElem scratch), zero at fixed dofs
 void launch_bk_adj_rhs(const Ctx &c, const double *phi, double *W, double *rhs,
                        cudaStream_t s);
+// block eigensolver kernels (kernels_eig.cu).  A basis of nblk blocks of m
+// columns (n rows, column-major): L[b] the vectors, A[b] and B[b] their
+// two operator images
+struct EigCols {
+  const double *L[3], *A[3], *B[3];
+};
+struct EigOut {
+  double *X[3], *P[3];   // per image group (vectors, A, B)
+};
+struct EigTheta {
+  double v[kMaxEigPairs];
+};
+// doubles of partial sums launch_eig_gram and launch_eig_resid_norms need
+// for a basis of k columns
+size_t eig_gram_scratch(int k);
+// H = L^T A and G = L^T B over all k = nblk m columns (k x k, column-major)
+void launch_eig_gram(int64_t n, int m, int nblk, const EigCols &cols, double *part, double *H,
+                     double *G, cudaStream_t s);
+// out.X[g] = [group g blocks] C (C: k x m) and, with want_p, out.P[g] the
+// same without block 0
+void launch_eig_combine(int64_t n, int m, int nblk, const EigCols &cols, const double *C,
+                        const EigOut &out, bool want_p, cudaStream_t s);
+// R = AX - BX diag(theta), nrm[j] = ||R_j||, nrm[m + j] = ||BX_j||
+void launch_eig_resid_norms(int64_t n, int m, const double *AX, const double *BX,
+                            const EigTheta &th, double *R, double *part, double *nrm,
+                            cudaStream_t s);
 // frequency (kernels_ks.cu): the lumped mass diagonal m (3 nn) from c.rho,
 // and the gradient g_e from nterms eigenvector columns (stride ld)
 void launch_lumped_mass(const Ctx &c, double scale, const double *mlump, double *m,
