@@ -127,6 +127,31 @@ def test_galerkin_levels_and_vcycle(T, oracle):
     assert rel(z32, ref.vcycle(r)) < 1e-4
 
 
+def test_mixed_setup_fp32_chebyshev_bounds(T, oracle):
+    """A hierarchy set up for the mixed form takes the Chebyshev bounds of
+    the fine level and the half-stored level below it from FP32 power
+    iterations (the levels whose smoothers then run in FP32); they agree
+    with the oracle's FP64 estimates to FP32 round-off, the coarser levels
+    stay FP64 and exact, and a set-up for the FP64 form restores the FP64
+    bounds.  The mixed solve on that hierarchy still matches the oracle."""
+    nel = (24, 12, 12)
+    t, ref = pair(T, oracle, nel, levels=3, seed=2)
+    t.FEAssemble(T.default_opts(precision=T.PREC_MIXED))
+    assert t.level_lambda(0) != ref.level_lambda(0)   # the FP32 estimate
+    for l in range(2):
+        lam, lo = t.level_lambda(l), ref.level_lambda(l)
+        assert abs(lam - lo) < 1e-5 * lo, (l, lam, lo)
+    U = np.zeros(3 * t.nNode)
+    t.set("U", U)
+    info = t.FESolve(T.default_opts(precision=T.PREC_MIXED))
+    Uo, st, _, _ = ref.solve()
+    assert info["status"] == 0 and st == 0
+    assert rel(t.U, Uo) < 1e-7
+    t.FEAssemble(T.default_opts(precision=T.PREC_FP64))
+    for l in range(2):
+        assert abs(t.level_lambda(l) - ref.level_lambda(l)) < 1e-10 * ref.level_lambda(l)
+
+
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_cfg0_solve_compliance_sensitivity(T, oracle, prec):
     nel = P.CONFIGS["cfg0"]["nel"]

@@ -14,7 +14,8 @@
 // block has been swept the matrix is -A^-1, and a last pass negates it and
 // fills the upper triangle.  A sweep is two launches: F and G for every row
 // block (k_sw_fg), and the rank-64 update of the lower tiles on 64 x 64
-// FP64 tiles (k_sw_update), one CTA of which then inverts the next
+// tiles with FP64 tensor-core MMAs (k_sw_update), one CTA of which then
+// inverts the next
 // diagonal block by scalar Gauss-Jordan with a 4 x 4 block of it in each
 // thread's registers (sweep_diag; k_sw_diag for the first block).
 #include "tpo_internal.h"
@@ -26,72 +27,92 @@ namespace {
 constexpr int kGB = 64;    // block size (rows / columns of a pivot block)
 constexpr int kGT = 256;   // threads per CTA: 16 x 16, 4 x 4 outputs each
 constexpr int kKC = 32;    // k-chunk staged in shared memory
+#ifndef TPO_SW_MINB
+#define TPO_SW_MINB 3
+#endif
 
-// the staging buffers of tile_gemm, declared once by each calling kernel
+// D (8 x 8) += A (8 x 4) B (4 x 8) in FP64 on the tensor cores.  Fragments
+// (PTX ISA, mma.m8n8k4 .f64): lane = 4 g + q holds A[g][q], B[q][g] and
+// D[g][2q], D[g][2q + 1].
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+// the staging buffers of tile_gemm, declared once by each calling kernel:
+// Xs[i][k] and Ys[j][k] for a chunk of kKC of the depth (rows padded to 36
+// doubles: the fragment reads of a warp then fall on distinct bank pairs)
+constexpr int kKP = kKC + 4;
 struct GemmSmem {
-  double Xs[kKC][kGB];
-  double Ys[kKC][kGB + 2];
+  double Xs[kGB][kKP];
+  double Ys[kGB][kKP];
 };
 
 // C (M x N, column-major, ldc) = (ACC ? C : 0) + s X Y for M, N <= 64 and a
 // depth Kd <= kGB, with X[i][k] = X[k * ldx + i] and Y[k][j] = Y[k * ldy + j]
 // (YT) or Y[j * ldy + k].  Every read of X and Y happens before the first
 // write of C.  X and Y are plain (coherent) loads: the caller may have
-// written them earlier in the same kernel.
+// written them earlier in the same kernel.  8 warps, each a 16 x 32 block
+// of the 64 x 64 tile as 2 x 4 tensor-core tiles of 8 x 8.
 template <bool ACC, bool YT>
 __device__ __forceinline__ void tile_gemm(GemmSmem &sm, int M, int N, int Kd,
                                           const double *X, int ldx, const double *Y,
                                           int ldy, double *C,
                                           int ldc, double s) {
-  auto &Xs = sm.Xs;
-  auto &Ys = sm.Ys;
-  const int t = threadIdx.x;
-  const int tx = t % 16, ty = t / 16;
-  double acc[4][4];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  const int r0 = (w >> 1) * 16, c0 = (w & 1) * 32;
+  double acc[2][4][2];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < 2; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
   for (int kc = 0; kc < Kd; kc += kKC) {
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < kKC * kGB / kGT; ++q) {
-      const int e = t + q * kGT;
-      const int i = e % kGB, k = e / kGB;   // rows contiguous
-      Xs[k][i] = (i < M && kc + k < Kd) ? X[(int64_t)(kc + k) * ldx + i] : 0.0;
+    for (int e8 = 0; e8 < kKC * kGB / kGT; ++e8) {
+      const int e = t + e8 * kGT;
+      {
+        const int i = e % kGB, k = e / kGB;   // X: rows contiguous
+        sm.Xs[i][k] = (i < M && kc + k < Kd) ? X[(int64_t)(kc + k) * ldx + i] : 0.0;
+      }
       if (YT) {
-        Ys[k][i] = (i < N && kc + k < Kd) ? Y[(int64_t)(kc + k) * ldy + i] : 0.0;
+        const int j = e % kGB, k = e / kGB;   // Y[k][j]: j contiguous
+        sm.Ys[j][k] = (j < N && kc + k < Kd) ? Y[(int64_t)(kc + k) * ldy + j] : 0.0;
       } else {
-        const int k2 = e % kKC, j = e / kKC;   // depth contiguous
-        Ys[k2][j] = (j < N && kc + k2 < Kd) ? Y[(int64_t)j * ldy + kc + k2] : 0.0;
+        const int k = e % kKC, j = e / kKC;   // Y[k][j] = Y[j * ldy + k]: k contiguous
+        sm.Ys[j][k] = (j < N && kc + k < Kd) ? Y[(int64_t)j * ldy + kc + k] : 0.0;
       }
     }
     __syncthreads();
-#pragma unroll 8
-    for (int k = 0; k < kKC; ++k) {
-      const double2 x01 = *reinterpret_cast<const double2 *>(&Xs[k][tx * 4]);
-      const double2 x23 = *reinterpret_cast<const double2 *>(&Xs[k][tx * 4 + 2]);
-      const double2 y01 = *reinterpret_cast<const double2 *>(&Ys[k][ty * 4]);
-      const double2 y23 = *reinterpret_cast<const double2 *>(&Ys[k][ty * 4 + 2]);
-      const double xv[4] = {x01.x, x01.y, x23.x, x23.y};
-      const double yv[4] = {y01.x, y01.y, y23.x, y23.y};
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+    for (int k0 = 0; k0 < kKC; k0 += 4) {
+      double av[2], bv[4];
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = fma(xv[a], yv[b], acc[a][b]);
+      for (int a = 0; a < 2; ++a) av[a] = sm.Xs[r0 + a * 8 + g][k0 + q];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) bv[b] = sm.Ys[c0 + b * 8 + g][k0 + q];
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) dmma(acc[a][b], av[a], bv[b]);
     }
   }
+  __syncthreads();   // C may alias an operand
 #pragma unroll
-  for (int b = 0; b < 4; ++b) {
-    const int j = ty * 4 + b;
-    if (j >= N) continue;
+  for (int a = 0; a < 2; ++a) {
+    const int i = r0 + a * 8 + g;
+    if (i >= M) continue;
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      const int i = tx * 4 + a;
-      if (i >= M) continue;
-      double *c = C + (int64_t)j * ldc + i;
-      *c = ACC ? fma(s, acc[a][b], *c) : s * acc[a][b];
-    }
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int j = c0 + b * 8 + 2 * q + h;
+        if (j >= N) continue;
+        double *c = C + (int64_t)j * ldc + i;
+        *c = ACC ? fma(s, acc[a][b][h], *c) : s * acc[a][b][h];
+      }
   }
 }
 
@@ -179,7 +200,7 @@ __global__ void __launch_bounds__(kGT) k_sw_diag(int n, double *A, int K0, int b
 // CTA I (I != K): F_I = the rows of tile I of the column block K (below the
 // diagonal: tile (I, K); above: the transposed tile (K, I) of the row
 // block), and G_I = F_I P; both n x bs, column-major
-__global__ void __launch_bounds__(kGT) k_sw_fg(int n, const double *A, int K0, int bs,
+__global__ void __launch_bounds__(kGT, 3) k_sw_fg(int n, const double *A, int K0, int bs,
                                                const double *P, double *F, double *G) {
   const int I = blockIdx.x, i0 = I * kGB;
   if (i0 == K0) return;
@@ -211,7 +232,7 @@ __global__ void __launch_bounds__(kGT) k_sw_fg(int n, const double *A, int K0, i
 // dispatched, and after its update inverts that block for the next sweep
 // (P and -P as k_sw_diag), so the diagonal inversion overlaps the rest of
 // the update instead of running alone between sweeps.
-__global__ void __launch_bounds__(kGT) k_sw_update(int n, double *A, int K0, int bs,
+__global__ void __launch_bounds__(kGT, TPO_SW_MINB) k_sw_update(int n, double *A, int K0, int bs,
                                                     const double *F, const double *G,
                                                     double *P, int *info) {
   int I = blockIdx.x, J = blockIdx.y;

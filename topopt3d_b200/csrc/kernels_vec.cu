@@ -139,22 +139,25 @@ __device__ __forceinline__ double start_value(uint64_t i) {
   return (double)(z >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
 }
 
-__global__ void k_power_start(int64_t n, double *a) {
+template <typename T>
+__global__ void k_power_start(int64_t n, T *a) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
-    a[i] = start_value((uint64_t)i);
+    a[i] = static_cast<T>(start_value((uint64_t)i));
 }
 
+// w *= dinv and ||w||^2, accumulated in FP64 for either storage type
+template <typename T>
 __global__ void __launch_bounds__(kRedThreads)
-    k_scale_diag_dot(int64_t n, double *__restrict__ w, const double *__restrict__ dinv,
+    k_scale_diag_dot(int64_t n, T *__restrict__ w, const T *__restrict__ dinv,
                      double *part, unsigned int *ticket, double *out,
                      double *shift_to) {
   double s = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const double wi = w[i] * dinv[i];
+    const T wi = w[i] * dinv[i];
     w[i] = wi;
-    s += wi * wi;
+    s += static_cast<double>(wi) * static_cast<double>(wi);
   }
   finish_reduction(s, part, ticket, out, shift_to);
 }
@@ -267,18 +270,28 @@ template void launch_cg_update<float>(const Ctx &, int64_t, float *, float *,
                                       const double *, double *, cudaStream_t,
                                       int);
 
-void launch_power_start(int64_t n, double *a, cudaStream_t s) {
+template <typename T>
+void launch_power_start(int64_t n, T *a, cudaStream_t s) {
   count_launch();
-  k_power_start<<<grid_for(n, 256), 256, 0, s>>>(n, a);
+  k_power_start<T><<<grid_for(n, 256), 256, 0, s>>>(n, a);
 }
+template void launch_power_start<double>(int64_t, double *, cudaStream_t);
+template void launch_power_start<float>(int64_t, float *, cudaStream_t);
 
-void launch_scale_diag_dot(const Ctx &c, int64_t n, double *w, const double *dinv,
-                           double *out, double *shift_to, cudaStream_t s,
-                           double *part, unsigned int *ticket) {
+template <typename T>
+void launch_scale_diag_dot(const Ctx &c, int64_t n, T *w, const T *dinv, double *out,
+                           double *shift_to, cudaStream_t s, double *part,
+                           unsigned int *ticket) {
   count_launch();
-  k_scale_diag_dot<<<red_grid(1), kRedThreads, 0, s>>>(
+  k_scale_diag_dot<T><<<red_grid(1), kRedThreads, 0, s>>>(
       n, w, dinv, part ? part : c.part, ticket ? ticket : c.ticket, out, shift_to);
 }
+template void launch_scale_diag_dot<double>(const Ctx &, int64_t, double *, const double *,
+                                            double *, double *, cudaStream_t, double *,
+                                            unsigned int *);
+template void launch_scale_diag_dot<float>(const Ctx &, int64_t, float *, const float *,
+                                           double *, double *, cudaStream_t, double *,
+                                           unsigned int *);
 
 void launch_to_f32_scaled(int64_t n, const double *a, const double *scal,
                           float *b, cudaStream_t s, int nb) {

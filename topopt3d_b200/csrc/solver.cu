@@ -381,19 +381,32 @@ void invalidate_graphs(Ctx &c) {
 // which leaves ||v_k||^2 in scal[SC_POWER + l] and ||v_{k-1}||^2 in
 // scal[SC_POWER_PREV + l].  lambda = ||v_k|| / ||v_{k-1}|| is then the
 // estimate ||D^-1 A a|| of the normalised iteration, a = v_{k-1}/||v_{k-1}||.
-void power_iteration(Ctx &c, int l, int its, cudaStream_t s, double *part,
-                     unsigned int *ticket) {
+template <typename T>
+void power_iteration_t(Ctx &c, int l, int its, cudaStream_t s, double *part,
+                       unsigned int *ticket) {
   Level &v = c.lev[l];
   const int64_t n = 3 * v.nn;
-  double *a = v.d64, *w = v.a64;
+  LV<T> wv = lv(v, (T *)nullptr);
+  T *a = wv.d, *w = wv.a;
   double *nrm = c.scal + SC_POWER + l, *prev = c.scal + SC_POWER_PREV + l;
-  launch_power_start(n, a, s);
-  launch_dot<double>(c, n, a, a, nrm, nullptr, s, 1, part, ticket);
+  launch_power_start<T>(n, a, s);
+  launch_dot<T>(c, n, a, a, nrm, nullptr, s, 1, part, ticket);
   for (int k = 0; k < its; ++k) {
-    level_apply<double>(c, l, a, nullptr, w, s);
-    launch_scale_diag_dot(c, n, w, v.dinv64, nrm, prev, s, part, ticket);
+    level_apply<T>(c, l, a, nullptr, w, s);
+    launch_scale_diag_dot<T>(c, n, w, wv.dinv, nrm, prev, s, part, ticket);
     std::swap(a, w);
   }
+}
+
+// fp32: the hierarchy is set up for the mixed form, whose smoothers run in
+// FP32; the fine level and the half-stored level below it (the levels with
+// FP32 operators) then take their Chebyshev bounds from FP32 iterations
+void power_iteration(Ctx &c, int l, int its, cudaStream_t s, double *part,
+                     unsigned int *ticket, bool fp32) {
+  if (fp32 && (l == 0 || l < c.ps))
+    power_iteration_t<float>(c, l, its, s, part, ticket);
+  else
+    power_iteration_t<double>(c, l, its, s, part, ticket);
 }
 
 // lambda of level l from the power iteration's two last squared norms in
@@ -404,7 +417,7 @@ double power_lambda(const Ctx &c, int l) {
 
 int estimate_lambda(Ctx &c, int l, int its, double *lam) {
   cudaStream_t s = c.stream;
-  power_iteration(c, l, its, s, nullptr, nullptr);
+  power_iteration(c, l, its, s, nullptr, nullptr, false);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(c.scal_h + SC_POWER, c.scal + SC_POWER,
                      sizeof(double) * (SC_POWER_PREV + kMaxLevels - SC_POWER),
@@ -431,7 +444,8 @@ int setup_on(Ctx &c, const tpo_solve_opts &o, cudaStream_t s) {
     CK(cudaEventRecord(c.lev_ev[l], s));
     CK(cudaStreamWaitEvent(c.aux_stream[i], c.lev_ev[l], 0));
     power_iteration(c, l, o.power_its, c.aux_stream[i],
-                    c.part + kAuxPart + i * kRedBlocks, c.ticket + kMaxBatch + i);
+                    c.part + kAuxPart + i * kRedBlocks, c.ticket + kMaxBatch + i,
+                    o.precision == TPO_PREC_MIXED);
     return TPO_OK;
   };
   auto join = [&]() {

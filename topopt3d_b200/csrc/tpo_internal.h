@@ -368,12 +368,14 @@ template <typename T>
 void launch_cg_update(const Ctx &c, int64_t n, T *x, T *r, const T *p,
                       const T *q, const double *scal, double *rr,
                       cudaStream_t s, int nb = 1);
-void launch_power_start(int64_t n, double *a, cudaStream_t s);
-// w *= dinv and its squared norm into *out (the previous *out into
-// *shift_to), one pass; reduction scratch as launch_dot's
-void launch_scale_diag_dot(const Ctx &c, int64_t n, double *w, const double *dinv,
-                           double *out, double *shift_to, cudaStream_t s,
-                           double *part, unsigned int *ticket);
+template <typename T>
+void launch_power_start(int64_t n, T *a, cudaStream_t s);
+// w *= dinv and its squared norm (FP64 sums) into *out (the previous *out
+// into *shift_to), one pass; reduction scratch as launch_dot's
+template <typename T>
+void launch_scale_diag_dot(const Ctx &c, int64_t n, T *w, const T *dinv, double *out,
+                           double *shift_to, cudaStream_t s, double *part,
+                           unsigned int *ticket);
 void launch_to_f32_scaled(int64_t n, const double *a, const double *scal,
                           float *b, cudaStream_t s, int nb = 1);
 void launch_axpy_f32(int64_t n, double *U, const float *d, const double *scal,
