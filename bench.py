@@ -54,7 +54,7 @@ def parse():
     # --config also selects the reference arm's problem (default 192x96x96)
     ap.add_argument("--kernel", default=None,
                     choices=["apply32", "apply64", "vcycle32", "vcycle64",
-                             "solve_mixed", "solve_fp64", "mma", "setup"])
+                             "solve_mixed", "solve_fp64", "mma", "setup", "setup_mixed"])
     ap.add_argument("--config", default=CONFIG)
     ap.add_argument("--reps", type=int, default=3)
     return ap.parse_args()
@@ -761,9 +761,11 @@ def run_kernel_case(args):
                                     C.byref(ch), L.MEM_DEVICE)
             assert rc == 0, lib.tpo_last_error(t._h)
             continue
-        if args.kernel == "setup":
+        if args.kernel in ("setup", "setup_mixed"):
             # FEAssemble / PCSetUp for the same design: the whole hierarchy
-            t.FEAssemble()
+            # (FP64 form, or the mixed form's FP32 Chebyshev bounds)
+            t.FEAssemble(T.default_opts(precision=T.PREC_MIXED)
+                         if args.kernel == "setup_mixed" else None)
             continue
         if args.kernel == "apply32":
             rc = lib.tpo_apply_f32(t._h, C.c_void_p(u32.data_ptr()),

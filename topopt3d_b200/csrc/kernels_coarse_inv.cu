@@ -26,7 +26,6 @@ namespace {
 
 constexpr int kGB = 64;    // block size (rows / columns of a pivot block)
 constexpr int kGT = 256;   // threads per CTA: 16 x 16, 4 x 4 outputs each
-constexpr int kKC = 32;    // k-chunk staged in shared memory
 #ifndef TPO_SW_MINB
 #define TPO_SW_MINB 3
 #endif
@@ -40,64 +39,87 @@ __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
                : "d"(a), "d"(b));
 }
 
-// the staging buffers of tile_gemm, declared once by each calling kernel:
-// Xs[i][k] and Ys[j][k] for a chunk of kKC of the depth (rows padded to 36
-// doubles: the fragment reads of a warp then fall on distinct bank pairs)
-constexpr int kKP = kKC + 4;
-struct GemmSmem {
-  double Xs[kGB][kKP];
-  double Ys[kGB][kKP];
-};
+// 8-byte asynchronous copy global -> shared; src_bytes 0 fills zeros (the
+// source address must still be valid)
+__device__ __forceinline__ void cp_async8(double *dst, const double *src, int src_bytes) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src),
+               "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// tile_gemm's operands in dynamic shared memory, the whole depth at once:
+// Xs[k][i] and, by layout, Ys[k][j] (YT) or Ys[j][k]; rows padded to 68
+// doubles so a warp's fragment reads fall on distinct bank pairs
+constexpr int kLd = kGB + 4;
+constexpr size_t kGemmSmem = 2 * sizeof(double) * kGB * kLd;
 
 // C (M x N, column-major, ldc) = (ACC ? C : 0) + s X Y for M, N <= 64 and a
 // depth Kd <= kGB, with X[i][k] = X[k * ldx + i] and Y[k][j] = Y[k * ldy + j]
-// (YT) or Y[j * ldy + k].  Every read of X and Y happens before the first
-// write of C.  X and Y are plain (coherent) loads: the caller may have
-// written them earlier in the same kernel.  8 warps, each a 16 x 32 block
-// of the 64 x 64 tile as 2 x 4 tensor-core tiles of 8 x 8.
+// (YT) or Y[j * ldy + k].  The operands are staged with asynchronous copies
+// and, with ACC, the thread's part of C is read while they are in flight;
+// every read of X and Y happens before the first write of C.  8 warps, each
+// a 16 x 32 block of the 64 x 64 tile as 2 x 4 tensor-core tiles of 8 x 8.
 template <bool ACC, bool YT>
-__device__ __forceinline__ void tile_gemm(GemmSmem &sm, int M, int N, int Kd,
+__device__ __forceinline__ void tile_gemm(double *smem, int M, int N, int Kd,
                                           const double *X, int ldx, const double *Y,
-                                          int ldy, double *C,
-                                          int ldc, double s) {
+                                          int ldy, double *C, int ldc, double s) {
+  double *Xs = smem, *Ys = smem + kGB * kLd;
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   const int g = lane >> 2, q = lane & 3;
   const int r0 = (w >> 1) * 16, c0 = (w & 1) * 32;
+  __syncthreads();   // the buffers are free (a previous use has finished)
+#pragma unroll 4
+  for (int e8 = 0; e8 < kGB * kGB / kGT; ++e8) {
+    const int e = t + e8 * kGT;
+    {
+      const int i = e % kGB, k = e / kGB;
+      const bool ok = i < M && k < Kd;
+      cp_async8(Xs + k * kLd + i, ok ? X + (int64_t)k * ldx + i : X, ok ? 8 : 0);
+    }
+    if (YT) {
+      const int j = e % kGB, k = e / kGB;
+      const bool ok = j < N && k < Kd;
+      cp_async8(Ys + k * kLd + j, ok ? Y + (int64_t)k * ldy + j : Y, ok ? 8 : 0);
+    } else {
+      const int k = e % kGB, j = e / kGB;
+      const bool ok = j < N && k < Kd;
+      cp_async8(Ys + j * kLd + k, ok ? Y + (int64_t)j * ldy + k : Y, ok ? 8 : 0);
+    }
+  }
+  double cv[2][4][2];
+  if (ACC) {
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int i = r0 + a * 8 + g, j = c0 + b * 8 + 2 * q + h;
+          cv[a][b][h] = (i < M && j < N) ? C[(int64_t)j * ldc + i] : 0.0;
+        }
+  }
   double acc[2][4][2];
 #pragma unroll
   for (int a = 0; a < 2; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
-  for (int kc = 0; kc < Kd; kc += kKC) {
-    __syncthreads();
+  cp_async_wait_all();
+  __syncthreads();
+#pragma unroll 4
+  for (int k0 = 0; k0 < kGB; k0 += 4) {
+    double av[2], bv[4];
 #pragma unroll
-    for (int e8 = 0; e8 < kKC * kGB / kGT; ++e8) {
-      const int e = t + e8 * kGT;
-      {
-        const int i = e % kGB, k = e / kGB;   // X: rows contiguous
-        sm.Xs[i][k] = (i < M && kc + k < Kd) ? X[(int64_t)(kc + k) * ldx + i] : 0.0;
-      }
-      if (YT) {
-        const int j = e % kGB, k = e / kGB;   // Y[k][j]: j contiguous
-        sm.Ys[j][k] = (j < N && kc + k < Kd) ? Y[(int64_t)(kc + k) * ldy + j] : 0.0;
-      } else {
-        const int k = e % kKC, j = e / kKC;   // Y[k][j] = Y[j * ldy + k]: k contiguous
-        sm.Ys[j][k] = (j < N && kc + k < Kd) ? Y[(int64_t)j * ldy + kc + k] : 0.0;
-      }
-    }
-    __syncthreads();
+    for (int a = 0; a < 2; ++a) av[a] = Xs[(k0 + q) * kLd + r0 + a * 8 + g];
 #pragma unroll
-    for (int k0 = 0; k0 < kKC; k0 += 4) {
-      double av[2], bv[4];
+    for (int b = 0; b < 4; ++b)
+      bv[b] = YT ? Ys[(k0 + q) * kLd + c0 + b * 8 + g] : Ys[(c0 + b * 8 + g) * kLd + k0 + q];
 #pragma unroll
-      for (int a = 0; a < 2; ++a) av[a] = sm.Xs[r0 + a * 8 + g][k0 + q];
+    for (int a = 0; a < 2; ++a)
 #pragma unroll
-      for (int b = 0; b < 4; ++b) bv[b] = sm.Ys[c0 + b * 8 + g][k0 + q];
-#pragma unroll
-      for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) dmma(acc[a][b], av[a], bv[b]);
-    }
+      for (int b = 0; b < 4; ++b) dmma(acc[a][b], av[a], bv[b]);
   }
   __syncthreads();   // C may alias an operand
 #pragma unroll
@@ -110,8 +132,7 @@ __device__ __forceinline__ void tile_gemm(GemmSmem &sm, int M, int N, int Kd,
       for (int h = 0; h < 2; ++h) {
         const int j = c0 + b * 8 + 2 * q + h;
         if (j >= N) continue;
-        double *c = C + (int64_t)j * ldc + i;
-        *c = ACC ? fma(s, acc[a][b][h], *c) : s * acc[a][b][h];
+        C[(int64_t)j * ldc + i] = ACC ? fma(s, acc[a][b][h], cv[a][b][h]) : s * acc[a][b][h];
       }
   }
 }
@@ -221,9 +242,9 @@ __global__ void __launch_bounds__(kGT, 3) k_sw_fg(int n, const double *A, int K0
     }
   }
   __syncthreads();
-  __shared__ __align__(16) GemmSmem sm;
+  extern __shared__ __align__(16) double gemm_smem[];
   // G_I (rows x bs) = F_I (rows x bs) P (bs x bs); P[k][j] = P[j * kGB + k]
-  tile_gemm<false, false>(sm, rows, bs, bs, F + i0, n, P, kGB, G + i0, n, 1.0);
+  tile_gemm<false, false>(gemm_smem, rows, bs, bs, F + i0, n, P, kGB, G + i0, n, 1.0);
 }
 
 // lower tile (I, J), I >= J: the column block gets G_I, the row block left
@@ -260,10 +281,10 @@ __global__ void __launch_bounds__(kGT, TPO_SW_MINB) k_sw_update(int n, double *A
     }
     return;
   }
-  __shared__ __align__(16) GemmSmem sm;
+  extern __shared__ __align__(16) double gemm_smem[];
   // Y[k][j] = F(j0 + j, k) = F[k * n + j0 + j]
-  tile_gemm<true, true>(sm, M, N, bs, G + i0, n, F + j0, n, A + (int64_t)j0 * n + i0, n,
-                        -1.0);
+  tile_gemm<true, true>(gemm_smem, M, N, bs, G + i0, n, F + j0, n, A + (int64_t)j0 * n + i0,
+                        n, -1.0);
   if (look && I == Kn && J == Kn) {
     __syncthreads();   // the tile's update is visible to the whole CTA
     sweep_diag(n, A, i0, M, P, info);
@@ -294,14 +315,23 @@ void launch_coarse_inverse(int64_t n64, double *A, double *work, int *info, cuda
   const int n = (int)n64;
   const int nt = (n + kGB - 1) / kGB;
   double *P = work, *F = work + kGB * kGB, *G = F + (size_t)n * kGB;
+  static unsigned long long attr_set = 0;   // bit per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!((attr_set >> (dev & 63)) & 1ull)) {
+    cudaFuncSetAttribute(k_sw_fg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
+    cudaFuncSetAttribute(k_sw_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kGemmSmem);
+    attr_set |= 1ull << (dev & 63);
+  }
   cudaMemsetAsync(info, 0, sizeof(int), s);
   count_launch();
   k_sw_diag<<<1, kGT, 0, s>>>(n, A, 0, std::min(kGB, n), P, info);
   for (int K0 = 0; K0 < n; K0 += kGB) {
     const int bs = std::min(kGB, n - K0);
     count_launch(2);
-    k_sw_fg<<<nt, kGT, 0, s>>>(n, A, K0, bs, P, F, G);
-    k_sw_update<<<dim3(nt, nt), kGT, 0, s>>>(n, A, K0, bs, F, G, P, info);
+    k_sw_fg<<<nt, kGT, kGemmSmem, s>>>(n, A, K0, bs, P, F, G);
+    k_sw_update<<<dim3(nt, nt), kGT, kGemmSmem, s>>>(n, A, K0, bs, F, G, P, info);
   }
   count_launch();
   k_sw_final<<<dim3(nt, nt), kGT, 0, s>>>(n, A);
