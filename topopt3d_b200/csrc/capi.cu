@@ -222,7 +222,7 @@ int alloc_solver(Ctx &c) {
       A(v.S64, 243 * v.nn);
       if (l < c.ps) {
         A(v.H64, 126 * v.nn);
-        A(v.H32, 126 * v.nn);
+        A(v.H32, 126 * ((v.nn + 31) / 32) * 32);   // tiles of 32 nodes (kernels_mg.cu)
       }
       if (l >= c.ps && l + 1 < c.L) {
         A(v.A64, 243 * v.nn);

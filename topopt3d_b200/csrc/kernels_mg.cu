@@ -308,6 +308,34 @@ __global__ void __launch_bounds__(32 * kStencilRows)
   }
 }
 
+// The FP32 copy of a half-stored stencil is grouped by tiles of 32 nodes:
+// coefficient hq (0..125) of node n at ((n / 32) * 126 + hq) * 32 + n % 32,
+// so the 126 x 32 values a warp reads for its 32 nodes are one contiguous
+// 16,128-byte block that one bulk L2 prefetch covers.  The FP64 copy stays
+// coefficient-major, hq * nn + n.
+constexpr int kH32Tile = 32;
+__host__ __device__ __forceinline__ int64_t h32_index(int hq, int64_t n) {
+  return ((n / kH32Tile) * 126 + hq) * kH32Tile + n % kH32Tile;
+}
+template <typename T>
+__device__ __forceinline__ const T *hcoef(const T *H, int hq, int64_t n, int64_t nn);
+template <>
+__device__ __forceinline__ const double *hcoef(const double *H, int hq, int64_t n,
+                                               int64_t nn) {
+  return H + hq * nn + n;
+}
+template <>
+__device__ __forceinline__ const float *hcoef(const float *H, int hq, int64_t n, int64_t) {
+  return H + h32_index(hq, n);
+}
+// one bulk prefetch of a 32-node tile of the FP32 stencil into L2
+__device__ __forceinline__ void prefetch_h32_tile(const float *H, int64_t n) {
+  const float *p = H + (n / kH32Tile) * 126 * kH32Tile;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p),
+               "r"(126 * kH32Tile * 4)
+               : "memory");
+}
+
 // Symmetric half of a Galerkin stencil: A(n, n+d) = A(n+d, n)^T, so only
 // the centre block and the 13 forward offsets (nb = 13..26) are stored,
 // H[(h*9 + 3r + s) * nn + n] with h = nb - 13.  The apply reads the forward
@@ -322,7 +350,8 @@ __global__ void k_stencil_to_half(int64_t nn, const double *__restrict__ S,
        t += (int64_t)gridDim.x * blockDim.x) {
     const double v = S[117 * nn + t];   // (13*9 + q) * nn + n
     H64[t] = v;
-    H32[t] = static_cast<float>(v);
+    const int64_t hq = t / nn, n = t - hq * nn;
+    H32[h32_index((int)hq, n)] = static_cast<float>(v);
   }
 }
 
@@ -367,22 +396,20 @@ __global__ void __launch_bounds__(128, 16)
     k_apply_stencil_sym1(int nx, int ny, int nz, const T *__restrict__ H,
                          const ApplyArgs<T> args) {
   const int nn = nx * ny * nz;
-  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nn;
-       n += gridDim.x * blockDim.x) {
+  // stride between the 9 coefficients of one block
+  const int64_t qs = sizeof(T) == 4 ? kH32Tile : (int64_t)nn;
+  const int stride = gridDim.x * blockDim.x;
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nn; n += stride) {
+    // FP32: a warp's 32 nodes are one tile of the stencil; the tile this
+    // warp takes next goes to L2 in one bulk prefetch
+    if (sizeof(T) == 4 && (threadIdx.x & 31) == 0 && n + stride < nn)
+      prefetch_h32_tile(reinterpret_cast<const float *>(H), n + stride);
     const int i = n % nx, j = (n / nx) % ny, k = n / (nx * ny);
     T a0 = 0, a1 = 0, a2 = 0;
 #pragma unroll 1
     for (int h = 0; h < 14; ++h) {
       const int nb = 13 + h;
       const int di = nb % 3 - 1, dj = (nb / 3) % 3 - 1, dk = nb / 9 - 1;
-      // FP32: the forward block two steps ahead into L2 while this one is
-      // used (the FP64 form measured slower with it)
-      if (sizeof(T) == 4 && h + 2 < 14) {
-        const T *pf = H + (int64_t)(h + 2) * 9 * nn + n;
-#pragma unroll
-        for (int q = 0; q < 9; ++q)
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(pf + q * (int64_t)nn));
-      }
       // forward block A(n, n+d): zero when n+d is outside, index clamped
       {
         const int mi = min(i + di, nx - 1), mj = min(max(j + dj, 0), ny - 1),
@@ -390,10 +417,10 @@ __global__ void __launch_bounds__(128, 16)
         const int m = (mk * ny + mj) * nx + max(mi, 0);
         const T u0 = sym_in<T, IN>(args, 3 * m), u1 = sym_in<T, IN>(args, 3 * m + 1),
                 u2 = sym_in<T, IN>(args, 3 * m + 2);
-        const T *s = H + (int64_t)h * 9 * nn + n;
-        a0 += s[0] * u0 + s[nn] * u1 + s[2 * (int64_t)nn] * u2;
-        a1 += s[3 * (int64_t)nn] * u0 + s[4 * (int64_t)nn] * u1 + s[5 * (int64_t)nn] * u2;
-        a2 += s[6 * (int64_t)nn] * u0 + s[7 * (int64_t)nn] * u1 + s[8 * (int64_t)nn] * u2;
+        const T *s = hcoef(H, h * 9, n, nn);
+        a0 += s[0] * u0 + s[qs] * u1 + s[2 * qs] * u2;
+        a1 += s[3 * qs] * u0 + s[4 * qs] * u1 + s[5 * qs] * u2;
+        a2 += s[6 * qs] * u0 + s[7 * qs] * u1 + s[8 * qs] * u2;
       }
       // backward block A(n, n-d) = A(n-d, n)^T, stored by node n-d
       if (h > 0) {
@@ -403,10 +430,10 @@ __global__ void __launch_bounds__(128, 16)
         const T w = in ? T(1) : T(0);
         const T u0 = w * sym_in<T, IN>(args, 3 * m), u1 = w * sym_in<T, IN>(args, 3 * m + 1),
                 u2 = w * sym_in<T, IN>(args, 3 * m + 2);
-        const T *s = H + (int64_t)h * 9 * nn + m;
-        a0 += s[0] * u0 + s[3 * (int64_t)nn] * u1 + s[6 * (int64_t)nn] * u2;
-        a1 += s[nn] * u0 + s[4 * (int64_t)nn] * u1 + s[7 * (int64_t)nn] * u2;
-        a2 += s[2 * (int64_t)nn] * u0 + s[5 * (int64_t)nn] * u1 + s[8 * (int64_t)nn] * u2;
+        const T *s = hcoef(H, h * 9, m, nn);
+        a0 += s[0] * u0 + s[3 * qs] * u1 + s[6 * qs] * u2;
+        a1 += s[qs] * u0 + s[4 * qs] * u1 + s[7 * qs] * u2;
+        a2 += s[2 * qs] * u0 + s[5 * qs] * u1 + s[8 * qs] * u2;
       }
     }
     const bool need_u = OUT == OUT_CHEB2 || OUT == OUT_POST0 || OUT == OUT_POST1;
@@ -425,8 +452,11 @@ __global__ void k_apply_stencil_sym(int nx, int ny, int nz,
                                     const T *__restrict__ b, T *__restrict__ y,
                                     int64_t ld) {
   const int nn = nx * ny * nz;
-  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nn;
-       n += gridDim.x * blockDim.x) {
+  const int64_t qs = sizeof(T) == 4 ? kH32Tile : (int64_t)nn;
+  const int stride = gridDim.x * blockDim.x;
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nn; n += stride) {
+    if (sizeof(T) == 4 && (threadIdx.x & 31) == 0 && n + stride < nn)
+      prefetch_h32_tile(reinterpret_cast<const float *>(H), n + stride);
     const int i = n % nx, j = (n / nx) % ny, k = n / (nx * ny);
     T a[NB][3];
 #pragma unroll
@@ -435,23 +465,15 @@ __global__ void k_apply_stencil_sym(int nx, int ny, int nz,
     for (int h = 0; h < 14; ++h) {
       const int nb = 13 + h;
       const int di = nb % 3 - 1, dj = (nb / 3) % 3 - 1, dk = nb / 9 - 1;
-      // FP32: the forward block two steps ahead into L2, as in the
-      // single-column kernel
-      if (sizeof(T) == 4 && h + 2 < 14) {
-        const T *pf = H + (int64_t)(h + 2) * 9 * nn + n;
-#pragma unroll
-        for (int q = 0; q < 9; ++q)
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(pf + q * (int64_t)nn));
-      }
       // forward block A(n, n+d): zero when n+d is outside, index clamped
       {
         const int mi = min(i + di, nx - 1), mj = min(max(j + dj, 0), ny - 1),
                   mk = min(k + dk, nz - 1);
         const int m = (mk * ny + mj) * nx + max(mi, 0);
-        const T *sp = H + (int64_t)h * 9 * nn + n;
+        const T *sp = hcoef(H, h * 9, n, nn);
         T c[9];
 #pragma unroll
-        for (int q = 0; q < 9; ++q) c[q] = sp[q * (int64_t)nn];
+        for (int q = 0; q < 9; ++q) c[q] = sp[q * qs];
 #pragma unroll
         for (int col = 0; col < NB; ++col) {
           const T *uc = u + col * ld;
@@ -467,10 +489,10 @@ __global__ void k_apply_stencil_sym(int nx, int ny, int nz,
         const bool in = mi >= 0 && mi < nx && mj >= 0 && mj < ny && mk >= 0 && mk < nz;
         const int m = in ? (mk * ny + mj) * nx + mi : n;
         const T w = in ? T(1) : T(0);
-        const T *sp = H + (int64_t)h * 9 * nn + m;
+        const T *sp = hcoef(H, h * 9, m, nn);
         T c[9];
 #pragma unroll
-        for (int q = 0; q < 9; ++q) c[q] = sp[q * (int64_t)nn];
+        for (int q = 0; q < 9; ++q) c[q] = sp[q * qs];
 #pragma unroll
         for (int col = 0; col < NB; ++col) {
           const T *uc = u + col * ld;
