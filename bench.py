@@ -134,6 +134,7 @@ class ClockSampler:
         self.file = None
 
     def __enter__(self):
+        self.skip = 0
         try:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(
@@ -142,6 +143,19 @@ class ClockSampler:
                 stdout=self.file, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return self
+        # the sampler takes a moment to start: wait (at most 5 s) for its
+        # first row, and count only the rows written after this point, so
+        # every sample used falls inside the timed region
+        t_end = time.perf_counter() + 5.0
+        while time.perf_counter() < t_end and self.proc.poll() is None:
+            self.file.flush()
+            with open(self.file.name) as f:
+                n = sum(1 for r in f if r.strip())
+            if n > 0:
+                self.skip = n
+                break
+            time.sleep(0.01)
         return self
 
     def __exit__(self, *a):
@@ -157,7 +171,7 @@ class ClockSampler:
             return None
         self.file.flush()
         with open(self.file.name) as f:
-            rows = [r.strip().split(", ") for r in f if r.strip()]
+            rows = [r.strip().split(", ") for r in f if r.strip()][self.skip:]
         os.unlink(self.file.name)
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
