@@ -274,13 +274,100 @@ int copy_slot(Ctx &c, int dst, int src, int nb) {
   return TPO_OK;
 }
 
+// The device-resident PCG loop.  A CUDA graph holds a while node whose
+// body is one CG iteration followed by k_loop_check, which applies the
+// host loop's per-column test on the device (breakdown: rho, pq not
+// positive or r.r not finite; convergence: r.r <= target) and freezes the
+// finished columns, then keeps the loop going while a column is active,
+// fewer than maxit iterations are done and no coarse-grid barrier has run
+// out.  k_loop_start opens the loop under the same condition; the while
+// node's default is closed, so a loop that is never opened runs nothing.
+__global__ void k_loop_start(double *scal, int nb, cudaGraphConditionalHandle h) {
+  bool any = false;
+  for (int j = 0; j < nb; ++j) any |= scal[j * kColScal + 6] == 0.0;
+  const bool go = any && scal[SC_LOOP_K] < scal[SC_LOOP_MAXIT] && scal[kSlotFault] == 0.0;
+  cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+__global__ void k_loop_check(double *scal, int nb, cudaGraphConditionalHandle h) {
+  const double k = scal[SC_LOOP_K] + 1.0;
+  scal[SC_LOOP_K] = k;
+  bool any = false;
+  for (int j = 0; j < nb; ++j) {
+    double *sc = scal + j * kColScal;
+    if (sc[6] != 0.0) continue;
+    scal[SC_LOOP_ITS + j] = k;
+    const double rho = sc[0], pq = sc[2], rr = sc[3];
+    if (!(rho > 0) || !(pq > 0) || !isfinite(rr)) {
+      scal[SC_LOOP_STATUS + j] = -1.0;
+      sc[6] = 1.0;
+    } else if (rr <= scal[SC_LOOP_TARGET + j]) {
+      scal[SC_LOOP_STATUS + j] = 1.0;
+      sc[6] = 1.0;
+    } else {
+      any = true;
+    }
+  }
+  const bool go = any && k < scal[SC_LOOP_MAXIT] && scal[kSlotFault] == 0.0;
+  cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+// the loop graph of cg_body (not the first iteration) for nb columns;
+// *body_nodes receives the kernel launches of one iteration
+template <typename T>
+int build_loop_graph(Ctx &c, const tpo_solve_opts &o, T *x, T *r, T *z, T *p, T *q,
+                     int nb, cudaGraphExec_t *exec, long long *body_nodes) {
+  cudaStream_t s = c.stream;
+  const int64_t n = 3 * c.nn;
+  cudaGraph_t graph = nullptr;
+  CK(cudaGraphCreate(&graph, 0));
+  cudaGraphConditionalHandle h;
+  CK(cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault));
+  cudaGraphNode_t start;
+  {
+    cudaKernelNodeParams kp = {};
+    double *scal = c.scal;
+    void *args[] = {&scal, &nb, &h};
+    kp.func = (void *)k_loop_start;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(1);
+    kp.kernelParams = args;
+    CK(cudaGraphAddKernelNode(&start, graph, nullptr, 0, &kp));
+  }
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t loop;
+  CK(cudaGraphAddNode(&loop, graph, &start, 1, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  const long long before = g_launches.load();
+  CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
+                                   cudaStreamCaptureModeThreadLocal));
+  cg_body<T>(c, n, x, r, z, p, q, o, false, s, nb);
+  k_loop_check<<<1, 1, 0, s>>>(c.scal, nb, h);
+  count_launch();
+  const cudaError_t ce = cudaStreamEndCapture(s, &body);
+  // captured launches run when the graph is launched, not now
+  *body_nodes = g_launches.load() - before;
+  count_launch(-*body_nodes);
+  CK(ce);
+  CK(cudaGraphInstantiate(exec, graph, 0));
+  CK(cudaGraphDestroy(graph));
+  return TPO_OK;
+}
+
 // PCG on the fine operator in precision T for nb columns.  x holds the
 // initial guesses and r must already hold b - K x; ||r_j||^2 is in slot 3
 // of the host mirror.  Column j stops at ||r_j||^2 <= target_rr[j]; columns
 // with frozen[j] set do not iterate.  On return its[j] = iterations of
 // column j and st[j] = its status.  resume: continue the previous run's
 // recurrence (the first iteration forms p = z + beta p from the p and rho
-// left in place) instead of starting with p = z.
+// left in place) instead of starting with p = z.  With o.use_graph the
+// iterations after the first run in one launch of the loop graph, with the
+// per-iteration test on the device; otherwise each iteration is launched
+// from the host and tested there.
 template <typename T>
 int pcg_loop(Ctx &c, const tpo_solve_opts &o, T *x, T *r, T *z, T *p, T *q,
              const double *target_rr, int maxit, int nb, double *frozen,
@@ -304,42 +391,13 @@ int pcg_loop(Ctx &c, const tpo_solve_opts &o, T *x, T *r, T *z, T *p, T *q,
   }
   if (!active) return TPO_OK;
   if (int rc = upload_slot(c, 6, frozen, nb)) return rc;
-  int k = 0;
-  while (k < maxit && active) {
-    const bool first = (k == 0) && !resume;
-    if (!first && o.use_graph) {
-      if (!g || gx != (const void *)x || gnb != nb) {
-        if (g) {
-          cudaGraphExecDestroy(g);
-          g = nullptr;
-        }
-        cudaGraph_t graph;
-        const long long before = g_launches.load();
-        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        cg_body<T>(c, n, x, r, z, p, q, o, false, s, nb);
-        CK(cudaStreamEndCapture(s, &graph));
-        // captured launches run when the graph is launched, not now
-        gnodes = g_launches.load() - before;
-        count_launch(-gnodes);
-        CK(cudaGraphInstantiate(&g, graph, 0));
-        CK(cudaGraphDestroy(graph));
-        gx = x;
-        gnb = nb;
-      }
-      CK(cudaGraphLaunch(g, s));
-      count_launch(gnodes);
-    } else {
-      cg_body<T>(c, n, x, r, z, p, q, o, first, s, nb);
-    }
-    CK(cudaGetLastError());
-    CK(c.coarse_err);
-    ++k;
-    if (int rc = readback(c, nb)) return rc;
+  // the host test of one iteration's scalars (in the mirror)
+  auto host_test = [&](int k) -> int {
     bool changed = false;
     for (int j = 0; j < nb; ++j) {
       if (frozen[j] != 0.0) continue;
-      const double *h = c.scal_h + j * kColScal;
-      const double rho = h[0], pq = h[2], rr = h[3];
+      const double *hs = c.scal_h + j * kColScal;
+      const double rho = hs[0], pq = hs[2], rr = hs[3];
       its[j] = k;
       if (!(rho > 0) || !(pq > 0) || !std::isfinite(rr)) {
         st[j] = TPO_E_BREAKDOWN;
@@ -355,6 +413,77 @@ int pcg_loop(Ctx &c, const tpo_solve_opts &o, T *x, T *r, T *z, T *p, T *q,
     }
     if (changed && active)
       if (int rc = upload_slot(c, 6, frozen, nb)) return rc;
+    return TPO_OK;
+  };
+  int k = 0;
+  if (!o.use_graph) {
+    while (k < maxit && active) {
+      cg_body<T>(c, n, x, r, z, p, q, o, k == 0 && !resume, s, nb);
+      CK(cudaGetLastError());
+      CK(c.coarse_err);
+      ++k;
+      if (int rc = readback(c, nb)) return rc;
+      if (int rc = host_test(k)) return rc;
+    }
+  } else {
+    if (!resume && maxit > 0) {   // the first iteration (p = z), from the host
+      cg_body<T>(c, n, x, r, z, p, q, o, true, s, nb);
+      CK(cudaGetLastError());
+      CK(c.coarse_err);
+      k = 1;
+      if (int rc = readback(c, nb)) return rc;
+      if (int rc = host_test(k)) return rc;
+    }
+    if (active && k < maxit) {
+      if (!g || gx != (const void *)x || gnb != nb) {
+        if (g) {
+          cudaGraphExecDestroy(g);
+          g = nullptr;
+        }
+        if (int rc = build_loop_graph<T>(c, o, x, r, z, p, q, nb, &g, &gnodes)) return rc;
+        CK(c.coarse_err);
+        gx = x;
+        gnb = nb;
+      }
+      // loop state: per column target, iterations so far and status; the
+      // iterations done and the limit (one copy from the pinned mirror; the
+      // host does not touch those mirror slots until the read-back below)
+      double *hs = c.scal_h;
+      for (int j = 0; j < kMaxBatch; ++j) {
+        hs[SC_LOOP_TARGET + j] = j < nb ? target_rr[j] : 0.0;
+        hs[SC_LOOP_ITS + j] = j < nb ? its[j] : 0.0;
+        hs[SC_LOOP_STATUS + j] = 0.0;
+      }
+      hs[SC_LOOP_K] = k;
+      hs[SC_LOOP_MAXIT] = maxit;
+      CK(cudaMemcpyAsync(c.scal + SC_LOOP_TARGET, hs + SC_LOOP_TARGET,
+                         sizeof(double) * (SC_LOOP_MAXIT + 1 - SC_LOOP_TARGET),
+                         cudaMemcpyHostToDevice, s));
+      CK(cudaGraphLaunch(g, s));
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(hs + SC_LOOP_ITS, c.scal + SC_LOOP_ITS,
+                         sizeof(double) * (SC_LOOP_K + 1 - SC_LOOP_ITS),
+                         cudaMemcpyDeviceToHost, s));
+      if (int rc = readback(c, nb)) return rc;   // synchronises
+      const int k_end = (int)hs[SC_LOOP_K];
+      count_launch(1 + (long long)(k_end - k) * gnodes);
+      k = k_end;
+      for (int j = 0; j < nb; ++j) {
+        if (frozen[j] != 0.0) continue;
+        its[j] = (int)hs[SC_LOOP_ITS + j];
+        const double stj = hs[SC_LOOP_STATUS + j];
+        if (stj < 0.0) {
+          st[j] = TPO_E_BREAKDOWN;
+          c.err = "CG breakdown (indefinite preconditioner/operator or non-finite residual)";
+        } else if (stj > 0.0) {
+          st[j] = TPO_OK;
+        } else {
+          continue;
+        }
+        frozen[j] = 1.0;
+        --active;
+      }
+    }
   }
   int worst = TPO_OK;
   for (int j = 0; j < nb; ++j)

@@ -216,7 +216,8 @@ struct Ctx {
   int mma_steps = 0;   // dual Newton steps of the last tpo_mma_update
   double *mma_h = nullptr;
 
-  // CUDA graphs of the CG iteration bodies, keyed on (x, columns)
+  // CUDA graphs of the CG iteration loop (a device-side while loop around
+  // the iteration body), keyed on (x, columns)
   cudaGraphExec_t graph64 = nullptr, graph32 = nullptr;
   const void *graph64_x = nullptr, *graph32_x = nullptr;
   int graph64_nb = 0, graph32_nb = 0;
@@ -251,7 +252,15 @@ enum { SC_COMPLIANCE = kScalMisc, SC_VOLUME, SC_OC_DG, SC_OC_CHANGE, SC_POWER };
 constexpr int SC_POWER_PREV = SC_POWER + kMaxLevels;
 // blocks that passed every barrier of tpo_barrier_selftest
 constexpr int SC_SELFTEST = SC_POWER_PREV + kMaxLevels;
-constexpr int kScalCount = SC_SELFTEST + 1;
+// the device-resident PCG loop (solver.cu): per column the target r.r,
+// the iteration count and the status (0 running, 1 converged, -1
+// breakdown); the iterations done and the iteration limit
+constexpr int SC_LOOP_TARGET = SC_SELFTEST + 1;
+constexpr int SC_LOOP_ITS = SC_LOOP_TARGET + kMaxBatch;
+constexpr int SC_LOOP_STATUS = SC_LOOP_ITS + kMaxBatch;
+constexpr int SC_LOOP_K = SC_LOOP_STATUS + kMaxBatch;
+constexpr int SC_LOOP_MAXIT = SC_LOOP_K + 1;
+constexpr int kScalCount = SC_LOOP_MAXIT + 1;
 constexpr int kSlotFault = 7;
 
 // fixed reduction grid (blocks per column) for a block of nb columns
