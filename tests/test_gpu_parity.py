@@ -153,6 +153,26 @@ def test_mixed_setup_fp32_chebyshev_bounds(T, oracle):
 
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_device_loop_matches_host_loop(T, oracle, prec):
+    """The PCG iterations run as a device-side graph loop (use_graph, the
+    default) or one launch and one host test per iteration: the same
+    iterations, the same residual replacements and the same solution."""
+    nel = (24, 12, 12)
+    spec = P.cantilever_bcs(nel)
+    x = np.random.default_rng(5).uniform(0.05, 1.0, int(np.prod(nel)))
+    runs = []
+    for use_graph in (1, 0):
+        t, _ = pair(T, oracle, nel, levels=3, spec=spec, x=x)
+        precision = T.PREC_FP64 if prec == "fp64" else T.PREC_MIXED
+        info = t.FESolve(T.default_opts(precision=precision, use_graph=use_graph))
+        assert info["status"] == 0
+        runs.append((info["iterations"], info["outer"], t.U.copy()))
+        t.close()
+    assert runs[0][0] == runs[1][0] and runs[0][1] == runs[1][1]
+    assert rel(runs[0][2], runs[1][2]) < 1e-14
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_cfg0_solve_compliance_sensitivity(T, oracle, prec):
     nel = P.CONFIGS["cfg0"]["nel"]
     x = P.design("cfg0")

@@ -416,7 +416,9 @@ int pcg_loop(Ctx &c, const tpo_solve_opts &o, T *x, T *r, T *z, T *p, T *q,
     return TPO_OK;
   };
   int k = 0;
-  if (!o.use_graph) {
+  // a device without conditional graph nodes runs the host-tested loop
+  static bool loop_graphs_ok = true;
+  if (!o.use_graph || !loop_graphs_ok) {
     while (k < maxit && active) {
       cg_body<T>(c, n, x, r, z, p, q, o, k == 0 && !resume, s, nb);
       CK(cudaGetLastError());
@@ -440,7 +442,26 @@ int pcg_loop(Ctx &c, const tpo_solve_opts &o, T *x, T *r, T *z, T *p, T *q,
           cudaGraphExecDestroy(g);
           g = nullptr;
         }
-        if (int rc = build_loop_graph<T>(c, o, x, r, z, p, q, nb, &g, &gnodes)) return rc;
+        if (build_loop_graph<T>(c, o, x, r, z, p, q, nb, &g, &gnodes) != TPO_OK) {
+          // not available here: clear the (non-sticky) error and continue
+          // with the host-tested loop from iteration k
+          cudaGetLastError();
+          c.err.clear();
+          if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+          }
+          loop_graphs_ok = false;
+          while (k < maxit && active) {
+            cg_body<T>(c, n, x, r, z, p, q, o, false, s, nb);
+            CK(cudaGetLastError());
+            CK(c.coarse_err);
+            ++k;
+            if (int rc = readback(c, nb)) return rc;
+            if (int rc = host_test(k)) return rc;
+          }
+          goto done;
+        }
         CK(c.coarse_err);
         gx = x;
         gnb = nb;
@@ -485,6 +506,7 @@ int pcg_loop(Ctx &c, const tpo_solve_opts &o, T *x, T *r, T *z, T *p, T *q,
       }
     }
   }
+done:
   int worst = TPO_OK;
   for (int j = 0; j < nb; ++j)
     if (st[j] < 0 ? st[j] < worst : (worst == TPO_OK && st[j] != TPO_OK))
