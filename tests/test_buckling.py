@@ -188,6 +188,21 @@ def test_buckling_small_column(T, precond):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("block", [5, 16, 32])
+def test_buckling_block_widths(T, block):
+    """The block eigensolver's tall-skinny kernels at other widths (5: a
+    partly filled accumulator block, 16, and 32, the largest block the ABI
+    takes, with its two-by-two Gram super-tiles): the same eigenvalues as
+    the golden fixture."""
+    g = fixture("buckling_column_8x4x8")
+    t = gpu_problem(T, g)
+    nev = min(int(g["nev"]), block)
+    lam = t.buckling(nev=nev, block=block, tol=1e-8)
+    assert t.last_eig["status"] == 0, t.last_eig
+    np.testing.assert_allclose(lam, g["lam"][:nev], rtol=1e-9)
+
+
+@pytest.mark.gpu
 def test_buckling_cfg4(T):
     """The 96x48x48 column (698,691 dof): the 6 largest lambda, block 12,
     against the oracle's ARPACK eigenvalues to 1e-6 relative."""

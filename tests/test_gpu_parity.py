@@ -152,6 +152,20 @@ def test_mixed_setup_fp32_chebyshev_bounds(T, oracle):
         assert abs(t.level_lambda(l) - ref.level_lambda(l)) < 1e-10 * ref.level_lambda(l)
 
 
+@pytest.mark.parametrize("nel,levels", [((2, 1, 1), 1), ((3, 2, 2), 1), ((5, 4, 3), 1),
+                                        ((8, 4, 4), 2), ((12, 12, 12), 2)])
+def test_coarsest_inverse_sizes(T, oracle, nel, levels):
+    """The dense inverse of the coarsest operator (blocked sweeps in blocks
+    of 64) at sizes below one block, across block boundaries and with a
+    partial last block (36, 108, 360, 135 and 1,029 dof): the FP64 solve
+    matches the oracle's."""
+    t, ref = pair(T, oracle, nel, levels=levels, seed=7)
+    Uo, st, _, _ = ref.solve()
+    info = t.FESolve(T.default_opts(precision=T.PREC_FP64))
+    assert st == 0 and info["status"] == 0
+    assert rel(t.U, Uo) < 1e-9
+
+
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_device_loop_matches_host_loop(T, oracle, prec):
     """The PCG iterations run as a device-side graph loop (use_graph, the
