@@ -54,7 +54,8 @@ def parse():
     # --config also selects the reference arm's problem (default 192x96x96)
     ap.add_argument("--kernel", default=None,
                     choices=["apply32", "apply64", "vcycle32", "vcycle64",
-                             "solve_mixed", "solve_fp64", "mma", "setup", "setup_mixed"])
+                             "solve_mixed", "solve_fp64", "mma", "setup", "setup_mixed",
+                             "level1_32", "level1_32_stencil"])
     ap.add_argument("--config", default=CONFIG)
     ap.add_argument("--reps", type=int, default=3)
     return ap.parse_args()
@@ -747,6 +748,12 @@ def run_kernel_case(args):
     u64 = torch.randn(n, dtype=torch.float64, device=dev)
     y64 = torch.empty_like(u64)
     u32, y32 = u64.float(), torch.empty(n, dtype=torch.float32, device=dev)
+    if args.kernel in ("level1_32", "level1_32_stencil"):
+        # the FP32 level-1 operator: the tensor-core form or the stored stencil
+        t.set_level1_form(1 if args.kernel == "level1_32_stencil" else 0)
+        n1 = 3 * int(np.prod(t.level_dims(1)))
+        u1 = torch.randn(n1, dtype=torch.float64, device=dev)
+        y1 = torch.empty_like(u1)
     if args.kernel == "mma":
         # MMA update (m = 2, the constraints of mma_pair) at the design, with the
         # compliance sensitivity of one solve; device-resident state, reset
@@ -780,6 +787,9 @@ def run_kernel_case(args):
             # (FP64 form, or the mixed form's FP32 Chebyshev bounds)
             t.FEAssemble(T.default_opts(precision=T.PREC_MIXED)
                          if args.kernel == "setup_mixed" else None)
+            continue
+        if args.kernel in ("level1_32", "level1_32_stencil"):
+            t.apply_level(1, u1, y1, precision=T.PREC_MIXED)
             continue
         if args.kernel == "apply32":
             rc = lib.tpo_apply_f32(t._h, C.c_void_p(u32.data_ptr()),

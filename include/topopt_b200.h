@@ -165,6 +165,19 @@ TPO_API int tpo_apply_f32(tpo_ctx *ctx, const float *u, float *y);
 /* y = A_l u on GMG level l with the assembled Galerkin operator (l >= 1) */
 TPO_API int tpo_apply_level(tpo_ctx *ctx, int32_t level, const double *u, double *y,
                     int mem);
+/* tpo_apply_level in a chosen precision: TPO_PREC_FP64 as tpo_apply_level,
+ * TPO_PREC_MIXED runs the FP32 operator the mixed-precision V-cycle uses on
+ * that level (u rounded to FP32, y widened back); levels 0 .. the last one
+ * above the persistent coarse levels. */
+TPO_API int tpo_apply_level_prec(tpo_ctx *ctx, int32_t level, const double *u, double *y,
+                                 int32_t precision, int mem);
+/* Form of the FP32 level-1 operator (the reference's Galerkin PCMG level,
+ * FEAnalysis.cpp:410-416): 0 automatic = the tensor-core matrix-free form
+ * sum_E sum_i E_i G_i u_E whenever every element count is even and level 1
+ * lies above the persistent coarse levels, else the stored stencil; 1 = the
+ * stored half stencil always.  *tensor (optional) receives 1 when the
+ * tensor-core form is in use.  Takes effect at the next apply or solve. */
+TPO_API int tpo_set_level1_form(tpo_ctx *ctx, int32_t form, int32_t *tensor);
 /* one application of the GMG V-cycle preconditioner z = M r (finest) */
 TPO_API int tpo_vcycle(tpo_ctx *ctx, const double *r, double *z, int32_t precision,
                int mem);

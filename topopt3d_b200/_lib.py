@@ -30,7 +30,7 @@ EXPORTS = (
     "tpo_sizes", "tpo_level_dims", "tpo_add_bc", "tpo_set_bc", "tpo_get_bc",
     "tpo_fe_initialize", "tpo_mat_int_fnc", "tpo_set_moduli",
     "tpo_fe_assemble", "tpo_fe_solve", "tpo_solve", "tpo_apply", "tpo_apply_f32",
-    "tpo_apply_level", "tpo_vcycle", "tpo_level_lambda", "tpo_get_vector",
+    "tpo_apply_level", "tpo_apply_level_prec", "tpo_set_level1_form", "tpo_vcycle", "tpo_level_lambda", "tpo_get_vector",
     "tpo_set_vector", "tpo_compliance", "tpo_volume", "tpo_filter",
     "tpo_oc_update", "tpo_sync", "tpo_set_stream", "tpo_kernel_launches",
     "tpo_sensitivity_noalloc", "tpo_default_eig_opts", "tpo_ks_assemble",
@@ -122,6 +122,8 @@ def load(path: str | None = None):
         "tpo_apply": (C.c_int, [vp, vp, vp, i32, i32, C.c_int]),
         "tpo_apply_f32": (C.c_int, [vp, vp, vp]),
         "tpo_apply_level": (C.c_int, [vp, i32, vp, vp, C.c_int]),
+        "tpo_apply_level_prec": (C.c_int, [vp, i32, vp, vp, i32, C.c_int]),
+        "tpo_set_level1_form": (C.c_int, [vp, i32, C.POINTER(i32)]),
         "tpo_vcycle": (C.c_int, [vp, vp, vp, i32, C.c_int]),
         "tpo_level_lambda": (C.c_int, [vp, i32, dp]),
         "tpo_get_vector": (C.c_int, [vp, C.c_char_p, vp, C.c_int]),

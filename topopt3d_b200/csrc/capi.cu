@@ -250,6 +250,8 @@ void free_all(Ctx &c) {
   dfree(c.E64); dfree(c.dEdz); dfree(c.E32); dfree(c.S0); dfree(c.K0lex);
   dfree(c.GMi); dfree(c.gk_slot); dfree(c.gk_elem); dfree(c.gk_count);
   dfree(c.gk_G); c.gk_cap = 0; dfree(c.gd_tmp);
+  dfree(c.l1_B); dfree(c.l1_rows); dfree(c.l1_C); c.l1_cap = 0; dfree(c.l1_cval);
+  dfree(c.l1_cflag); dfree(c.l1_count); dfree(c.l1_fault); c.l1_bimg_ready = false;
   dfree(c.Ainv); dfree(c.Adense); dfree(c.dev_info);
   dfree(c.finv); dfree(c.taps_d);
   dfree(c.w64);
@@ -447,6 +449,17 @@ int tpo_create(const tpo_mesh_params *p, tpo_ctx **out) {
   }
   A(c.x, c.ne); A(c.rho, c.ne); A(c.E64, c.ne); A(c.dEdz, c.ne); A(c.E32, c.ne);
   A(c.Es64, c.ne); A(c.dEsdz64, c.ne);
+  // level 1 on the tensor cores: even element counts (every level-1
+  // element holds 2 x 2 x 2 fine ones) and level 1 above the persistent
+  // levels
+  c.l1tc_ok = c.L >= 2 && c.ps > 1 && c.nel[0] % 2 == 0 && c.nel[1] % 2 == 0 &&
+              c.nel[2] % 2 == 0;
+  if (c.l1tc_ok) {
+    int tx = 0, ty = 0, zc = 0, nz = 0;
+    tpo::l1tc_grid(c.lev[1], &tx, &ty, &zc, &nz);
+    A(c.l1_B, 2 * 192 * 24); A(c.l1_cval, 3 * c.lev[1].nn); A(c.l1_cflag, (size_t)tx * ty * nz);
+    A(c.l1_count, 1); A(c.l1_fault, 1);
+  }
   A(c.fix, c.nn); A(c.idm, c.nn); A(c.F, 3 * c.nn); A(c.U, 3 * c.nn);
   A(c.scal, tpo::kScalCount); A(c.part, tpo::kPartCount); A(c.ticket, tpo::kMaxBatch + tpo::kAuxStreams);
   A(c.gbar, 1);
@@ -1105,6 +1118,47 @@ int tpo_apply_level(tpo_ctx *ctx, int32_t level, const double *u, double *y,
   else
     tpo::launch_apply_stencil<double>(c.lev[level], c.lev[level].S64, du, nullptr, dy, c.stream);
   if (int rc = copy_out(c, y, dy, n, mem)) return rc;
+  return finish(c, TPO_OK);
+}
+
+int tpo_apply_level_prec(tpo_ctx *ctx, int32_t level, const double *u, double *y,
+                         int32_t precision, int mem) {
+  if (precision == TPO_PREC_FP64) return tpo_apply_level(ctx, level, u, y, mem);
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  if (int rc = check_mem(c, mem, {u, y})) return rc;
+  REQUIRE(c.assembled, "tpo_fe_assemble must be called first");
+  REQUIRE(precision == TPO_PREC_MIXED, "precision must be TPO_PREC_FP64 or TPO_PREC_MIXED");
+  REQUIRE(level >= 0 && (level == 0 || level < c.ps) && u && y,
+          "FP32 operators exist on the levels above the persistent ones");
+  const size_t n = 3 * c.lev[level].nn;
+  const double *du = nullptr;
+  if (int rc = stage_in(c, u, n, mem, c.io_a, &du)) return rc;
+  double *dy = (mem == TPO_MEM_DEVICE) ? y : c.io_b;
+  tpo::launch_d2f((int64_t)n, du, c.r32, c.stream);
+  if (level == 0) {
+    tpo::launch_apply_fine<float>(c, c.E32, c.r32, nullptr, c.q32, c.stream);
+  } else if (level == 1 && tpo::l1_tensor(c)) {
+    tpo::ApplyArgs<float> a{};
+    a.u = c.r32;
+    a.y = c.q32;
+    tpo::launch_l1tc(c, tpo::IN_U, tpo::OUT_Y, a, c.stream);
+  } else {
+    tpo::launch_apply_stencil_sym<float>(c.lev[level], c.lev[level].H32, c.r32, nullptr,
+                                         c.q32, c.stream, 1);
+  }
+  tpo::launch_f2d((int64_t)n, c.q32, dy, c.stream);
+  if (int rc = copy_out(c, y, dy, n, mem)) return rc;
+  return finish(c, TPO_OK);
+}
+
+int tpo_set_level1_form(tpo_ctx *ctx, int32_t form, int32_t *tensor) {
+  if (int rc = begin(ctx)) return rc;
+  Ctx &c = ctx->c;
+  REQUIRE(form == 0 || form == 1, "form must be 0 (automatic) or 1 (stored stencil)");
+  c.l1_form = form;
+  tpo::invalidate_graphs(c);
+  if (tensor) *tensor = tpo::l1_tensor(c) ? 1 : 0;
   return finish(c, TPO_OK);
 }
 

@@ -17,6 +17,7 @@
 
 #include "tpo_internal.h"
 #include "transfer.cuh"
+#include "fused_out.cuh"
 
 namespace tpo {
 
@@ -352,37 +353,6 @@ __global__ void k_stencil_to_half(int64_t nn, const double *__restrict__ S,
     H64[t] = v;
     const int64_t hq = t / nn, n = t - hq * nn;
     H32[h32_index((int)hq, n)] = static_cast<float>(v);
-  }
-}
-
-// one column; IN / OUT select how the input is formed and what the
-// epilogue writes, as in the fine-level kernel (kernels_apply_staged.cu,
-// finish_dof): IN_U reads u, IN_CHEB forms the Chebyshev start
-// invtheta D^-1 b on the fly; OUT_Y / OUT_RESID / OUT_CHEB2 / OUT_POST0 /
-// OUT_POST1 write Au, b - Au or the fused Chebyshev(2) updates
-template <typename T, int IN>
-__device__ __forceinline__ T sym_in(const ApplyArgs<T> &a, int i) {
-  if (IN == IN_CHEB) return a.invtheta * (a.dinv[i] * a.b[i]);
-  return a.u[i];
-}
-
-template <typename T, int OUT>
-__device__ __forceinline__ void sym_out(const ApplyArgs<T> &a, int i, T Au, T u) {
-  if (OUT == OUT_Y) {
-    a.y[i] = Au;
-  } else if (OUT == OUT_RESID) {
-    a.y[i] = a.b[i] - Au;
-  } else if (OUT == OUT_CHEB2) {
-    const T di = a.dinv[i], bi = a.b[i];
-    const T r1 = di * bi - di * Au;
-    a.y[i] = u + (a.c1 * u + a.c2 * r1);
-  } else if (OUT == OUT_POST0) {
-    const T d0 = a.invtheta * (a.dinv[i] * (a.b[i] - Au));
-    a.y[i] = d0;
-    a.y2[i] = u + d0;
-  } else {   // OUT_POST1
-    const T r1 = a.theta * u - a.dinv[i] * Au;
-    a.y[i] = a.y2[i] + (a.c1 * u + a.c2 * r1);
   }
 }
 
@@ -771,7 +741,8 @@ int launch_galerkin_fine(Ctx &c, double *Sc, cudaStream_t s) {
   count_launch();
   k_galerkin_fine<<<grid_for(27 * c.lev[1].nn, 128, 1 << 20), 128, 0, s>>>(
       c.nel[0], c.nel[1], c.nel[2], c.E64, c.idm, c.gk_slot, c.gk_G, c.GMi, Sc);
-  return TPO_OK;
+  // the tensor-core form of the FP32 level-1 operator (kernels_l1tc.cu)
+  return l1tc_prepare(c, Sc, (int)nslots, s);
 }
 
 void launch_galerkin_dims(const Level &fine, const double *Sf, double *Sc,

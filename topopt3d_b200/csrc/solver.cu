@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <type_traits>
 
 #include "coarse.h"
 #include "solver.h"
@@ -62,6 +63,16 @@ void level_apply(Ctx &c, int l, const T *u, const T *b, T *y, cudaStream_t s,
   if (l == 0) {
     launch_apply_fine<T>(c, fineE(c, (T *)nullptr), u, b, y, s, nb);
   } else if (l < c.ps) {
+    if constexpr (std::is_same<T, float>::value) {
+      if (l == 1 && nb == 1 && l1_tensor(c)) {
+        ApplyArgs<float> a{};
+        a.u = u;
+        a.b = b;
+        a.y = y;
+        launch_l1tc(c, IN_U, b ? OUT_RESID : OUT_Y, a, s);
+        return;
+      }
+    }
     launch_apply_stencil_sym<T>(c.lev[l], halfS(c.lev[l], (T *)nullptr), u, b,
                                 y, s, nb);
   } else {
@@ -157,11 +168,16 @@ void vcycle_rec(Ctx &c, int l, const T *b, T *x, const tpo_solve_opts &o,
     a.theta = static_cast<T>(ch.theta);
     a.c1 = static_cast<T>(rn * ch.rho0);
     a.c2 = static_cast<T>(2.0 * rn / ch.delta);
+    bool tensor = false;   // level 1 in FP32 on the tensor cores
+    if constexpr (std::is_same<T, float>::value) tensor = l == 1 && l1_tensor(c);
     auto fused = [&](int in, int out) {
-      if (fine_fused)
+      if (fine_fused) {
         launch_apply_fused<T>(c, E, in, out, a, s, nb);
-      else
+      } else if (tensor) {
+        if constexpr (std::is_same<T, float>::value) launch_l1tc(c, in, out, a, s);
+      } else {
         launch_apply_sym_fused<T>(v, H, in, out, a, s);
+      }
     };
     a.y = x;
     fused(IN_CHEB, OUT_CHEB2);                                 // pre-smooth
@@ -241,12 +257,15 @@ int readback(Ctx &c, int nb) {
                      cudaMemcpyDeviceToHost, c.stream));
   CK(cudaStreamSynchronize(c.stream));
   if (c.scal_h[kSlotFault] != 0.0) {
-    // a grid barrier of the coarse-grid kernel gave up waiting: the blocks
-    // returned and the counter may be mid-barrier, so clear both
+    // 1: a grid barrier of the coarse-grid kernel gave up waiting (the
+    // blocks returned and the counter may be mid-barrier, so clear both);
+    // 2: the level-1 tensor-core kernel gave up waiting for an MMA
+    const bool mma = c.scal_h[kSlotFault] == 2.0;
     c.scal_h[kSlotFault] = 0.0;
     CK(cudaMemsetAsync(c.gbar, 0, sizeof(unsigned int), c.stream));
     CK(cudaMemsetAsync(c.scal + kSlotFault, 0, sizeof(double), c.stream));
-    c.err = "coarse-grid kernel: a grid-barrier wait ran out";
+    c.err = mma ? "level-1 tensor-core kernel: an MMA wait ran out"
+                : "coarse-grid kernel: a grid-barrier wait ran out";
     return TPO_E_CUDA;
   }
   return TPO_OK;
@@ -645,9 +664,16 @@ int setup_on(Ctx &c, const tpo_solve_opts &o, cudaStream_t s) {
   launch_to_dense(cl, Sc, c.Ainv, s);
   launch_coarse_inverse(nc, c.Ainv, c.Adense, c.dev_info, s);
   CK(cudaGetLastError());
-  int info_h = 0;
+  int info_h = 0, l1_fault_h = 0;
   CK(cudaMemcpyAsync(&info_h, c.dev_info, sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (c.l1tc_ok)
+    CK(cudaMemcpyAsync(&l1_fault_h, c.l1_fault, sizeof(int), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
+  if (l1_fault_h != 0) {
+    c.err = "level-1 correction rows exceed their capacity";
+    join();
+    return TPO_E_CUDA;
+  }
   if (info_h != 0) {
     c.err = "coarsest operator is not positive definite (pivot " +
             std::to_string(info_h - 1) + ")";

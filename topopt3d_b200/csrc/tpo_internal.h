@@ -167,6 +167,25 @@ struct Ctx {
   unsigned int *gk_count = nullptr;
   double *gk_G = nullptr;
   size_t gk_cap = 0;
+  // level 1 in FP32 on the tensor cores (kernels_l1tc.cu): the form
+  // requested (0 automatic, 1 always the stored stencil), whether the
+  // context qualifies (even element counts, level 1 above the persistent
+  // levels), the operand image of the 8 blocks G_i (hi and lo TF32 parts),
+  // the correction rows of the nodes next to general-path coarse elements
+  // (node of each row, rows of 243 values, capacity in rows), C u on those
+  // rows as a dense level-1 vector, the CTAs holding such nodes, the row
+  // count and the overflow flag
+  int l1_form = 0;
+  bool l1tc_ok = false;
+  bool l1_bimg_ready = false;
+  float *l1_B = nullptr;
+  int *l1_rows = nullptr;
+  float *l1_C = nullptr;
+  size_t l1_cap = 0;
+  float *l1_cval = nullptr;
+  uint8_t *l1_cflag = nullptr;
+  unsigned int *l1_count = nullptr;
+  int *l1_fault = nullptr;
   // scratch of the dimension-by-dimension Galerkin products (levels >= 1)
   double *gd_tmp = nullptr;
   double *Ainv = nullptr;   // dense inverse of the coarsest operator
@@ -315,6 +334,17 @@ void launch_apply_sym_fused(const Level &v, const T *H, int in, int out,
                             const ApplyArgs<T> &a, cudaStream_t s);
 void launch_stencil_to_half(int64_t nn, const double *S, double *H64,
                             float *H32, cudaStream_t s);
+// level 1 on the tensor cores (kernels_l1tc.cu)
+// true when the FP32 level-1 operator runs on the tensor-core kernel
+inline bool l1_tensor(const Ctx &c) { return c.l1tc_ok && c.l1_form == 0; }
+// per-context operand image and per-assembly correction rows; syncs the
+// stream once when the correction capacity has to grow
+int l1tc_prepare(Ctx &c, const double *Sc, int nslots, cudaStream_t s);
+// y = A_1 u (OUT_Y), b - A_1 u (OUT_RESID) or the fused Chebyshev(2)
+// forms, one column (two launches: the correction rows, then the apply)
+void launch_l1tc(const Ctx &c, int in, int out, const ApplyArgs<float> &a, cudaStream_t s);
+// the grid of the kernel: x tiles, y tiles, node planes per CTA, z chunks
+void l1tc_grid(const Level &v, int *tx, int *ty, int *zchunk, int *nz);
 // the same product one dimension at a time (three launches through tmp,
 // galerkin_dims_scratch doubles)
 void launch_galerkin_dims(const Level &fine, const double *Sf, double *Sc,

@@ -183,12 +183,22 @@ class TopOpt:
                     "apply")
         return y
 
-    def apply_level(self, level, u, y):
+    def apply_level(self, level, u, y, precision=L.PREC_FP64):
         up, mem, k1 = _buf(u)
         yp, _, k2 = _buf(y, writable=True)
-        self._check(self._lib.tpo_apply_level(self._h, level, up, yp, mem),
+        self._check(self._lib.tpo_apply_level_prec(self._h, level, up, yp,
+                                                   precision, mem),
                     "apply_level")
         return y
+
+    def set_level1_form(self, form):
+        """0: tensor-core level-1 operator where the mesh allows it (the
+        default), 1: the stored stencil.  Returns True when the tensor-core
+        form is in use."""
+        on = C.c_int32()
+        self._check(self._lib.tpo_set_level1_form(self._h, form, C.byref(on)),
+                    "set_level1_form")
+        return bool(on.value)
 
     def vcycle(self, r, z, precision=L.PREC_FP64):
         rp, mem, k1 = _buf(r, 3 * self.nNode)
