@@ -29,7 +29,9 @@
 // to them add a stored correction: their full stencil row (k_galerkin_fine)
 // minus the sum above, 27 blocks of 3 x 3.  A small kernel ahead of the
 // apply forms C u on those rows (one warp per row) into a dense vector that
-// the apply's CTAs holding such nodes add in their epilogue.
+// the apply's CTAs holding such nodes add in their epilogue.  The apply is a
+// programmatic dependent launch: its CTAs start while the small kernel runs,
+// and only the CTAs that read the vector wait for it (griddepcontrol).
 #include <algorithm>
 
 #include "fused_out.cuh"
@@ -151,6 +153,16 @@ __global__ void k_l1_corr(int cx, int cy, int cz, int64_t cap_rows, const double
   }
 }
 
+// programmatic dependent launch: let the next kernel in the stream start,
+// and wait for the grids this one depends on (no-ops without the launch
+// attribute)
+__device__ __forceinline__ void pdl_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // cval[3 n + r] = (C u)_r on the correction rows, one warp per row; u in the
 // input form IN of the apply
 template <int IN>
@@ -159,6 +171,7 @@ __global__ void k_l1_corr_apply(int cx, int cy, int cz, int64_t cap_rows,
                                 const unsigned int *__restrict__ count,
                                 const float *__restrict__ C, const ApplyArgs<float> a,
                                 float *__restrict__ cval) {
+  pdl_launch_dependents();   // the apply may start; it waits where it reads cval
   const int lane = threadIdx.x & 31;
   const int64_t nrows = min((int64_t)*count, cap_rows);
   const int64_t wstride = (int64_t)gridDim.x * (blockDim.x / 32);
@@ -371,6 +384,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         issue(0, tmem);
       }
     }
+    if (corr) pdl_wait();   // cval comes from the kernel launched just before
     float carry[3] = {0.0f, 0.0f, 0.0f};
     for (int k = kfirst; k <= klast; ++k) {
       const int it = k - kfirst, b = it & 1;
@@ -468,19 +482,35 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
   }
   if (failed) *p.fault = 2.0;
+  pdl_wait();   // this grid completes after the kernel it was launched behind
 }
 
+// pdl: launched behind k_l1_corr_apply as a programmatic dependent launch
 template <int IN, int OUT>
-void launch_mode(const L1Params &p, dim3 grid, const ApplyArgs<float> &a, cudaStream_t s) {
+void launch_mode(const L1Params &p, dim3 grid, const ApplyArgs<float> &a, bool pdl,
+                 cudaStream_t s) {
   static int attr_dev = -1;
   int dev = 0;
   cudaGetDevice(&dev);
   if (attr_dev != dev) {
     cudaFuncSetAttribute(k_apply_l1_tc<IN, OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          kSmemBytes);
+    // two CTAs per SM need the largest shared-memory carveout
+    cudaFuncSetAttribute(k_apply_l1_tc<IN, OUT>,
+                         cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     attr_dev = dev;
   }
-  k_apply_l1_tc<IN, OUT><<<grid, kThreads, kSmemBytes, s>>>(p, a);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = kSmemBytes;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k_apply_l1_tc<IN, OUT>, p, a);
 }
 
 int grid_for(int64_t n, int threads) {
@@ -546,17 +576,21 @@ void launch_l1tc(const Ctx &c, int in, int out, const ApplyArgs<float> &a, cudaS
   const Level &v = c.lev[1];
   int tx, ty, zc, nz;
   l1tc_grid(v, &tx, &ty, &zc, &nz);
-  // C u on the correction rows first (a warp per row)
-  const int corr_blocks = (int)std::min<size_t>((c.l1_cap + 7) / 8, 148 * 8);
-  count_launch(2);
-  if (in == IN_CHEB)
-    k_l1_corr_apply<IN_CHEB><<<corr_blocks, 256, 0, s>>>(
-        v.dims[0], v.dims[1], v.dims[2], (int64_t)c.l1_cap, c.l1_rows, c.l1_count, c.l1_C, a,
-        c.l1_cval);
-  else
-    k_l1_corr_apply<IN_U><<<corr_blocks, 256, 0, s>>>(v.dims[0], v.dims[1], v.dims[2],
-                                                       (int64_t)c.l1_cap, c.l1_rows,
-                                                       c.l1_count, c.l1_C, a, c.l1_cval);
+  // C u on the correction rows first (a warp per row; the row count is the
+  // one the last set-up read back)
+  const bool pdl = c.l1_nrows > 0;
+  if (pdl) {
+    const int blocks = (c.l1_nrows + 3) / 4;
+    count_launch();
+    if (in == IN_CHEB)
+      k_l1_corr_apply<IN_CHEB><<<blocks, 128, 0, s>>>(v.dims[0], v.dims[1], v.dims[2],
+                                                       (int64_t)c.l1_cap, c.l1_rows, c.l1_count,
+                                                       c.l1_C, a, c.l1_cval);
+    else
+      k_l1_corr_apply<IN_U><<<blocks, 128, 0, s>>>(v.dims[0], v.dims[1], v.dims[2],
+                                                    (int64_t)c.l1_cap, c.l1_rows, c.l1_count,
+                                                    c.l1_C, a, c.l1_cval);
+  }
   L1Params p;
   p.cx = v.dims[0];
   p.cy = v.dims[1];
@@ -569,16 +603,17 @@ void launch_l1tc(const Ctx &c, int in, int out, const ApplyArgs<float> &a, cudaS
   p.cflag = c.l1_cflag;
   p.fault = c.scal + kSlotFault;
   const dim3 grid(tx * ty, nz);
+  count_launch();
   if (in == IN_CHEB && out == OUT_CHEB2)
-    launch_mode<IN_CHEB, OUT_CHEB2>(p, grid, a, s);
+    launch_mode<IN_CHEB, OUT_CHEB2>(p, grid, a, pdl, s);
   else if (out == OUT_POST0)
-    launch_mode<IN_U, OUT_POST0>(p, grid, a, s);
+    launch_mode<IN_U, OUT_POST0>(p, grid, a, pdl, s);
   else if (out == OUT_POST1)
-    launch_mode<IN_U, OUT_POST1>(p, grid, a, s);
+    launch_mode<IN_U, OUT_POST1>(p, grid, a, pdl, s);
   else if (out == OUT_RESID)
-    launch_mode<IN_U, OUT_RESID>(p, grid, a, s);
+    launch_mode<IN_U, OUT_RESID>(p, grid, a, pdl, s);
   else
-    launch_mode<IN_U, OUT_Y>(p, grid, a, s);
+    launch_mode<IN_U, OUT_Y>(p, grid, a, pdl, s);
 }
 
 }  // namespace tpo

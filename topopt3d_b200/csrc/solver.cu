@@ -665,10 +665,14 @@ int setup_on(Ctx &c, const tpo_solve_opts &o, cudaStream_t s) {
   launch_coarse_inverse(nc, c.Ainv, c.Adense, c.dev_info, s);
   CK(cudaGetLastError());
   int info_h = 0, l1_fault_h = 0;
+  unsigned int l1_rows_h = 0;
   CK(cudaMemcpyAsync(&info_h, c.dev_info, sizeof(int), cudaMemcpyDeviceToHost, s));
-  if (c.l1tc_ok)
+  if (c.l1tc_ok) {
     CK(cudaMemcpyAsync(&l1_fault_h, c.l1_fault, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&l1_rows_h, c.l1_count, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+  }
   CK(cudaStreamSynchronize(s));
+  c.l1_nrows = (int)std::min<size_t>(l1_rows_h, c.l1_cap);
   if (l1_fault_h != 0) {
     c.err = "level-1 correction rows exceed their capacity";
     join();

@@ -185,6 +185,7 @@ struct Ctx {
   float *l1_cval = nullptr;
   uint8_t *l1_cflag = nullptr;
   unsigned int *l1_count = nullptr;
+  int l1_nrows = 0;   // host copy of the row count (read at the end of set-up)
   int *l1_fault = nullptr;
   // scratch of the dimension-by-dimension Galerkin products (levels >= 1)
   double *gd_tmp = nullptr;
@@ -341,7 +342,8 @@ inline bool l1_tensor(const Ctx &c) { return c.l1tc_ok && c.l1_form == 0; }
 // stream once when the correction capacity has to grow
 int l1tc_prepare(Ctx &c, const double *Sc, int nslots, cudaStream_t s);
 // y = A_1 u (OUT_Y), b - A_1 u (OUT_RESID) or the fused Chebyshev(2)
-// forms, one column (two launches: the correction rows, then the apply)
+// forms, one column (two launches: the correction rows, then the apply,
+// which starts while the first runs)
 void launch_l1tc(const Ctx &c, int in, int out, const ApplyArgs<float> &a, cudaStream_t s);
 // the grid of the kernel: x tiles, y tiles, node planes per CTA, z chunks
 void l1tc_grid(const Level &v, int *tx, int *ty, int *zchunk, int *nz);
