@@ -58,6 +58,9 @@ def parse():
                              "level1_32", "level1_32_stencil"])
     ap.add_argument("--config", default=CONFIG)
     ap.add_argument("--reps", type=int, default=3)
+    # profiling cases: issue the CG iterations from the host instead of the
+    # device-side loop graph, so that a profiler lists every kernel launch
+    ap.add_argument("--no-graph", action="store_true")
     return ap.parse_args()
 
 
@@ -803,7 +806,7 @@ def run_kernel_case(args):
         else:
             prec = T.PREC_MIXED if args.kernel == "solve_mixed" else T.PREC_FP64
             t.set("U", torch.zeros(n, dtype=torch.float64, device=dev))
-            t.FESolve(T.default_opts(precision=prec))
+            t.FESolve(T.default_opts(precision=prec, use_graph=0 if args.no_graph else 1))
     torch.cuda.synchronize(dev)
     extra = ""
     if args.kernel == "mma":
