@@ -4,6 +4,7 @@
 // the partials in a fixed tree order and writes the result to a device
 // scalar, so the CG recurrences never round-trip through the host.
 #include <algorithm>
+#include <cstdint>
 
 #include "tpo_internal.h"
 
@@ -64,6 +65,39 @@ __device__ __forceinline__ void finish_reduction(double v, double *part,
   }
 }
 
+// 16-byte vectors of the streamed kernels: 4 floats or 2 doubles
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  using V = float4;
+  static constexpr int W = 4;
+  __device__ static float get(const V &v, int k) {
+    return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
+  }
+  __device__ static void set(V &v, int k, float x) {
+    if (k == 0) v.x = x; else if (k == 1) v.y = x; else if (k == 2) v.z = x; else v.w = x;
+  }
+};
+template <>
+struct Vec16<double> {
+  using V = double2;
+  static constexpr int W = 2;
+  __device__ static double get(const V &v, int k) { return k == 0 ? v.x : v.y; }
+  __device__ static void set(V &v, int k, double x) {
+    if (k == 0) v.x = x; else v.y = x;
+  }
+};
+
+__device__ __forceinline__ bool aligned16(const void *p) {
+  return (reinterpret_cast<uintptr_t>(p) & 15u) == 0;
+}
+
+// The streamed kernels walk a column in 16-byte vectors when its pointers
+// allow (then the tail, fewer than one vector, element by element), else
+// element by element; either way each thread's share and the order of its
+// sums are fixed, so the reductions stay deterministic.
+
 // a.b per column (blockIdx.y); a column whose skip flag is set (every block
 // of it returns, so its ticket stays zero) keeps its out/shift_to slots
 template <typename T>
@@ -71,13 +105,29 @@ __global__ void __launch_bounds__(kRedThreads)
     k_dot(int64_t n, const T *__restrict__ a, const T *__restrict__ b,
           double *part, unsigned int *ticket, double *out, double *shift_to,
           const double *skip) {
+  using VT = Vec16<T>;
+  using V = typename VT::V;
   const int j = blockIdx.y;
   if (skip && skip[j * kColScal] != 0.0) return;
   a += j * n;
   b += j * n;
+  const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t st = (int64_t)gridDim.x * blockDim.x;
   double s = 0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
+  int64_t tail = 0;
+  if (aligned16(a) && aligned16(b)) {
+    const int64_t nv = n / VT::W;
+    const V *av = reinterpret_cast<const V *>(a);
+    const V *bv = reinterpret_cast<const V *>(b);
+    for (int64_t i = t0; i < nv; i += st) {
+      const V x = av[i], y = bv[i];
+#pragma unroll
+      for (int k = 0; k < VT::W; ++k)
+        s += static_cast<double>(VT::get(x, k)) * static_cast<double>(VT::get(y, k));
+    }
+    tail = nv * VT::W;
+  }
+  for (int64_t i = tail + t0; i < n; i += st)
     s += static_cast<double>(a[i]) * static_cast<double>(b[i]);
   finish_reduction(s, part + j * gridDim.x, ticket + j, out + j * kColScal,
                    shift_to ? shift_to + j * kColScal : nullptr);
@@ -88,15 +138,33 @@ __global__ void __launch_bounds__(kRedThreads)
 template <typename T>
 __global__ void k_cg_p(int64_t n, const T *__restrict__ z, T *__restrict__ p,
                        const double *__restrict__ scal, bool first) {
+  using VT = Vec16<T>;
+  using V = typename VT::V;
   const int j = blockIdx.y;
   const double *sc = scal + j * kColScal;
   if (sc[6] != 0.0) return;
   z += j * n;
   p += j * n;
   const T beta = first ? T(0) : static_cast<T>(sc[0] / sc[1]);
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    p[i] = first ? z[i] : z[i] + beta * p[i];
+  const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t st = (int64_t)gridDim.x * blockDim.x;
+  int64_t tail = 0;
+  if (aligned16(z) && aligned16(p)) {
+    const int64_t nv = n / VT::W;
+    const V *zv = reinterpret_cast<const V *>(z);
+    V *pv = reinterpret_cast<V *>(p);
+    for (int64_t i = t0; i < nv; i += st) {
+      const V zz = zv[i];
+      V pp = first ? zz : pv[i];
+      if (!first) {
+#pragma unroll
+        for (int k = 0; k < VT::W; ++k) VT::set(pp, k, VT::get(zz, k) + beta * VT::get(pp, k));
+      }
+      pv[i] = pp;
+    }
+    tail = nv * VT::W;
+  }
+  for (int64_t i = tail + t0; i < n; i += st) p[i] = first ? z[i] : z[i] + beta * p[i];
 }
 
 // x += alpha p ; r -= alpha q ; rr = r.r   with alpha = rho / (p.q), per
@@ -107,6 +175,8 @@ __global__ void __launch_bounds__(kRedThreads)
                 const T *__restrict__ p, const T *__restrict__ q,
                 const double *__restrict__ scal, double *part,
                 unsigned int *ticket, double *rr) {
+  using VT = Vec16<T>;
+  using V = typename VT::V;
   const int j = blockIdx.y;
   const double *sc = scal + j * kColScal;
   const bool frozen = sc[6] != 0.0;
@@ -115,9 +185,36 @@ __global__ void __launch_bounds__(kRedThreads)
   r += j * n;
   p += j * n;
   q += j * n;
+  const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t st = (int64_t)gridDim.x * blockDim.x;
   double s = 0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
+  int64_t tail = 0;
+  if (aligned16(x) && aligned16(r) && aligned16(p) && aligned16(q)) {
+    const int64_t nv = n / VT::W;
+    V *xv = reinterpret_cast<V *>(x);
+    V *rv = reinterpret_cast<V *>(r);
+    const V *pv = reinterpret_cast<const V *>(p);
+    const V *qv = reinterpret_cast<const V *>(q);
+    for (int64_t i = t0; i < nv; i += st) {
+      V rr_ = rv[i];
+      if (!frozen) {
+        V xx = xv[i];
+        const V pp = pv[i], qq = qv[i];
+#pragma unroll
+        for (int k = 0; k < VT::W; ++k) {
+          VT::set(xx, k, VT::get(xx, k) + alpha * VT::get(pp, k));
+          VT::set(rr_, k, VT::get(rr_, k) - alpha * VT::get(qq, k));
+        }
+        xv[i] = xx;
+        rv[i] = rr_;
+      }
+#pragma unroll
+      for (int k = 0; k < VT::W; ++k)
+        s += static_cast<double>(VT::get(rr_, k)) * static_cast<double>(VT::get(rr_, k));
+    }
+    tail = nv * VT::W;
+  }
+  for (int64_t i = tail + t0; i < n; i += st) {
     T ri = r[i];
     if (!frozen) {
       x[i] += alpha * p[i];
