@@ -57,6 +57,19 @@ def test_noalloc_argument_checks_need_no_gpu():
         assert rc in (_lib.TPO_E_ARG, _lib.TPO_E_UNSUPPORTED), bad
 
 
+def test_level1_form_and_level_apply_refuse_a_null_context():
+    """The level-1 form switch and the precision-selectable level apply
+    answer TPO_E_ARG for a null context without touching a GPU."""
+    import ctypes as C
+
+    from topopt3d_b200 import _lib
+    L = _lib.load()
+    on = C.c_int32(-1)
+    assert L.tpo_set_level1_form(None, 0, C.byref(on)) == _lib.TPO_E_ARG
+    assert L.tpo_apply_level_prec(None, 1, None, None, _lib.PREC_MIXED,
+                                  _lib.MEM_HOST) == _lib.TPO_E_ARG
+
+
 def test_k0_anisotropic_elements_decouple(oracle):
     """K0 of box elements with unequal edges and other materials keeps the
     properties the modal apply relies on: symmetric, 6 rigid-body modes,

@@ -113,6 +113,37 @@ def test_mixed_solve_with_tensor_level1(T, oracle, bc):
     assert abs(out[0][1] - out[1][1]) <= 1
 
 
+def test_level1_tensor_form_anisotropic_elements_and_material(T, oracle):
+    """Element edges (1, 0.5, 2), E0 = 210, nu = 0.25: the 8 blocks G_i come
+    from that K0, so the tensor-core operator must still match the oracle's
+    Galerkin level 1 and the stored FP32 stencil."""
+    dx, E0, nu = (1.0, 0.5, 2.0), 210.0, 0.25
+    spec = P.cantilever_bcs(NEL, dx)
+    ne = int(np.prod(NEL))
+    x = np.random.default_rng(14).uniform(0.05, 1.0, ne)
+    ref = oracle.Problem(NEL, dx=dx, E0=E0, nu=nu, rmin=1.5, mg_levels=LEVELS)
+    P.apply_bcs(ref, spec)
+    ref.set_design(x, 3.0, 1e-10)
+    ref.assemble(oracle.default_opts())
+    t = T.TopOpt(NEL, dx=dx, E0=E0, Nu0=nu, rmin=1.5, mg_levels=LEVELS)
+    P.apply_bcs(t, spec)
+    t.FEInitialize()
+    t.MatIntFnc(x)
+    t.FEAssemble()
+    n1 = ref.level_nodes(1)[0]
+    u = np.random.default_rng(7).standard_normal(3 * n1)
+    y_ref = ref.apply_level(1, u)
+    assert t.set_level1_form(0) is True
+    y_tc = t.apply_level(1, u, np.zeros_like(u), precision=T.PREC_MIXED)
+    t.set_level1_form(1)
+    y_st = t.apply_level(1, u, np.zeros_like(u), precision=T.PREC_MIXED)
+    t.set_level1_form(0)
+    assert rel(y_tc, y_ref) < 1e-5
+    assert rel(y_tc, y_st) < 2e-6
+
+
 def test_level1_form_needs_even_counts(T):
     t = T.TopOpt((127, 64, 64), rmin=1.5, mg_levels=LEVELS)
     assert t.set_level1_form(0) is False
+    with pytest.raises(T.TopOptError, match="form must be 0"):
+        t.set_level1_form(2)
