@@ -526,9 +526,20 @@ void l1tc_grid(const Level &v, int *tx, int *ty, int *zchunk, int *nz) {
   const int cx = v.dims[0], cy = v.dims[1], cz = v.dims[2];
   *tx = (cx + kOwnX - 1) / kOwnX;
   *ty = (cy + kOwnY - 1) / kOwnY;
-  // about two CTAs per SM (their TMEM and shared memory allow two)
+  // about two CTAs per SM (their TMEM and shared memory allow two); the SM
+  // count of the current device, read once per device
+  static int sm_count[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int &sms = sm_count[dev & 63];
+  if (sms == 0) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1)
+      n = 148;
+    sms = n;
+  }
   const int tiles = *tx * *ty;
-  int want = (2 * 148 + tiles / 2) / tiles;
+  int want = (2 * sms + tiles / 2) / tiles;
   want = std::max(1, std::min(want, cz));
   *zchunk = (cz + want - 1) / want;
   *nz = (cz + *zchunk - 1) / *zchunk;
